@@ -1,0 +1,190 @@
+/*
+ * within_gpu.h -- C ABI of the B200 (sm_100a) fixed-effects solve library
+ * `libwithin_gpu.so`.
+ *
+ * It is a drop-in for leostimpfle/within's preconditioned modified-LSMR solve
+ * of D'WD x = D'W y.  Every entry point names the reference interface it
+ * replaces (paths relative to the reference checkout).  Plain pointers and
+ * sizes only; no torch or CUDA runtime types cross the boundary (streams are
+ * passed as `void*` holding a cudaStream_t, NULL = the library's own stream).
+ *
+ * Conventions
+ *  - Return value: WITHIN_OK (0) or one of the WITHIN_ERR_* codes; the message
+ *    of the last failure on the calling thread is within_last_error().
+ *  - "host" buffers are ordinary CPU memory (pageable or pinned); "dev" buffers
+ *    are device pointers on the solver's device.
+ *  - Observation vectors are in the caller's order unless a name says
+ *    "internal" (the design's locality-sorted order, domain.rs:225-238).
+ *  - Multi-RHS arrays are column-major: column j of Y (n_obs x k) starts at
+ *    Y + j*n_obs, as in BatchSolveResult (solver.rs:246-293).
+ *  - Non-convergence is not an error: stats.converged = 0 (lsmr.rs:363-370).
+ */
+#ifndef WITHIN_GPU_H
+#define WITHIN_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes: crates/within/src/error.rs:9-146 and
+ * crates/schwarz-precond/src/error.rs:63-90. */
+#define WITHIN_OK 0
+#define WITHIN_ERR_INVALID_INPUT 1   /* SolveError::InvalidInput */
+#define WITHIN_ERR_BUILD 2           /* BuildError: validation (empty, mismatch, weights, DOF span) */
+#define WITHIN_ERR_UNSCALABLE 3      /* BuildError::UnscalableComponent */
+#define WITHIN_ERR_SINGULAR 4        /* BuildError::SingularDiagonal */
+#define WITHIN_ERR_INDEFINITE 5      /* mlsmr: preconditioner not positive definite (bidiag.rs:98-111) */
+#define WITHIN_ERR_DIMENSION 6       /* BuildError::PreconditionerDimensionMismatch */
+#define WITHIN_ERR_CUDA 7            /* device failure (allocation, launch) */
+#define WITHIN_ERR_UNSUPPORTED 8     /* request outside this build's limits */
+
+/* PreconditionerConfig (crates/within/src/config.rs:133-157) with
+ * LocalSolverConfig / ApproxCholConfig / ApproxSchurConfig / ScalingConfig. */
+#define WITHIN_PRECOND_OFF 0
+#define WITHIN_PRECOND_ADDITIVE 1
+#define WITHIN_PRECOND_DIAGONAL 2
+typedef struct {
+    int32_t kind;                 /* WITHIN_PRECOND_* */
+    uint64_t approx_chol_seed;    /* ApproxCholConfig.seed (config.rs:20-26) */
+    uint32_t approx_chol_split;   /* ApproxCholConfig.split_merge, 0 = None */
+    int32_t schur_exact;          /* SchurMode::Exact (config.rs:46-59) */
+    uint64_t schur_seed;          /* ApproxSchurConfig.seed */
+    uint32_t schur_split;         /* ApproxSchurConfig.split (>= 1) */
+    uint64_t dense_threshold;     /* LocalSolverConfig.dense_threshold (default 24) */
+    double scaling_tolerance;     /* ScalingConfig.tolerance (default 1e-9) */
+    uint64_t scaling_max_sweeps;  /* ScalingConfig.max_sweeps (default 2048) */
+    int32_t scaling_error;        /* ScalingFailure::Error (1) or ::Warn (0) */
+    int32_t reduction;            /* ReductionStrategy; accepted, the GPU combine is always a
+                                     deterministic gather (schwarz/planning.rs:48-152) */
+} within_precond_config;
+
+/* LsmrOptions (config.rs:159-178) */
+typedef struct {
+    double tol;                   /* default 1e-8 */
+    uint64_t maxiter;             /* default 1000 */
+    uint64_t local_size;          /* 0 = None (no windowed reorthogonalisation) */
+} within_lsmr_options;
+
+/* Arithmetic of the operator and preconditioner applies. */
+#define WITHIN_PRECISION_FP64 0      /* everything FP64 (the reference's arithmetic) */
+#define WITHIN_PRECISION_MIXED 1     /* FP32 applies inside FP64 iterative refinement */
+
+/* Per-RHS outcome: SolveResult fields (solver.rs:205-242). */
+typedef struct {
+    int32_t converged;
+    uint64_t iterations;          /* LSMR iterations (summed over refinement sweeps) */
+    double residual;              /* relative normal-equation residual estimate */
+    double time_total, time_setup, time_solve;   /* seconds */
+} within_solve_stats;
+
+typedef struct within_design within_design;
+typedef struct within_solver within_solver;
+typedef struct within_preconditioner within_preconditioner;
+
+/* ---- defaults ---- */
+/* PreconditionerConfig::default() / LsmrOptions::default() */
+void within_precond_config_default(within_precond_config* cfg);
+void within_lsmr_options_default(within_lsmr_options* opts);
+
+/* ---- design: crates/within/src/domain.rs, solver.rs:26-60 ---- */
+
+/* IntoDesign for ArrayView2<u32> (solver.rs:34-48): codes is n_obs x n_factors,
+ * column-major (F order), intercept-only factors, n_levels = max+1. */
+int within_design_from_categories(const uint32_t* codes, uint64_t n_obs, uint64_t n_factors,
+                                  within_design** out);
+/* Design::new(Vec<Effect>) (domain.rs:155-171, effect.rs:12-42): effect e has
+ * level codes levels[e] (n_obs each), an intercept flag and n_slopes[e] slope
+ * columns slopes[s] taken consecutively from the flat `slopes` pointer array. */
+int within_design_from_effects(uint64_t n_obs, uint64_t n_effects, const uint32_t* const* levels,
+                               const int32_t* intercept, const uint64_t* n_slopes,
+                               const double* const* slopes, within_design** out);
+void within_design_free(within_design* d);
+uint64_t within_design_n_obs(const within_design* d);
+uint64_t within_design_n_dofs(const within_design* d);
+
+/* ---- solver: crates/within/src/solver.rs:295-593 ---- */
+
+/* Solver::new (solver.rs:361-411).  weights (host, caller order) may be NULL;
+ * cfg NULL = PreconditionerInput::Default; prebuilt non-NULL =
+ * PreconditionerInput::Prebuilt (its DOF count must match).  device < 0 picks
+ * the current device.  The design is copied; it may be freed afterwards. */
+int within_solver_new(const within_design* design, const double* weights,
+                      const within_precond_config* cfg, const within_preconditioner* prebuilt,
+                      int32_t device, within_solver** out);
+void within_solver_free(within_solver* s);
+uint64_t within_solver_n_obs(const within_solver* s);
+uint64_t within_solver_n_dofs(const within_solver* s);
+/* Solver::warnings (solver.rs:415-417): number of BuildWarnings */
+uint64_t within_solver_n_warnings(const within_solver* s);
+/* SolveResult::unidentified: (term, level, column) triples; returns the count */
+uint64_t within_solver_unidentified(const within_solver* s, uint64_t* triples, uint64_t cap);
+/* CoefficientLayout (solver.rs:125-200): per term n_levels, offset, n_columns */
+uint64_t within_solver_n_terms(const within_solver* s);
+int within_solver_term_layout(const within_solver* s, uint64_t term, uint64_t* n_levels,
+                              uint64_t* offset, uint64_t* n_columns);
+/* Design::obs_perm (domain.rs:150-152): internal position -> caller index.
+ * Returns 1 and fills out (n_obs) when the design was locality-sorted, else 0. */
+int within_solver_obs_perm(const within_solver* s, uint32_t* out);
+/* Solver::preconditioner (solver.rs:579-582): a shared handle, NULL when the
+ * solver runs unpreconditioned.  Free it with within_preconditioner_free. */
+within_preconditioner* within_solver_preconditioner(const within_solver* s);
+/* Select the precision of subsequent solves (default WITHIN_PRECISION_FP64). */
+int within_solver_set_precision(within_solver* s, int32_t precision);
+
+/* Solver::solve (solver.rs:503-527): host y (caller order) -> host x (n_dofs,
+ * term-major, user parametrisation) and host demeaned (n_obs, caller order).
+ * Either output pointer may be NULL. */
+int within_solver_solve(within_solver* s, const double* y, const within_lsmr_options* opts,
+                        double* x_out, double* demeaned_out, within_solve_stats* stats);
+/* Solver::solve_batch (solver.rs:530-577): Y is n_obs x k column-major on the
+ * host; all k columns advance together through one multi-RHS LSMR that reads
+ * the design once per apply for every column.  stats has k entries. */
+int within_solver_solve_batch(within_solver* s, const double* Y, uint64_t k,
+                              const within_lsmr_options* opts, double* X_out, double* D_out,
+                              within_solve_stats* stats);
+/* Device-resident variant of solve_batch: Y_dev, X_dev, D_dev are device
+ * buffers (same layouts); stream NULL = the solver's stream. */
+int within_solver_solve_batch_device(within_solver* s, const double* Y_dev, uint64_t k,
+                                     const within_lsmr_options* opts, double* X_dev,
+                                     double* D_dev, within_solve_stats* stats, void* stream);
+
+/* One-shot solve / solve_batch (solver.rs:611-646): Solver::new + solve. */
+int within_solve(const within_design* design, const double* y, const double* weights,
+                 const within_lsmr_options* opts, const within_precond_config* cfg,
+                 double* x_out, double* demeaned_out, within_solve_stats* stats);
+int within_solve_batch(const within_design* design, const double* Y, uint64_t k,
+                       const double* weights, const within_lsmr_options* opts,
+                       const within_precond_config* cfg, double* X_out, double* D_out,
+                       within_solve_stats* stats);
+
+/* ---- Operator trait (crates/schwarz-precond/src/lib.rs:47-57) for the design
+ * operator A = W^{1/2} D of a solver (operator/design.rs:89-117), on device
+ * buffers in the INTERNAL observation order. ---- */
+int within_solver_operator_apply(within_solver* s, const double* x_dev, double* y_dev,
+                                 void* stream);
+int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, double* y_dev,
+                                         void* stream);
+
+/* ---- Preconditioner handle (operator/schwarz.rs:115-183) ---- */
+void within_preconditioner_free(within_preconditioner* p);
+uint64_t within_preconditioner_n(const within_preconditioner* p);
+/* "Additive" or "Diagonal" */
+const char* within_preconditioner_variant_name(const within_preconditioner* p);
+/* Preconditioner::apply: y = M^{-1} x on device buffers (n each). */
+int within_preconditioner_apply(const within_preconditioner* p, const double* x_dev,
+                                double* y_dev, void* stream);
+
+/* ---- diagnostics ---- */
+const char* within_last_error(void);
+/* Kernel launches issued by this library on the calling thread since the last
+ * reset (graph replays count every kernel node they run). */
+uint64_t within_launch_count(void);
+void within_launch_count_reset(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WITHIN_GPU_H */

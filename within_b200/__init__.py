@@ -1,0 +1,488 @@
+"""B200-native fixed-effects projection: the preconditioned modified-LSMR solve
+of ``D'WD x = D'W y`` from leostimpfle/within, on sm_100a.
+
+Drop-in for the ``within`` Python API (python/within/__init__.py,
+crates/within-py/src/api.rs):
+
+    import numpy as np
+    import within_b200 as within
+
+    categories = np.asfortranarray(np.column_stack([a, b]).astype(np.uint32))
+    result = within.solve(categories, y)          # SolveResult
+    solver = within.Solver(categories)            # reusable preconditioner
+    r1, r2 = solver.solve(y1), solver.solve(y2)
+    batch = solver.solve_batch(Y)                 # Y: (n_obs, k), one RHS per column
+
+Every solve runs in ``libwithin_gpu.so`` on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from . import config
+from .config import (AdditiveSchwarz, ApproxCholConfig, ApproxSchurConfig, LocalSolverConfig,
+                     ReductionStrategy, ScalingConfig, Schur)
+
+__all__ = [
+    "BatchSolveResult",
+    "CoefficientLayout",
+    "Effect",
+    "LsmrOptions",
+    "Preconditioner",
+    "PreconditionerConfig",
+    "SolveResult",
+    "Solver",
+    "UnidentifiedDirection",
+    "solve",
+    "solve_batch",
+    "config",
+]
+
+
+# ---------------------------------------------------------------------------
+# configuration objects (crates/within-py/src/config.rs)
+
+class PreconditionerConfig:
+    """Preconditioner selection shortcut: ``Additive`` (default), ``Off``, ``Diagonal``."""
+
+    __slots__ = ("kind",)
+
+    def __init__(self, kind: int):
+        self.kind = kind
+
+    def __repr__(self) -> str:
+        return "PreconditionerConfig." + {0: "Off", 1: "Additive", 2: "Diagonal"}[self.kind]
+
+    def __eq__(self, other):
+        return isinstance(other, PreconditionerConfig) and other.kind == self.kind
+
+    def __hash__(self):
+        return hash(self.kind)
+
+
+PreconditionerConfig.Off = PreconditionerConfig(_ffi.PRECOND_OFF)
+PreconditionerConfig.Additive = PreconditionerConfig(_ffi.PRECOND_ADDITIVE)
+PreconditionerConfig.Diagonal = PreconditionerConfig(_ffi.PRECOND_DIAGONAL)
+
+
+@dataclass(frozen=True)
+class LsmrOptions:
+    """LsmrOptions (crates/within/src/config.rs:159-178)."""
+
+    tol: float = 1e-8
+    maxiter: int = 1000
+    local_size: int | None = None
+
+    def _c(self) -> _ffi.LsmrOptionsC:
+        return _ffi.LsmrOptionsC(float(self.tol), int(self.maxiter), int(self.local_size or 0))
+
+
+class Effect:
+    """One term of a design: level codes, an intercept flag, slope covariates
+    (crates/within/src/domain/effect.rs:12-42)."""
+
+    __slots__ = ("levels", "intercept", "slopes")
+
+    def __init__(self, levels, intercept: bool = True, slopes=None):
+        lv = np.asarray(levels)
+        if lv.ndim != 1:
+            raise TypeError("levels must be a 1-D uint32 array")
+        if lv.dtype != np.uint32:
+            if not np.issubdtype(lv.dtype, np.integer):
+                raise TypeError(f"levels must be a 1-D uint32 array, got dtype {lv.dtype}")
+            if lv.size and lv.min() < 0:
+                raise ValueError("levels must be non-negative")
+            lv = lv.astype(np.uint32)
+        self.levels = np.ascontiguousarray(lv)
+        self.intercept = bool(intercept)
+        sl = []
+        for j, s in enumerate(slopes or []):
+            a = np.ascontiguousarray(np.asarray(s, dtype=np.float64))
+            if a.ndim != 1:
+                raise TypeError(f"slope {j} must be a 1-D float64 array")
+            if a.shape[0] != self.levels.shape[0]:
+                raise ValueError(f"slope {j} has {a.shape[0]} values, expected {self.levels.shape[0]}")
+            sl.append(a)
+        self.slopes = tuple(sl)
+        if not self.intercept and not self.slopes:
+            raise ValueError("an effect must have an intercept or at least one slope")
+
+
+@dataclass(frozen=True)
+class UnidentifiedDirection:
+    """A per-level direction the data cannot identify (term, level, column)."""
+
+    term: int
+    level: int
+    column: int
+
+    def __repr__(self) -> str:
+        return f"UnidentifiedDirection(term={self.term}, level={self.level}, column={self.column})"
+
+
+class CoefficientLayout:
+    """Flat ``x`` index <-> (term, level, column) (crates/within/src/solver.rs:125-200)."""
+
+    def __init__(self, terms: list[tuple[int, int, int]], n_dofs: int):
+        self._terms = terms  # (offset, n_levels, n_columns)
+        self._n_dofs = n_dofs
+
+    def n_dofs(self) -> int:
+        return self._n_dofs
+
+    def n_terms(self) -> int:
+        return len(self._terms)
+
+    def n_levels(self, term: int) -> int:
+        if not 0 <= term < len(self._terms):
+            raise IndexError(f"term {term} out of range")
+        return self._terms[term][1]
+
+    def n_columns(self, term: int) -> int:
+        if not 0 <= term < len(self._terms):
+            raise IndexError(f"term {term} out of range")
+        return self._terms[term][2]
+
+    def index(self, term: int, level: int, column: int) -> int:
+        if not 0 <= term < len(self._terms):
+            raise IndexError(f"term {term} out of range")
+        off, nl, nc = self._terms[term]
+        if not (0 <= level < nl and 0 <= column < nc):
+            raise IndexError(f"address ({term}, {level}, {column}) out of range")
+        return off + column * nl + level
+
+    def address(self, index: int) -> tuple[int, int, int]:
+        if not 0 <= index < self._n_dofs:
+            raise IndexError(f"index {index} out of range")
+        term = max(t for t, (off, _, _) in enumerate(self._terms) if off <= index)
+        off, nl, _ = self._terms[term]
+        within = index - off
+        return term, within % nl, within // nl
+
+
+@dataclass
+class SolveResult:
+    """Result of one solve (crates/within/src/solver.rs:205-242)."""
+
+    x: np.ndarray
+    unidentified: list
+    layout: CoefficientLayout
+    demeaned: np.ndarray
+    converged: bool
+    iterations: int
+    residual: float
+    time_total: float
+    time_setup: float
+    time_solve: float
+
+
+@dataclass
+class BatchSolveResult:
+    """Result of a batch solve (solver.rs:246-293); ``x`` is (n_dofs, k), ``demeaned`` (n_obs, k)."""
+
+    x: np.ndarray
+    unidentified: list
+    layout: CoefficientLayout
+    demeaned: np.ndarray
+    converged: list
+    iterations: list
+    residual: list
+    time_solve: list
+    time_setup: float
+    time_total: float
+
+
+class Preconditioner:
+    """Opaque handle to a built preconditioner, reusable across solvers of the
+    same design (operator/schwarz.rs:115-183).  It lives on the GPU."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _ffi.lib().within_preconditioner_free(h)
+            self._h = None
+
+    @property
+    def variant_name(self) -> str:
+        return _ffi.lib().within_preconditioner_variant_name(self._h).decode()
+
+    def nrows(self) -> int:
+        return int(_ffi.lib().within_preconditioner_n(self._h))
+
+    def ncols(self) -> int:
+        return self.nrows()
+
+    def apply_device(self, x, y, stream=None) -> None:
+        """``y = M^-1 x`` on CUDA float64 tensors of length n (Preconditioner::apply)."""
+        _ffi.check(_ffi.lib().within_preconditioner_apply(
+            self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+            None if stream is None else C.c_void_p(stream)))
+
+    def __repr__(self) -> str:
+        return f"Preconditioner({self.variant_name}, n={self.nrows()})"
+
+    def __reduce__(self):
+        raise TypeError("within_b200.Preconditioner lives in GPU memory and is not picklable")
+
+
+# ---------------------------------------------------------------------------
+# lowering helpers
+
+def _precond_config(p) -> _ffi.PrecondConfigC | None:
+    """PreconditionerInput resolution (solver.rs:62-110, within-py config.rs)."""
+    if p is None:
+        return None
+    c = _ffi.PrecondConfigC()
+    _ffi.lib().within_precond_config_default(C.byref(c))
+    if isinstance(p, PreconditionerConfig):
+        c.kind = p.kind
+        return c
+    if isinstance(p, AdditiveSchwarz):
+        c.kind = _ffi.PRECOND_ADDITIVE
+        ls = p.local_solver or LocalSolverConfig()
+        if ls.approx_chol is not None:
+            c.approx_chol_seed = ls.approx_chol.seed
+            c.approx_chol_split = ls.approx_chol.split_merge or 0
+        if ls.schur is not None:
+            c.schur_exact = 1 if ls.schur.exact_mode else 0
+            if ls.schur.config is not None:
+                c.schur_seed = ls.schur.config.seed
+                c.schur_split = ls.schur.config.split
+        if ls.dense_threshold is not None:
+            c.dense_threshold = int(ls.dense_threshold)
+        if ls.scaling is not None:
+            if ls.scaling.tolerance is not None:
+                c.scaling_tolerance = float(ls.scaling.tolerance)
+            if ls.scaling.max_sweeps is not None:
+                c.scaling_max_sweeps = int(ls.scaling.max_sweeps)
+            if ls.scaling.on_failure is not None:
+                if ls.scaling.on_failure not in ("warn", "error"):
+                    raise ValueError("ScalingConfig.on_failure must be 'warn' or 'error'")
+                c.scaling_error = 1 if ls.scaling.on_failure == "error" else 0
+        return c
+    raise TypeError(f"unsupported preconditioner argument {p!r}")
+
+
+class _Design:
+    def __init__(self, design):
+        L = _ffi.lib()
+        h = C.c_void_p()
+        if isinstance(design, np.ndarray) or hasattr(design, "__array_interface__"):
+            cats = np.asarray(design)
+            if cats.ndim != 2 or cats.dtype != np.uint32:
+                raise TypeError(f"design must be a 2-D uint32 array, got {cats.dtype} with ndim {cats.ndim}")
+            if not cats.flags.f_contiguous and cats.shape[1] > 1:
+                warnings.warn("categories array is C-ordered; an F-ordered copy is made "
+                              "(np.asfortranarray avoids it)", stacklevel=4)
+            codes = np.asfortranarray(cats)
+            self._keep = codes
+            self.n_obs = cats.shape[0]
+            _ffi.check(L.within_design_from_categories(_ffi.ptr(codes.reshape(-1, order="F")),
+                                                       cats.shape[0], cats.shape[1], C.byref(h)))
+        else:
+            effects = list(design)
+            if not effects or not all(isinstance(e, Effect) for e in effects):
+                raise TypeError("design must be a uint32 categories matrix or a list of Effect")
+            n = effects[0].levels.shape[0]
+            for e in effects:
+                if e.levels.shape[0] != n:
+                    raise ValueError("all effects must have the same number of observations")
+            lv = (C.c_void_p * len(effects))(*[e.levels.ctypes.data for e in effects])
+            icpt = np.array([1 if e.intercept else 0 for e in effects], np.int32)
+            ns = np.array([len(e.slopes) for e in effects], np.uint64)
+            sl_list = [s for e in effects for s in e.slopes]
+            sl = (C.c_void_p * max(1, len(sl_list)))(*[s.ctypes.data for s in sl_list])
+            self._keep = (effects, lv, icpt, ns, sl)
+            self.n_obs = n
+            _ffi.check(L.within_design_from_effects(n, len(effects), lv, _ffi.ptr(icpt), _ffi.ptr(ns),
+                                                    sl, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _ffi.lib().within_design_free(self.h)
+            self.h = None
+
+
+def _as_f64_1d(name, a):
+    arr = np.asarray(a)
+    if arr.ndim != 1 or arr.dtype != np.float64:
+        raise TypeError(f"{name} must be a 1-D float64 array, got dtype {arr.dtype}")
+    return np.ascontiguousarray(arr)
+
+
+def _as_f64_2d(name, a):
+    arr = np.asarray(a)
+    if arr.ndim != 2 or arr.dtype != np.float64:
+        raise TypeError(f"{name} must be a 2-D float64 array, got dtype {arr.dtype}")
+    return np.asfortranarray(arr)
+
+
+# ---------------------------------------------------------------------------
+
+class Solver:
+    """Persistent solver owning its preconditioner (crates/within/src/solver.rs:295-593)."""
+
+    def __init__(self, design, weights=None, preconditioner=None, device: int = -1):
+        L = _ffi.lib()
+        d = _Design(design)
+        w = None if weights is None else _as_f64_1d("weights", weights)
+        if w is not None and w.shape[0] != d.n_obs:
+            raise ValueError(f"weights has length {w.shape[0]}, expected {d.n_obs}")
+        prebuilt = preconditioner._h if isinstance(preconditioner, Preconditioner) else None
+        cfg = None if prebuilt is not None else _precond_config(preconditioner)
+        h = C.c_void_p()
+        _ffi.check(L.within_solver_new(d.h, _ffi.ptr(w), None if cfg is None else C.byref(cfg),
+                                       prebuilt, device, C.byref(h)))
+        self._h = h
+        self._n_obs = int(L.within_solver_n_obs(h))
+        self._n_dofs = int(L.within_solver_n_dofs(h))
+        terms = []
+        for t in range(int(L.within_solver_n_terms(h))):
+            nl, off, nc = C.c_uint64(), C.c_uint64(), C.c_uint64()
+            _ffi.check(L.within_solver_term_layout(h, t, C.byref(nl), C.byref(off), C.byref(nc)))
+            terms.append((off.value, nl.value, nc.value))
+        self._layout = CoefficientLayout(terms, self._n_dofs)
+        cap = 1 << 16
+        buf = np.zeros(3 * cap, np.uint64)
+        k = int(L.within_solver_unidentified(h, _ffi.ptr(buf), cap))
+        self._unidentified = [UnidentifiedDirection(int(buf[3 * i]), int(buf[3 * i + 1]), int(buf[3 * i + 2]))
+                              for i in range(min(k, cap))]
+        nw = int(L.within_solver_n_warnings(h))
+        for _ in range(nw):
+            warnings.warn("signed component: dominance scaling uncertified; deficits clamped, "
+                          "preconditioner quality may degrade", UserWarning, stacklevel=2)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _ffi.lib().within_solver_free(h)
+            self._h = None
+
+    @property
+    def n_dofs(self) -> int:
+        return self._n_dofs
+
+    @property
+    def n_obs(self) -> int:
+        return self._n_obs
+
+    @property
+    def layout(self) -> CoefficientLayout:
+        return self._layout
+
+    @property
+    def preconditioner(self) -> Preconditioner | None:
+        h = _ffi.lib().within_solver_preconditioner(self._h)
+        return Preconditioner(C.c_void_p(h)) if h else None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def obs_perm(self) -> np.ndarray | None:
+        out = np.zeros(self._n_obs, np.uint32)
+        return out if _ffi.lib().within_solver_obs_perm(self._h, _ffi.ptr(out)) else None
+
+    def solve(self, y, options: LsmrOptions | None = None) -> SolveResult:
+        y = _as_f64_1d("y", y)
+        if y.shape[0] != self._n_obs:
+            raise ValueError(f"response vector length ({y.shape[0]}) does not match number of "
+                             f"observations ({self._n_obs})")
+        x = np.zeros(self._n_dofs)
+        dm = np.zeros(self._n_obs)
+        st = _ffi.SolveStatsC()
+        opts = (options or LsmrOptions())._c()
+        _ffi.check(_ffi.lib().within_solver_solve(self._h, _ffi.ptr(y), C.byref(opts), _ffi.ptr(x),
+                                                  _ffi.ptr(dm), C.byref(st)))
+        return SolveResult(x, list(self._unidentified), self._layout, dm, bool(st.converged),
+                           int(st.iterations), float(st.residual), st.time_total, st.time_setup,
+                           st.time_solve)
+
+    def solve_batch(self, Y, options: LsmrOptions | None = None) -> BatchSolveResult:
+        Y = _as_f64_2d("Y", Y)
+        if Y.shape[0] != self._n_obs:
+            raise ValueError(f"Y has {Y.shape[0]} rows but solver has {self._n_obs} observations")
+        k = Y.shape[1]
+        X = np.zeros((self._n_dofs, k), order="F")
+        D = np.zeros((self._n_obs, k), order="F")
+        st = (_ffi.SolveStatsC * max(1, k))()
+        opts = (options or LsmrOptions())._c()
+        if k:
+            _ffi.check(_ffi.lib().within_solver_solve_batch(self._h, _ffi.ptr(Y), k, C.byref(opts),
+                                                            _ffi.ptr(X), _ffi.ptr(D), st))
+        return BatchSolveResult(X, list(self._unidentified), self._layout, D,
+                                [bool(st[i].converged) for i in range(k)],
+                                [int(st[i].iterations) for i in range(k)],
+                                [float(st[i].residual) for i in range(k)],
+                                [st[i].time_solve for i in range(k)], 0.0,
+                                max([st[i].time_total for i in range(k)] or [0.0]))
+
+    def solve_device(self, Y, options: LsmrOptions | None = None, X=None, D=None, stream=None):
+        """Device-resident solve_batch on CUDA float64 tensors (column-major (n_obs, k)
+        storage: pass ``Y.t().contiguous().t()`` or a 1-D tensor for k = 1)."""
+        import torch
+        if Y.dtype != torch.float64 or not Y.is_cuda:
+            raise TypeError("Y must be a CUDA float64 tensor")
+        k = 1 if Y.dim() == 1 else Y.shape[1]
+        if X is None:
+            X = torch.empty((k, self._n_dofs), dtype=torch.float64, device=Y.device).t()
+        if D is None:
+            D = torch.empty((k, self._n_obs), dtype=torch.float64, device=Y.device).t()
+        st = (_ffi.SolveStatsC * k)()
+        opts = (options or LsmrOptions())._c()
+        if stream is None:
+            stream = torch.cuda.current_stream(Y.device).cuda_stream
+        _ffi.check(_ffi.lib().within_solver_solve_batch_device(
+            self._h, C.c_void_p(Y.data_ptr()), k, C.byref(opts), C.c_void_p(X.data_ptr()),
+            C.c_void_p(D.data_ptr()), st, C.c_void_p(stream)))
+        stats = [(bool(st[i].converged), int(st[i].iterations), float(st[i].residual)) for i in range(k)]
+        return X, D, stats
+
+    # Operator trait plumbing (internal observation order, device buffers)
+    def operator_apply_device(self, x, y, stream=None) -> None:
+        _ffi.check(_ffi.lib().within_solver_operator_apply(
+            self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+            None if stream is None else C.c_void_p(stream)))
+
+    def operator_apply_adjoint_device(self, u, y, stream=None) -> None:
+        _ffi.check(_ffi.lib().within_solver_operator_apply_adjoint(
+            self._h, C.c_void_p(u.data_ptr()), C.c_void_p(y.data_ptr()),
+            None if stream is None else C.c_void_p(stream)))
+
+
+def solve(design, y, weights=None, options: LsmrOptions | None = None, preconditioner=None) -> SolveResult:
+    """One-shot ``Solver(design, weights, preconditioner).solve(y, options)``
+    (crates/within/src/solver.rs:611-626)."""
+    import time
+    t0 = time.perf_counter()
+    s = Solver(design, weights, preconditioner)
+    t1 = time.perf_counter()
+    r = s.solve(y, options)
+    r.time_setup += t1 - t0
+    r.time_total = time.perf_counter() - t0
+    return r
+
+
+def solve_batch(design, Y, weights=None, options: LsmrOptions | None = None,
+                preconditioner=None) -> BatchSolveResult:
+    """One-shot batch solve (solver.rs:632-646)."""
+    import time
+    t0 = time.perf_counter()
+    s = Solver(design, weights, preconditioner)
+    t1 = time.perf_counter()
+    Ya = np.asarray(Y)
+    if Ya.ndim == 2 and Ya.shape[0] != s.n_obs:
+        raise ValueError(f"Y has {Ya.shape[0]} rows but the design has {s.n_obs} observations")
+    r = s.solve_batch(Y, options)
+    r.time_setup = t1 - t0
+    r.time_total = time.perf_counter() - t0
+    return r

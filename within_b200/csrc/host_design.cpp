@@ -1,0 +1,293 @@
+// host_design.cpp -- design lowering, locality sort, slope reparametrisation
+// and segmented-reduction tile plans (host side, once per Solver).
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+
+#include "host.hpp"
+
+namespace wgpu {
+
+// Stable argsort of observations by level (crates/within/src/domain.rs:110-140).
+// The reference switches between a counting sort and a stable comparison sort
+// on n_obs < n_levels; both give the same permutation, which is all that is
+// observable, so the counting sort runs whenever its bucket array is small.
+void stable_argsort_u32(const uint32_t* key, size_t n, size_t n_levels, uint32_t* perm) {
+    if (n < n_levels && n_levels > (size_t)1 << 26) {
+        for (size_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+        std::stable_sort(perm, perm + n, [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+        return;
+    }
+    std::vector<uint64_t> cur(n_levels + 1, 0);
+    for (size_t i = 0; i < n; ++i) ++cur[(size_t)key[i] + 1];
+    for (size_t l = 0; l < n_levels; ++l) cur[l + 1] += cur[l];
+    for (size_t i = 0; i < n; ++i) perm[cur[key[i]]++] = (uint32_t)i;
+}
+
+// Design::new / Design::build (domain.rs:155-247) with Effect::new validation
+// (effect.rs:12-42): term-major layout, n_levels = max code + 1, sortedness
+// flags, and the locality sort by the dominant term -- the last term holding
+// the most DOFs (Rust's max_by_key tie rule), applied when it is unsorted.
+HostDesign make_design(uint64_t n_obs, const std::vector<EffectIn>& effects) {
+    HostDesign d;
+    if (effects.size() > (size_t)MAX_TERMS)
+        throw WError(ERR_UNSUPPORTED, "at most " + std::to_string(MAX_TERMS) + " effects are supported");
+    for (size_t e = 0; e < effects.size(); ++e) {
+        const EffectIn& ef = effects[e];
+        Term t;
+        if (ef.intercept) t.cols.push_back(-1);
+        for (size_t s = 0; s < ef.slopes.size(); ++s) {
+            const double* z = ef.slopes[s];
+            for (uint64_t i = 0; i < n_obs; ++i)
+                if (!std::isfinite(z[i]))
+                    throw WError(ERR_BUILD, "slope " + std::to_string(s) + " loading at index " +
+                                                std::to_string(i) + " must be finite, got " +
+                                                std::to_string(z[i]));
+            d.loads.emplace_back(z, z + n_obs);
+            t.cols.push_back((int)d.loads.size() - 1);
+        }
+        if (t.cols.empty()) throw WError(ERR_BUILD, "an effect must have an intercept or at least one slope");
+        if (t.cols.size() > (size_t)MAX_COLS)
+            throw WError(ERR_UNSUPPORTED, "at most " + std::to_string(MAX_COLS - 1) + " slopes per effect are supported");
+        d.terms.push_back(t);
+        d.codes.emplace_back(ef.levels, ef.levels + n_obs);
+    }
+    if (d.loads.size() > (size_t)MAX_LOADS)
+        throw WError(ERR_UNSUPPORTED, "at most " + std::to_string(MAX_LOADS) + " slope columns are supported");
+    if (n_obs == 0) throw WError(ERR_BUILD, "no observations provided");
+    if (n_obs > (uint64_t)std::numeric_limits<uint32_t>::max())
+        throw WError(ERR_UNSUPPORTED, "more than 2^32-1 observations in one design");
+    d.n_obs = n_obs;
+    uint64_t offset = 0;
+    for (size_t q = 0; q < d.terms.size(); ++q) {
+        uint32_t mx = 0, prev = 0;
+        bool sorted = true;
+        for (uint32_t v : d.codes[q]) {
+            mx = std::max(mx, v);
+            sorted = sorted && v >= prev;
+            prev = v;
+        }
+        Term& t = d.terms[q];
+        uint64_t nl = (uint64_t)mx + 1;
+        t.sorted = sorted;
+        t.offset = (uint32_t)std::min<uint64_t>(offset, std::numeric_limits<uint32_t>::max());
+        offset += nl * t.cols.size();
+        t.n_levels = (uint32_t)std::min<uint64_t>(nl, std::numeric_limits<uint32_t>::max());
+    }
+    if (offset > (uint64_t)std::numeric_limits<uint32_t>::max())
+        throw WError(ERR_BUILD, "design has " + std::to_string(offset) +
+                                    " degrees of freedom, exceeding the u32 column-index limit");
+    d.n_dofs = offset;
+    if (!d.terms.empty()) {
+        size_t dom = 0;
+        for (size_t q = 1; q < d.terms.size(); ++q)
+            if (d.terms[q].n_dofs() >= d.terms[dom].n_dofs()) dom = q;
+        if (!d.terms[dom].sorted) {
+            d.obs_perm.resize(n_obs);
+            stable_argsort_u32(d.codes[dom].data(), n_obs, d.terms[dom].n_levels, d.obs_perm.data());
+            std::vector<uint32_t> tmp(n_obs);
+            for (auto& col : d.codes) {
+                for (uint64_t i = 0; i < n_obs; ++i) tmp[i] = col[d.obs_perm[i]];
+                col.swap(tmp);
+            }
+            std::vector<double> tz(n_obs);
+            for (auto& col : d.loads) {
+                for (uint64_t i = 0; i < n_obs; ++i) tz[i] = col[d.obs_perm[i]];
+                col.swap(tz);
+            }
+            for (size_t q = 0; q < d.terms.size(); ++q)
+                d.terms[q].sorted = std::is_sorted(d.codes[q].begin(), d.codes[q].end());
+        }
+    }
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+// Slope reparametrisation (crates/within/src/solver/reparam.rs:48-316): per
+// level, weighted Welford moments of the slope covariates, a pivoted
+// Gram-Schmidt in the coordinates of the level Gram (RANK_TOL = 1e-10), and
+// the loading columns overwritten by the whitened u = W (z - center).
+
+namespace {
+constexpr double RANK_TOL = 1e-10;
+inline size_t tri(size_t j, size_t k) { return j * (j + 1) / 2 + k; }
+
+void pivoted_gs(const std::vector<double>& g, size_t v, std::vector<double>& basis,
+                std::vector<char>& kept) {
+    std::vector<double> res(v);
+    for (size_t j = 0; j < v; ++j) res[j] = g[j * v + j];
+    kept.assign(v, 0);
+    basis.clear();
+    for (;;) {
+        long p = -1;
+        for (size_t j = 0; j < v; ++j) {
+            if (kept[j] || !std::isfinite(res[j]) || !(res[j] > RANK_TOL * g[j * v + j])) continue;
+            if (p < 0 || !(res[j] < res[p])) p = (long)j;
+        }
+        if (p < 0) return;
+        kept[p] = 1;
+        std::vector<double> q(v, 0.0);
+        q[p] = 1.0;
+        for (size_t b = 0; b < basis.size(); b += v) {
+            double c = 0;
+            for (size_t j = 0; j < v; ++j) c += g[p * v + j] * basis[b + j];
+            for (size_t j = 0; j < v; ++j) q[j] -= c * basis[b + j];
+        }
+        double nrm = std::sqrt(res[p]);
+        for (double& x : q) x /= nrm;
+        for (size_t j = 0; j < v; ++j) {
+            double c = 0;
+            for (size_t i = 0; i < v; ++i) c += g[j * v + i] * q[i];
+            res[j] -= c * c;
+        }
+        basis.insert(basis.end(), q.begin(), q.end());
+    }
+}
+}  // namespace
+
+Reparam build_reparam(HostDesign& d, const double* w) {
+    Reparam out;
+    for (size_t term = 0; term < d.terms.size(); ++term) {
+        const Term& t = d.terms[term];
+        std::vector<uint32_t> zc;
+        Reparam::TermR tr;
+        tr.offset = t.offset;
+        tr.n_levels = t.n_levels;
+        for (size_t c = 0; c < t.cols.size(); ++c) {
+            if (t.cols[c] < 0) {
+                tr.intercept_col = (int)c;
+            } else {
+                tr.slope_cols.push_back((uint32_t)c);
+                zc.push_back((uint32_t)t.cols[c]);
+            }
+        }
+        if (zc.empty()) continue;
+        const bool icpt = tr.intercept_col >= 0;
+        const size_t v = zc.size(), L = t.n_levels, tl = v * (v + 1) / 2;
+        const uint32_t* lev = d.codes[term].data();
+        std::vector<double> wsum(L, 0.0), mean(L * v, 0.0), com(L * tl, 0.0), delta(v), z(v);
+        for (uint64_t i = 0; i < d.n_obs; ++i) {
+            double wi = w ? w[i] : 1.0;
+            if (wi <= 0.0) continue;
+            size_t l = lev[i];
+            for (size_t j = 0; j < v; ++j) z[j] = d.loads[zc[j]][i];
+            wsum[l] += wi;
+            double ratio = wi / wsum[l];
+            double* mu = &mean[l * v];
+            for (size_t j = 0; j < v; ++j) {
+                delta[j] = z[j] - mu[j];
+                mu[j] += ratio * delta[j];
+            }
+            double* cm = &com[l * tl];
+            for (size_t j = 0; j < v; ++j) {
+                double dev = wi * (z[j] - mu[j]);
+                for (size_t k = 0; k <= j; ++k) cm[tri(j, k)] += delta[k] * dev;
+            }
+        }
+        tr.w.resize(L);
+        tr.center.resize(L);
+        std::vector<double> g(v * v), basis;
+        std::vector<char> kept;
+        for (size_t l = 0; l < L; ++l) {
+            const double* cm = &com[l * tl];
+            const double* mu = &mean[l * v];
+            for (size_t j = 0; j < v; ++j)
+                for (size_t k = 0; k <= j; ++k) {
+                    double gv = cm[tri(j, k)];
+                    if (!icpt) gv += wsum[l] * mu[j] * mu[k];
+                    g[j * v + k] = gv;
+                    g[k * v + j] = gv;
+                }
+            pivoted_gs(g, v, basis, kept);
+            if (icpt && wsum[l] == 0.0) {
+                out.unidentified.insert(out.unidentified.end(), {term, l, 0});
+            }
+            for (size_t j = 0; j < v; ++j)
+                if (!kept[j]) out.unidentified.insert(out.unidentified.end(), {term, l, tr.slope_cols[j]});
+            tr.w[l] = basis;
+            if (icpt) tr.center[l].assign(mu, mu + v);
+            else tr.center[l].assign(v, 0.0);
+        }
+        std::vector<std::vector<double>> u(v, std::vector<double>(d.n_obs, 0.0));
+        for (uint64_t i = 0; i < d.n_obs; ++i) {
+            size_t l = lev[i];
+            const auto& wl = tr.w[l];
+            const auto& cl = tr.center[l];
+            for (size_t j = 0; j < v; ++j) z[j] = d.loads[zc[j]][i] - cl[j];
+            for (size_t r = 0; r * v < wl.size(); ++r) {
+                double s = 0;
+                for (size_t j = 0; j < v; ++j) s += wl[r * v + j] * z[j];
+                u[r][i] = s;
+            }
+        }
+        for (size_t j = 0; j < v; ++j) d.loads[zc[j]].swap(u[j]);
+        out.terms.push_back(std::move(tr));
+    }
+    return out;
+}
+
+// reparam.rs:173-194
+void Reparam::back_transform(double* x) const {
+    for (const auto& t : terms) {
+        const size_t v = t.slope_cols.size();
+        std::vector<double> b(v);
+        for (size_t l = 0; l < t.w.size(); ++l) {
+            const auto& wl = t.w[l];
+            if (wl.empty()) continue;
+            std::fill(b.begin(), b.end(), 0.0);
+            for (size_t k = 0; k * v < wl.size(); ++k) {
+                double bk = x[t.offset + (size_t)t.slope_cols[k] * t.n_levels + l];
+                for (size_t j = 0; j < v; ++j) b[j] += wl[k * v + j] * bk;
+            }
+            for (size_t j = 0; j < v; ++j) x[t.offset + (size_t)t.slope_cols[j] * t.n_levels + l] = b[j];
+            if (t.intercept_col >= 0) {
+                double s = 0;
+                for (size_t j = 0; j < v; ++j) s += b[j] * t.center[l][j];
+                x[t.offset + (size_t)t.intercept_col * t.n_levels + l] -= s;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tile plan of one segmented-reduction problem (see segreduce.cuh).
+void HostPlan::add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, int T) {
+    // positions of this problem are [ptr[0], ptr[n_seg]); tiles start at ptr[0]
+    const uint32_t pbase = ptr[0];
+    const uint32_t npos = ptr[n_seg] - pbase;
+    const uint32_t nt = npos == 0 ? 1u : (npos + (uint32_t)T - 1) / (uint32_t)T;
+    const uint32_t base = (uint32_t)tiles.size();
+    for (uint32_t lt = 0; lt < nt; ++lt) {
+        SRTile t{};
+        t.problem = problem;
+        t.p0 = pbase + lt * (uint32_t)T;
+        t.p1 = pbase + (uint32_t)std::min<uint64_t>((uint64_t)lt * (uint32_t)T + (uint32_t)T, npos);
+        t.own_lo = t.own_hi = 0;
+        t.cont_split = -1;
+        t.tail_split = -1;
+        tiles.push_back(t);
+    }
+    // owned ranges: segment s belongs to the tile holding its first position
+    // (segments starting at the end of the range belong to the last tile).
+    uint32_t s = 0;
+    for (uint32_t lt = 0; lt < nt; ++lt) {
+        SRTile& t = tiles[base + lt];
+        t.own_lo = s;
+        bool last = lt + 1 == nt;
+        while (s < n_seg && (last || ptr[s] < t.p1)) ++s;
+        t.own_hi = s;
+    }
+    for (uint32_t g = 0; g < n_seg; ++g) {
+        uint32_t a = ptr[g] - pbase, b = ptr[g + 1] - pbase;
+        if (b <= a) continue;
+        uint32_t t0 = a / (uint32_t)T, t1 = (b - 1) / (uint32_t)T;
+        if (t1 == t0) continue;
+        int id = (int)splits.size();
+        splits.push_back(SRSplit{problem, g, base + t0, base + t1});
+        tiles[base + t0].tail_split = id;
+        for (uint32_t t = t0 + 1; t <= t1; ++t) tiles[base + t].cont_split = id;
+    }
+}
+
+}  // namespace wgpu

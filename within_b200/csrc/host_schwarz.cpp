@@ -1,0 +1,973 @@
+// host_schwarz.cpp -- construction of the Diagonal and additive-Schwarz
+// preconditioners (once per Solver, host side), packed for the GPU apply.
+//
+// Construction follows the reference's steps (crates/within/src/domain/
+// {cross_tab,factor_pairs}*, block_elim/*, operator/schwarz.rs):
+//   channel pairs -> weighted cross-tab C of active levels -> bipartite
+//   connected components -> orient (eliminate the larger block) -> SDDM form
+//   (known Laplacian, or signed/scaled General with a Gremban cover when
+//   frustrated) -> partition-of-unity weights -> reduced system
+//   D_k - C^T D_e^-1 C (exact for small kept blocks, clique-tree sampled
+//   otherwise) as an explicit Laplacian.
+// The reduced Laplacian is then factored for the GPU:
+//   * n <= DENSE_MAX: dense LDL^T with a pseudo-inverse pivot, stored as the
+//     dense generalised inverse (one batched mat-vec per apply).  For the
+//     reference's exact route (n_kept <= dense_threshold) this is the same
+//     operator the reference applies.
+//   * otherwise: approximate Cholesky (Gao-Kyng-Spielman clique-tree sampling,
+//     arXiv:2303.00709) whose elimination proceeds in rounds of independent
+//     vertices.  Vertices of one round share no edge, so their columns are
+//     computed from the same graph and the triangular solves run one round
+//     per parallel step (level scheduling by construction).
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <numeric>
+
+#include "host.hpp"
+
+namespace wgpu {
+namespace {
+
+constexpr uint32_t DENSE_MAX = 64;
+
+struct Csr {
+    std::vector<uint32_t> ptr{0}, col;
+    std::vector<double> val;
+    uint32_t nr = 0, nc = 0;
+    uint32_t nnz() const { return (uint32_t)val.size(); }
+};
+
+Csr transpose(const Csr& a) {
+    Csr t;
+    t.nr = a.nc;
+    t.nc = a.nr;
+    t.ptr.assign(a.nc + 1, 0);
+    for (uint32_t c : a.col) ++t.ptr[c + 1];
+    for (uint32_t i = 0; i < a.nc; ++i) t.ptr[i + 1] += t.ptr[i];
+    std::vector<uint32_t> cur(t.ptr.begin(), t.ptr.end() - 1);
+    t.col.resize(a.nnz());
+    t.val.resize(a.nnz());
+    for (uint32_t r = 0; r < a.nr; ++r)
+        for (uint32_t k = a.ptr[r]; k < a.ptr[r + 1]; ++k) {
+            uint32_t p = cur[a.col[k]]++;
+            t.col[p] = r;
+            t.val[p] = a.val[k];
+        }
+    return t;
+}
+
+struct Bip {  // C (rows = first block) and C^T
+    Csr c, ct;
+    uint32_t nr() const { return c.nr; }
+    uint32_t nc() const { return c.nc; }
+    uint32_t nl() const { return c.nr + c.nc; }
+    template <class F>
+    void nb(uint32_t i, F f) const {
+        if (i < c.nr) {
+            for (uint32_t k = c.ptr[i]; k < c.ptr[i + 1]; ++k) f(c.nr + c.col[k], c.val[k]);
+        } else {
+            uint32_t r = i - c.nr;
+            for (uint32_t k = ct.ptr[r]; k < ct.ptr[r + 1]; ++k) f(ct.col[k], ct.val[k]);
+        }
+    }
+};
+
+double neumaier(const double* v, size_t n) {
+    double s = 0, c = 0;
+    for (size_t i = 0; i < n; ++i) {
+        double t = s + v[i];
+        c += std::fabs(s) >= std::fabs(v[i]) ? (s - t) + v[i] : (v[i] - t) + s;
+        s = t;
+    }
+    return s + c;
+}
+
+// ---- SDDM conversion (domain/factor_pairs/sddm.rs) ----
+struct Comp {
+    Bip m;
+    std::vector<double> diag, ground;
+    bool grounded = false;
+    bool laplacian = true;      // false: signed, needs the Gremban cover
+    std::vector<double> factors;  // empty: canonical (negate kept block)
+};
+
+double budget(double ulps, size_t n, double total) {
+    return ulps * DBL_EPSILON * std::sqrt((double)std::max<size_t>(n, 1)) * total;
+}
+
+std::vector<double> sums(const Bip& m, bool mag) {
+    std::vector<double> s(m.nl());
+    for (uint32_t i = 0; i < m.nl(); ++i) {
+        double a = 0;
+        m.nb(i, [&](uint32_t, double v) { a += mag ? std::fabs(v) : v; });
+        s[i] = a;
+    }
+    return s;
+}
+
+bool finalize(Comp& c, std::vector<double> sd, const std::vector<double>& rs, const PrecondCfg& cfg,
+              double& clamped) {
+    size_t n = sd.size();
+    std::vector<double> g(n, 0.0);
+    double td = 0, ts = 0;
+    clamped = 0;
+    for (size_t i = 0; i < n; ++i) {
+        double& d = sd[i];
+        if (!std::isfinite(d) || d <= 0.0) return false;
+        double deficit = (rs[i] - d) / d;
+        if (deficit > cfg.scaling_tol) {
+            if (cfg.scaling_error) return false;
+            clamped = std::max(clamped, deficit);
+        }
+        d = std::max(d, rs[i]);
+        g[i] = std::max(d - rs[i], 0.0);
+        td += d;
+        ts += g[i];
+    }
+    bool floats = ts <= budget(4.0, n, td);
+    if (floats) {
+        sd = rs;
+        std::fill(g.begin(), g.end(), 0.0);
+    }
+    c.diag = std::move(sd);
+    c.ground = std::move(g);
+    c.grounded = !floats;
+    return true;
+}
+
+bool convert_general(Comp& c, const std::vector<double>& diag, const PrecondCfg& cfg, bool& warn) {
+    const uint32_t n = c.m.nl(), nr = c.m.nr();
+    // folding signs: a bipartite signature making every off-diagonal <= 0
+    std::vector<double> sg(n, 0.0);
+    bool has_sg = true;
+    std::vector<uint32_t> st;
+    for (uint32_t r = 0; r < n && has_sg; ++r) {
+        if (sg[r] != 0.0) continue;
+        sg[r] = 1.0;
+        st.push_back(r);
+        while (!st.empty() && has_sg) {
+            uint32_t i = st.back();
+            st.pop_back();
+            c.m.nb(i, [&](uint32_t j, double v) {
+                double e = -sg[i] * (std::signbit(v) ? -1.0 : 1.0);
+                if (sg[j] == 0.0) {
+                    sg[j] = e;
+                    st.push_back(j);
+                } else if (sg[j] != e) {
+                    has_sg = false;
+                }
+            });
+        }
+    }
+    // dominance scaling (sddm.rs:416-483)
+    for (double d : diag)
+        if (!std::isfinite(d) || d <= 0.0) return false;
+    std::vector<double> scales(n, 1.0);
+    double violation = 0.0;
+    bool dom = true;
+    for (uint32_t i = 0; i < n && dom; ++i) {
+        double rs = 0;
+        c.m.nb(i, [&](uint32_t, double v) { rs += std::fabs(v); });
+        dom = rs <= diag[i] * (1.0 + cfg.scaling_tol);
+    }
+    if (!dom) {
+        std::vector<double> is(n), mu(n, 1.0);
+        for (uint32_t i = 0; i < n; ++i) is[i] = 1.0 / std::sqrt(diag[i]);
+        auto target = [&](uint32_t i) {
+            double t = 0;
+            c.m.nb(i, [&](uint32_t j, double v) { t += std::fabs(v) * is[i] * is[j] * mu[j]; });
+            return t;
+        };
+        auto viol = [&]() {
+            double m = 0;
+            for (uint32_t i = 0; i < n; ++i) m = std::fmax(m, target(i) / mu[i] - 1.0);
+            return m;
+        };
+        violation = viol();
+        uint64_t sweeps = 0;
+        while (violation > cfg.scaling_tol && sweeps < cfg.scaling_max_sweeps) {
+            for (uint32_t i = 0; i < n; ++i) {
+                double t = target(i);
+                if (t > mu[i]) mu[i] = t;
+            }
+            double pk = 0;
+            for (double v : mu) pk = std::fmax(pk, v);
+            if (!std::isfinite(pk)) return false;
+            for (double& v : mu) v /= pk;
+            violation = viol();
+            ++sweeps;
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            scales[i] = mu[i] * is[i];
+            if (!(std::isfinite(scales[i]) && scales[i] > 0.0)) return false;
+        }
+        violation = std::max(violation, 0.0);
+    }
+    if (violation > cfg.scaling_tol && cfg.scaling_error) return false;
+    std::vector<double> f(n);
+    if (has_sg) {
+        for (uint32_t i = 0; i < n; ++i) f[i] = sg[i] * scales[i];
+    } else {
+        for (uint32_t i = 0; i < n; ++i) f[i] = i < nr ? scales[i] : -scales[i];
+    }
+    // assemble (sddm.rs:237-291)
+    for (uint32_t i = 0; i < nr; ++i)
+        for (uint32_t k = c.m.c.ptr[i]; k < c.m.c.ptr[i + 1]; ++k) {
+            double fo = -f[i] * f[nr + c.m.c.col[k]] * c.m.c.val[k];
+            if (!std::isfinite(fo) || (has_sg && fo < 0.0)) return false;
+            c.m.c.val[k] = fo;
+        }
+    c.m.ct = transpose(c.m.c);
+    std::vector<double> sd(n);
+    for (uint32_t i = 0; i < n; ++i) sd[i] = diag[i] * f[i] * f[i];
+    bool canonical = true;
+    for (uint32_t i = 0; i < n; ++i) canonical = canonical && f[i] == (i < nr ? 1.0 : -1.0);
+    c.laplacian = has_sg;
+    c.factors = canonical ? std::vector<double>() : f;
+    double clamped = 0;
+    if (!finalize(c, sd, sums(c.m, true), cfg, clamped)) return false;
+    warn = std::max(violation, clamped) > cfg.scaling_tol;
+    return true;
+}
+
+// ---- reduced Laplacians (block_elim/schur.rs) ----
+struct Lap {  // symmetric CSR with explicit diagonal
+    uint32_t n = 0;
+    std::vector<uint32_t> ptr{0}, col;
+    std::vector<double> val;
+};
+
+Lap exact_reduced(const Comp& c, const std::vector<double>& inv_e) {
+    const uint32_t ne = c.m.nr(), nk = c.m.nc();
+    std::vector<double> surplus(nk, 0.0);
+    if (c.grounded) {
+        for (uint32_t i = 0; i < nk; ++i) {
+            double acc = c.ground[ne + i];
+            for (uint32_t a = c.m.ct.ptr[i]; a < c.m.ct.ptr[i + 1]; ++a)
+                acc += c.m.ct.val[a] * (inv_e[c.m.ct.col[a]] * c.ground[c.m.ct.col[a]]);
+            surplus[i] = acc;
+        }
+    }
+    Lap L;
+    L.n = nk + (c.grounded ? 1 : 0);
+    std::vector<double> work(nk, 0.0);
+    std::vector<uint32_t> touched;
+    for (uint32_t i = 0; i < nk; ++i) {
+        work[i] = c.diag[ne + i];
+        touched.push_back(i);
+        for (uint32_t a = c.m.ct.ptr[i]; a < c.m.ct.ptr[i + 1]; ++a) {
+            uint32_t k = c.m.ct.col[a];
+            double w = c.m.ct.val[a], inv = inv_e[k];
+            for (uint32_t b = c.m.c.ptr[k]; b < c.m.c.ptr[k + 1]; ++b) {
+                uint32_t j = c.m.c.col[b];
+                if (work[j] == 0.0 && j != i) touched.push_back(j);
+                work[j] -= (w * c.m.c.val[b]) * inv;
+            }
+        }
+        std::sort(touched.begin(), touched.end());
+        touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+        double adjacency = 0;
+        size_t dpos = 0;
+        for (uint32_t j : touched) {
+            double v = work[j];
+            work[j] = 0.0;
+            if (j == i) {
+                dpos = L.col.size();
+                L.col.push_back(j);
+                L.val.push_back(0.0);
+            } else if (v != 0.0) {
+                adjacency -= v;
+                L.col.push_back(j);
+                L.val.push_back(v);
+            }
+        }
+        L.val[dpos] = adjacency + surplus[i];
+        if (c.grounded && surplus[i] > 0.0) {
+            L.col.push_back(nk);
+            L.val.push_back(-surplus[i]);
+        }
+        L.ptr.push_back((uint32_t)L.col.size());
+        touched.clear();
+    }
+    if (c.grounded) {
+        for (uint32_t i = 0; i < nk; ++i)
+            if (surplus[i] > 0.0) {
+                L.col.push_back(i);
+                L.val.push_back(-surplus[i]);
+            }
+        L.col.push_back(nk);
+        L.val.push_back(neumaier(surplus.data(), surplus.size()));
+        L.ptr.push_back((uint32_t)L.col.size());
+    }
+    return L;
+}
+
+uint64_t mix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+struct Rng {
+    uint64_t s;
+    double unit() { s = mix64(s); return (double)(s >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+struct Edge { uint32_t lo, hi; double w; };
+
+// Clique-tree sample of one star (GKS): neighbours ascending by weight, each
+// linked to a later one drawn in proportion to weight, weight w_i S_i / d.
+// `split` > 1 first splits every neighbour edge into that many equal copies.
+void sample_star(std::vector<std::pair<uint32_t, double>>& e, uint32_t split, Rng& rng,
+                 std::vector<Edge>& out) {
+    if (split > 1) {
+        std::vector<std::pair<uint32_t, double>> s;
+        s.reserve(e.size() * split);
+        for (auto& x : e)
+            for (uint32_t k = 0; k < split; ++k) s.push_back({x.first, x.second / split});
+        e.swap(s);
+    }
+    if (e.size() <= 1) return;
+    std::sort(e.begin(), e.end(), [](const std::pair<uint32_t, double>& a, const std::pair<uint32_t, double>& b) {
+        return a.second != b.second ? a.second < b.second : a.first < b.first;
+    });
+    const size_t m = e.size();
+    std::vector<double> pre(m + 1, 0.0);
+    for (size_t i = 0; i < m; ++i) pre[i + 1] = pre[i] + e[i].second;
+    const double d = pre[m];
+    for (size_t i = 0; i + 1 < m; ++i) {
+        double S = d - pre[i + 1];
+        if (!(S > 0.0)) continue;
+        double tgt = pre[i + 1] + rng.unit() * S;
+        size_t j = (size_t)(std::upper_bound(pre.begin() + i + 2, pre.end(), tgt) - pre.begin()) - 1;
+        j = std::min(std::max(j, i + 1), m - 1);
+        if (e[i].first == e[j].first) continue;
+        out.push_back({std::min(e[i].first, e[j].first), std::max(e[i].first, e[j].first),
+                       e[i].second * S / d});
+    }
+}
+
+Lap lap_from_edges(std::vector<Edge>& edges, uint32_t n) {
+    std::sort(edges.begin(), edges.end(), [](const Edge& a, const Edge& b) {
+        if (a.lo != b.lo) return a.lo < b.lo;
+        if (a.hi != b.hi) return a.hi < b.hi;
+        return a.w < b.w;
+    });
+    std::vector<Edge> dd;
+    for (auto& e : edges) {
+        if (!dd.empty() && dd.back().lo == e.lo && dd.back().hi == e.hi) dd.back().w += e.w;
+        else dd.push_back(e);
+    }
+    std::vector<std::vector<std::pair<uint32_t, double>>> rows(n);
+    std::vector<double> diag(n, 0.0);
+    for (auto& e : dd) {
+        rows[e.lo].push_back({e.hi, -e.w});
+        rows[e.hi].push_back({e.lo, -e.w});
+        diag[e.lo] += e.w;
+        diag[e.hi] += e.w;
+    }
+    Lap L;
+    L.n = n;
+    for (uint32_t i = 0; i < n; ++i) {
+        rows[i].push_back({i, diag[i]});
+        std::sort(rows[i].begin(), rows[i].end());
+        for (auto& p : rows[i]) {
+            L.col.push_back(p.first);
+            L.val.push_back(p.second);
+        }
+        L.ptr.push_back((uint32_t)L.col.size());
+    }
+    return L;
+}
+
+Lap sampled_reduced(const Comp& c, uint64_t seed, uint32_t split) {
+    const uint32_t ne = c.m.nr(), nk = c.m.nc();
+    std::vector<Edge> edges;
+    std::vector<std::pair<uint32_t, double>> ent;
+    for (uint32_t k = 0; k < ne; ++k) {
+        ent.clear();
+        for (uint32_t a = c.m.c.ptr[k]; a < c.m.c.ptr[k + 1]; ++a) ent.push_back({c.m.c.col[a], c.m.c.val[a]});
+        if (ent.empty()) continue;
+        if (c.grounded && c.ground[k] > 0.0) ent.push_back({nk, c.ground[k]});
+        if (ent.size() <= 1) continue;
+        Rng r{mix64(seed * 0x100000001B3ull + k)};
+        sample_star(ent, split, r, edges);
+    }
+    if (c.grounded)
+        for (uint32_t i = 0; i < nk; ++i)
+            if (c.ground[ne + i] > 0.0) edges.push_back({i, nk, c.ground[ne + i]});
+    return lap_from_edges(edges, nk + (c.grounded ? 1 : 0));
+}
+
+// ---- factors of a reduced Laplacian ----
+struct Factor {
+    uint32_t n = 0;
+    bool dense = false;
+    std::vector<double> pinv;                 // dense generalised inverse, n x n
+    std::vector<uint32_t> round;              // per vertex: elimination round
+    std::vector<double> dinv;                 // per vertex
+    std::vector<std::vector<std::pair<uint32_t, double>>> colv;  // per vertex: (later row, l)
+    uint32_t n_rounds = 0;
+};
+
+// Dense LDL^T in natural order with pseudo-inverse pivots, materialised as
+// G = L^-T D^+ L^-1 (n <= DENSE_MAX).  Returns false on a clearly negative pivot.
+bool dense_pinv(const Lap& m, Factor& f) {
+    const uint32_t n = m.n;
+    std::vector<double> a((size_t)n * n, 0.0);
+    double maxd = 0;
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t k = m.ptr[i]; k < m.ptr[i + 1]; ++k) {
+            a[(size_t)i * n + m.col[k]] += m.val[k];
+            if (m.col[k] == i) maxd = std::max(maxd, std::fabs(m.val[k]));
+        }
+    const double fl = 1e-13 * std::max(maxd, DBL_MIN) * std::max<uint32_t>(n, 1);
+    std::vector<double> piv(n, 0.0);
+    for (uint32_t k = 0; k < n; ++k) {
+        double d = a[(size_t)k * n + k];
+        if (d < -fl) return false;
+        if (d <= fl) {
+            piv[k] = 0.0;
+            for (uint32_t i = k + 1; i < n; ++i) a[(size_t)i * n + k] = 0.0;
+            continue;
+        }
+        piv[k] = d;
+        for (uint32_t i = k + 1; i < n; ++i) {
+            double lik = a[(size_t)i * n + k];
+            if (lik == 0.0) continue;
+            for (uint32_t j = k + 1; j < n; ++j) a[(size_t)i * n + j] -= lik * a[(size_t)k * n + j] / d;
+        }
+        for (uint32_t i = k + 1; i < n; ++i) a[(size_t)i * n + k] /= d;  // L below diagonal
+    }
+    f.n = n;
+    f.dense = true;
+    f.pinv.assign((size_t)n * n, 0.0);
+    std::vector<double> x(n);
+    for (uint32_t c = 0; c < n; ++c) {
+        std::fill(x.begin(), x.end(), 0.0);
+        x[c] = 1.0;
+        for (uint32_t k = 0; k < n; ++k)
+            for (uint32_t i = k + 1; i < n; ++i) x[i] -= a[(size_t)i * n + k] * x[k];
+        for (uint32_t k = 0; k < n; ++k) x[k] = piv[k] > 0.0 ? x[k] / piv[k] : 0.0;
+        for (uint32_t k = n; k-- > 0;) {
+            double s = x[k];
+            for (uint32_t i = k + 1; i < n; ++i) s -= a[(size_t)i * n + k] * x[i];
+            x[k] = s;
+        }
+        for (uint32_t r = 0; r < n; ++r) f.pinv[(size_t)r * n + c] = x[r];
+    }
+    // symmetrise the roundoff
+    for (uint32_t r = 0; r < n; ++r)
+        for (uint32_t c = r + 1; c < n; ++c) {
+            double v = 0.5 * (f.pinv[(size_t)r * n + c] + f.pinv[(size_t)c * n + r]);
+            f.pinv[(size_t)r * n + c] = v;
+            f.pinv[(size_t)c * n + r] = v;
+        }
+    return true;
+}
+
+// Round-parallel approximate Cholesky of a Laplacian.  Each round eliminates an
+// independent set: vertices whose (capped degree, hash, id) key is smaller than
+// every alive neighbour's.  Low-degree vertices therefore go first, which keeps
+// fill low; the clique of an eliminated vertex is replaced by a sampled tree.
+void ac_rounds(const Lap& m, uint64_t seed, uint32_t split, Factor& f) {
+    const uint32_t n = m.n;
+    std::vector<std::vector<std::pair<uint32_t, double>>> adj(n);
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t k = m.ptr[i]; k < m.ptr[i + 1]; ++k)
+            if (m.col[k] != i && m.val[k] < 0.0) adj[i].push_back({m.col[k], -m.val[k]});
+    f.n = n;
+    f.dense = false;
+    f.round.assign(n, 0);
+    f.dinv.assign(n, 0.0);
+    f.colv.assign(n, {});
+    std::vector<char> alive(n, 1);
+    std::vector<uint32_t> live(n);
+    std::iota(live.begin(), live.end(), 0u);
+    std::vector<uint64_t> key(n);
+    std::vector<double> acc(n, 0.0);
+    std::vector<char> seen(n, 0);
+    std::vector<uint32_t> sel;
+    std::vector<Edge> fill;
+    std::vector<std::pair<uint32_t, double>> ent;
+    uint32_t r = 0;
+    while (!live.empty()) {
+        // compact adjacency: drop dead neighbours, merge parallel edges
+        for (uint32_t v : live) {
+            auto& a = adj[v];
+            size_t w = 0;
+            std::vector<uint32_t> order;
+            for (auto& e : a) {
+                if (!alive[e.first] || e.first == v) continue;
+                if (!seen[e.first]) {
+                    seen[e.first] = 1;
+                    order.push_back(e.first);
+                }
+                acc[e.first] += e.second;
+            }
+            std::sort(order.begin(), order.end());
+            a.resize(order.size());
+            for (uint32_t u : order) {
+                a[w++] = {u, acc[u]};
+                acc[u] = 0.0;
+                seen[u] = 0;
+            }
+            uint64_t deg = std::min<uint64_t>(a.size(), 255);
+            key[v] = (deg << 56) | (mix64(seed ^ ((uint64_t)v << 20) ^ r) & 0x00FFFFFFFF000000ull) | 0;
+        }
+        sel.clear();
+        for (uint32_t v : live) {
+            bool best = true;
+            for (auto& e : adj[v]) {
+                uint32_t u = e.first;
+                if (key[u] < key[v] || (key[u] == key[v] && u < v)) {
+                    best = false;
+                    break;
+                }
+            }
+            if (best) sel.push_back(v);
+        }
+        fill.clear();
+        for (uint32_t v : sel) {
+            f.round[v] = r;
+            double d = 0;
+            for (auto& e : adj[v]) d += e.second;
+            if (!(d > 0.0)) {
+                f.dinv[v] = 0.0;
+                continue;
+            }
+            f.dinv[v] = 1.0 / d;
+            auto& cv = f.colv[v];
+            for (auto& e : adj[v]) cv.push_back({e.first, -e.second / d});
+            ent = adj[v];
+            Rng rng{mix64(seed * 0x9E3779B97F4A7C15ull + v + 1)};
+            sample_star(ent, split, rng, fill);
+        }
+        for (uint32_t v : sel) {
+            alive[v] = 0;
+            adj[v].clear();
+            adj[v].shrink_to_fit();
+        }
+        for (auto& e : fill) {
+            adj[e.lo].push_back({e.hi, e.w});
+            adj[e.hi].push_back({e.lo, e.w});
+        }
+        size_t w = 0;
+        for (uint32_t v : live)
+            if (alive[v]) live[w++] = v;
+        live.resize(w);
+        ++r;
+    }
+    f.n_rounds = r;
+}
+
+void factor_lap(const Lap& L, const PrecondCfg& cfg, Factor& f) {
+    if (L.n <= DENSE_MAX && dense_pinv(L, f)) return;
+    ac_rounds(L, cfg.ac_seed, cfg.ac_split, f);
+}
+
+// Gremban cover of a signed matrix (block_elim/solver.rs:220-271).
+Comp cover_of(const Comp& c) {
+    const Csr& a = c.m.c;
+    const uint32_t nr = a.nr, nc = a.nc;
+    Comp o;
+    o.m.c.nr = 2 * nr;
+    o.m.c.nc = 2 * nc;
+    for (int copy = 0; copy < 2; ++copy)
+        for (uint32_t i = 0; i < nr; ++i) {
+            for (int cs = 0; cs < 2; ++cs) {
+                uint32_t base = cs ? nc : 0;
+                bool neg = (cs != 0) != (copy != 0);
+                for (uint32_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+                    double v = a.val[k];
+                    if ((v < 0.0) != neg) continue;
+                    o.m.c.col.push_back(a.col[k] + base);
+                    o.m.c.val.push_back(std::fabs(v));
+                }
+            }
+            o.m.c.ptr.push_back((uint32_t)o.m.c.col.size());
+        }
+    o.m.ct = transpose(o.m.c);
+    auto dbl = [&](const std::vector<double>& v) {
+        std::vector<double> r;
+        r.insert(r.end(), v.begin(), v.begin() + nr);
+        r.insert(r.end(), v.begin(), v.begin() + nr);
+        r.insert(r.end(), v.begin() + nr, v.end());
+        r.insert(r.end(), v.begin() + nr, v.end());
+        return r;
+    };
+    o.diag = dbl(c.diag);
+    o.ground = dbl(c.ground);
+    o.grounded = c.grounded;
+    o.laplacian = true;
+    return o;
+}
+
+std::vector<double> inv_elim(const Comp& c) {
+    std::vector<double> inv(c.m.nr());
+    for (uint32_t i = 0; i < c.m.nr(); ++i) {
+        if (!(c.diag[i] > 0.0)) throw WError(ERR_SINGULAR, "zero diagonal in preconditioner at index " + std::to_string(i));
+        inv[i] = 1.0 / c.diag[i];
+    }
+    return inv;
+}
+
+// LocalSolverConfig routing of factor_reduced (block_elim/solver.rs:191-217):
+// exact reduced system when n_kept <= dense_threshold or SchurMode::Exact,
+// otherwise the clique-tree sampled one.
+Lap reduced_for(const Comp& c, const std::vector<double>& inv_e, const PrecondCfg& cfg) {
+    bool exact = cfg.schur_exact || (cfg.dense_threshold > 0 && c.m.nc() <= cfg.dense_threshold);
+    return exact ? exact_reduced(c, inv_e) : sampled_reduced(c, cfg.schur_seed, std::max(1u, cfg.schur_split));
+}
+
+struct Domain {
+    std::vector<uint32_t> globals;
+    std::vector<double> pw;
+    Comp comp;
+    std::vector<double> inv_e;
+    Factor fac;
+    int mode = 0;   // 0 floating, 1 grounded, 2 cover
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+BuildResult build_preconditioner(const HostDesign& d, const double* w, const PrecondCfg& cfg) {
+    BuildResult out;
+    if (cfg.kind == 0) return out;
+    if (cfg.kind == 2) {  // operator/schwarz.rs:185-229
+        out.kind = 2;
+        out.inv_diag.assign(d.n_dofs, 0.0);
+        for (size_t q = 0; q < d.terms.size(); ++q) {
+            const Term& t = d.terms[q];
+            const uint32_t* lv = d.codes[q].data();
+            for (size_t c = 0; c < t.cols.size(); ++c) {
+                double* sl = &out.inv_diag[t.offset + c * t.n_levels];
+                int k = t.cols[c];
+                for (uint64_t i = 0; i < d.n_obs; ++i) {
+                    double wi = w ? w[i] : 1.0;
+                    sl[lv[i]] += k < 0 ? wi : wi * d.loads[k][i] * d.loads[k][i];
+                }
+            }
+        }
+        for (size_t i = 0; i < out.inv_diag.size(); ++i) {
+            double& v = out.inv_diag[i];
+            if (v == 0.0) continue;
+            double inv = 1.0 / v;
+            if (!std::isfinite(inv)) throw WError(ERR_SINGULAR, "zero diagonal in preconditioner at index " + std::to_string(i));
+            v = inv;
+        }
+        return out;
+    }
+
+    // ---- additive Schwarz: subdomains (domain/factor_pairs.rs:36-152) ----
+    struct Ch { uint32_t term, col; };
+    std::vector<Ch> ch;
+    for (uint32_t t = 0; t < d.terms.size(); ++t)
+        for (uint32_t c = 0; c < d.terms[t].cols.size(); ++c) ch.push_back({t, c});
+    bool any_slope = false;
+    for (auto& x : ch) any_slope = any_slope || d.terms[x.term].cols[x.col] >= 0;
+    std::vector<std::vector<char>> active(d.terms.size());
+    for (size_t t = 0; t < d.terms.size(); ++t) {
+        active[t].assign(d.terms[t].n_levels, 0);
+        for (uint32_t v : d.codes[t]) active[t][v] = 1;
+    }
+    std::vector<Domain> doms;
+    for (size_t a = 0; a < ch.size(); ++a)
+        for (size_t b = a + 1; b < ch.size(); ++b) {
+            Ch R = ch[a], Cc = ch[b];
+            if (R.term == Cc.term) continue;
+            const Term& TR = d.terms[R.term];
+            const Term& TC = d.terms[Cc.term];
+            std::vector<uint32_t> rmap(TR.n_levels, UINT32_MAX), cmap(TC.n_levels, UINT32_MAX), l2g;
+            uint32_t nr = 0, nc = 0;
+            for (uint32_t j = 0; j < TR.n_levels; ++j)
+                if (active[R.term][j]) { rmap[j] = nr++; l2g.push_back(TR.offset + R.col * TR.n_levels + j); }
+            for (uint32_t k = 0; k < TC.n_levels; ++k)
+                if (active[Cc.term][k]) { cmap[k] = nc++; l2g.push_back(TC.offset + Cc.col * TC.n_levels + k); }
+            if (nr == 0 || nc == 0) continue;
+            // weighted cross-tab, each cell summed in observation order (accumulate.rs)
+            const uint32_t* rl = d.codes[R.term].data();
+            const uint32_t* cl = d.codes[Cc.term].data();
+            int kr = TR.cols[R.col], kc = TC.cols[Cc.col];
+            std::vector<double> rdiag(nr, 0.0), cdiag(nc, 0.0);
+            std::vector<uint32_t> cnt(nr + 1, 0);
+            for (uint64_t i = 0; i < d.n_obs; ++i) ++cnt[rmap[rl[i]] + 1];
+            for (uint32_t i = 0; i < nr; ++i) cnt[i + 1] += cnt[i];
+            std::vector<uint32_t> bc(d.n_obs), cur(cnt.begin(), cnt.end() - 1);
+            std::vector<double> bv(d.n_obs);
+            for (uint64_t i = 0; i < d.n_obs; ++i) {
+                uint32_t cj = rmap[rl[i]], ck = cmap[cl[i]];
+                double wi = w ? w[i] : 1.0;
+                double lr = kr < 0 ? 1.0 : d.loads[kr][i];
+                double lc = kc < 0 ? 1.0 : d.loads[kc][i];
+                rdiag[cj] += wi * lr * lr;
+                cdiag[ck] += wi * lc * lc;
+                uint32_t p = cur[cj]++;
+                bc[p] = ck;
+                bv[p] = wi * lr * lc;
+            }
+            Bip full;
+            full.c.nr = nr;
+            full.c.nc = nc;
+            {
+                std::vector<double> work(nc, 0.0);
+                std::vector<uint32_t> touched;
+                std::vector<char> mark(nc, 0);
+                for (uint32_t r = 0; r < nr; ++r) {
+                    for (uint32_t p = cnt[r]; p < cnt[r + 1]; ++p) {
+                        if (!mark[bc[p]]) { mark[bc[p]] = 1; touched.push_back(bc[p]); }
+                        work[bc[p]] += bv[p];
+                    }
+                    std::sort(touched.begin(), touched.end());
+                    for (uint32_t col : touched) {
+                        if (work[col] != 0.0) { full.c.col.push_back(col); full.c.val.push_back(work[col]); }
+                        work[col] = 0.0;
+                        mark[col] = 0;
+                    }
+                    full.c.ptr.push_back((uint32_t)full.c.col.size());
+                    touched.clear();
+                }
+            }
+            std::vector<uint32_t>().swap(bc);
+            std::vector<double>().swap(bv);
+            full.ct = transpose(full.c);
+            const bool known = kr < 0 && kc < 0;
+            // components (cross_tab.rs:175-211): label by DFS, then group
+            const uint32_t nl = nr + nc;
+            std::vector<uint32_t> lab(nl, UINT32_MAX), stk;
+            uint32_t ncomp = 0;
+            for (uint32_t s0 = 0; s0 < nl; ++s0) {
+                if (lab[s0] != UINT32_MAX) continue;
+                lab[s0] = ncomp;
+                stk.push_back(s0);
+                while (!stk.empty()) {
+                    uint32_t v = stk.back();
+                    stk.pop_back();
+                    full.nb(v, [&](uint32_t j, double) {
+                        if (lab[j] == UINT32_MAX) { lab[j] = ncomp; stk.push_back(j); }
+                    });
+                }
+                ++ncomp;
+            }
+            std::vector<std::vector<uint32_t>> crow(ncomp), ccol(ncomp);
+            for (uint32_t i = 0; i < nr; ++i) crow[lab[i]].push_back(i);
+            for (uint32_t k = 0; k < nc; ++k) ccol[lab[nr + k]].push_back(k);
+            std::vector<uint32_t> rre(nr, UINT32_MAX), cre(nc, UINT32_MAX);
+            for (uint32_t ci = 0; ci < ncomp; ++ci) {
+                Comp cp;
+                std::vector<double> diag;
+                if (ncomp == 1) {
+                    cp.m = full;
+                    diag = rdiag;
+                    diag.insert(diag.end(), cdiag.begin(), cdiag.end());
+                } else {
+                    for (uint32_t i = 0; i < crow[ci].size(); ++i) rre[crow[ci][i]] = i;
+                    for (uint32_t i = 0; i < ccol[ci].size(); ++i) cre[ccol[ci][i]] = i;
+                    cp.m.c.nr = (uint32_t)crow[ci].size();
+                    cp.m.c.nc = (uint32_t)ccol[ci].size();
+                    for (uint32_t o : crow[ci]) {
+                        for (uint32_t k = full.c.ptr[o]; k < full.c.ptr[o + 1]; ++k) {
+                            uint32_t nj = cre[full.c.col[k]];
+                            if (nj != UINT32_MAX) { cp.m.c.col.push_back(nj); cp.m.c.val.push_back(full.c.val[k]); }
+                        }
+                        cp.m.c.ptr.push_back((uint32_t)cp.m.c.col.size());
+                    }
+                    cp.m.ct = transpose(cp.m.c);
+                    for (uint32_t o : crow[ci]) { rre[o] = UINT32_MAX; diag.push_back(rdiag[o]); }
+                    for (uint32_t o : ccol[ci]) { cre[o] = UINT32_MAX; diag.push_back(cdiag[o]); }
+                }
+                bool allzero = true;
+                for (double v : diag) allzero = allzero && v == 0.0;
+                if (allzero) continue;
+                std::vector<uint32_t> globals;
+                for (uint32_t o : crow[ci]) globals.push_back(l2g[o]);
+                for (uint32_t o : ccol[ci]) globals.push_back(l2g[nr + o]);
+                if (cp.m.nc() > cp.m.nr()) {  // orient_for_elimination (sddm.rs:85-106)
+                    uint32_t k = cp.m.nr();
+                    std::rotate(diag.begin(), diag.begin() + k, diag.end());
+                    std::rotate(globals.begin(), globals.begin() + k, globals.end());
+                    std::swap(cp.m.c, cp.m.ct);
+                }
+                bool ok = true, warn = false;
+                if (known) {  // convert_known_laplacian (sddm.rs:172-195)
+                    auto rs = sums(cp.m, false);
+                    double td = 0, tm = 0;
+                    for (size_t i = 0; i < diag.size(); ++i) { td += diag[i]; tm += std::fabs(diag[i] - rs[i]); }
+                    ok = tm <= budget(64.0, cp.m.nl(), td);
+                    cp.diag = rs;
+                    cp.ground.assign(cp.m.nl(), 0.0);
+                    cp.grounded = false;
+                    cp.laplacian = true;
+                } else {
+                    ok = convert_general(cp, diag, cfg, warn);
+                }
+                if (!ok) throw WError(ERR_UNSCALABLE, "signed component between term " + std::to_string(R.term) +
+                                                          " column " + std::to_string(R.col) + " and term " +
+                                                          std::to_string(Cc.term) + " column " + std::to_string(Cc.col) +
+                                                          " is not diagonally scalable to SDDM form");
+                if (warn) ++out.n_warnings;
+                Domain dm;
+                dm.globals = std::move(globals);
+                dm.comp = std::move(cp);
+                doms.push_back(std::move(dm));
+            }
+        }
+    if (doms.empty()) return out;  // no subdomains: unpreconditioned (operator/schwarz.rs:249-252)
+
+    if (!any_slope) {  // compute_partition_weights (factor_pairs.rs:154-194)
+        std::vector<uint32_t> cnt(d.n_dofs, 0);
+        for (auto& dm : doms)
+            for (uint32_t g : dm.globals) ++cnt[g];
+        for (auto& dm : doms) {
+            bool uniq = true;
+            for (uint32_t g : dm.globals) uniq = uniq && cnt[g] <= 1;
+            if (uniq) continue;
+            dm.pw.resize(dm.globals.size());
+            for (size_t i = 0; i < dm.globals.size(); ++i) dm.pw[i] = 1.0 / std::sqrt((double)cnt[dm.globals[i]]);
+        }
+    }
+
+    // ---- local solvers: reduced systems and their factors ----
+    for (auto& dm : doms) {
+        dm.inv_e = inv_elim(dm.comp);
+        if (dm.comp.laplacian) {
+            Lap L = reduced_for(dm.comp, dm.inv_e, cfg);
+            factor_lap(L, cfg, dm.fac);
+            dm.mode = dm.comp.grounded ? 1 : 0;
+        } else {
+            Comp cov = cover_of(dm.comp);
+            std::vector<double> inv_c = inv_elim(cov);
+            Lap L = reduced_for(cov, inv_c, cfg);
+            factor_lap(L, cfg, dm.fac);
+            dm.mode = 2;
+        }
+    }
+
+    // ---- pack (layout documented on SchwarzHost) ----
+    out.kind = 1;
+    SchwarzHost& S = out.schwarz;
+    S.n_dofs = (uint32_t)d.n_dofs;
+    S.n_sub = (uint32_t)doms.size();
+    S.loc_ptr.push_back(0);
+    S.kept_ptr.push_back(0);
+    S.ct_ptr.push_back(0);
+    S.c_ptr.push_back(0);
+    uint32_t red = 0, rounds = 0;
+    for (uint32_t s = 0; s < S.n_sub; ++s) {
+        const Domain& dm = doms[s];
+        const uint32_t ne = dm.comp.m.nr(), nk = dm.comp.m.nc(), nloc = ne + nk;
+        const uint32_t lo = S.loc_ptr.back();
+        S.n_elim.push_back(ne);
+        S.n_kept.push_back(nk);
+        S.red_off.push_back(red);
+        S.red_n.push_back(dm.fac.n);
+        S.mode.push_back(dm.mode);
+        for (uint32_t j = 0; j < nloc; ++j) {
+            double f = dm.comp.factors.empty() ? (j < ne ? 1.0 : -1.0) : dm.comp.factors[j];
+            double pw = dm.pw.empty() ? 1.0 : dm.pw[j];
+            S.glob.push_back(dm.globals[j]);
+            S.scale.push_back(pw * f);
+            S.slot_sub.push_back(s);
+            S.inv_e.push_back(j < ne ? dm.inv_e[j] : 0.0);
+        }
+        S.loc_ptr.push_back(lo + nloc);
+        // C^T rows (kept), columns = local slots of eliminated entries
+        for (uint32_t k = 0; k < nk; ++k) {
+            const Csr& ct = dm.comp.m.ct;
+            for (uint32_t a = ct.ptr[k]; a < ct.ptr[k + 1]; ++a) {
+                S.ct_col.push_back(lo + ct.col[a]);
+                S.ct_val.push_back(ct.val[a]);
+            }
+            S.ct_ptr.push_back((uint32_t)S.ct_col.size());
+            S.ct_row_slot.push_back(lo + ne + k);
+            S.ct_row_red.push_back(red + k);
+        }
+        S.kept_ptr.push_back(S.kept_ptr.back() + nk);
+        // C rows (eliminated), columns = reduced slot of the kept entry
+        for (uint32_t e = 0; e < ne; ++e) {
+            const Csr& c = dm.comp.m.c;
+            for (uint32_t a = c.ptr[e]; a < c.ptr[e + 1]; ++a) {
+                S.c_col.push_back(red + c.col[a]);
+                S.c_val.push_back(c.val[a]);
+            }
+            S.c_ptr.push_back((uint32_t)S.c_col.size());
+            S.elim_slot.push_back(lo + e);
+        }
+        S.cross_nnz += 2ull * dm.comp.m.c.nnz();
+        for (uint32_t i = 0; i < dm.fac.n; ++i) S.red_sub.push_back(s);
+        red += dm.fac.n;
+        if (!dm.fac.dense) rounds = std::max(rounds, dm.fac.n_rounds);
+    }
+    S.n_red = red;
+    S.dinv.assign(red, 0.0);
+    // dense blocks
+    S.dense_rows_ptr.push_back(0);
+    for (uint32_t s = 0; s < S.n_sub; ++s) {
+        const Factor& f = doms[s].fac;
+        if (!f.dense) continue;
+        for (uint32_t r = 0; r < f.n; ++r) {
+            for (uint32_t c = 0; c < f.n; ++c) {
+                S.dense_col.push_back(S.red_off[s] + c);
+                S.dense_val.push_back(f.pinv[(size_t)r * f.n + c]);
+            }
+            S.dense_rows_ptr.push_back((uint32_t)S.dense_col.size());
+            S.dense_row_slot.push_back(S.red_off[s] + r);
+        }
+        S.factor_nnz += (uint64_t)f.n * f.n;
+    }
+    // round-scheduled factors: forward rows pull from earlier columns, backward
+    // rows (= eliminated columns) pull from later rows.
+    S.n_rounds = rounds;
+    std::vector<std::vector<uint32_t>> by_round(rounds);
+    std::vector<std::vector<std::vector<std::pair<uint32_t, double>>>> rowents(S.n_sub);
+    for (uint32_t s = 0; s < S.n_sub; ++s) {
+        const Factor& f = doms[s].fac;
+        if (f.dense) continue;
+        const uint32_t ro = S.red_off[s];
+        rowents[s].assign(f.n, {});
+        for (uint32_t v = 0; v < f.n; ++v) {
+            S.dinv[ro + v] = f.dinv[v];
+            by_round[f.round[v]].push_back(ro + v);
+            for (auto& e : f.colv[v]) rowents[s][e.first].push_back({ro + v, e.second});
+            S.factor_nnz += f.colv[v].size();
+        }
+    }
+    S.fwd_round_ptr.push_back(0);
+    S.fwd_ptr.push_back(0);
+    S.bwd_round_ptr.push_back(0);
+    S.bwd_ptr.push_back(0);
+    for (uint32_t r = 0; r < rounds; ++r) {
+        S.max_round_rows = std::max<uint32_t>(S.max_round_rows, (uint32_t)by_round[r].size());
+        for (uint32_t slot : by_round[r]) {
+            uint32_t s = S.red_sub[slot], v = slot - S.red_off[s];
+            S.fwd_row.push_back(slot);
+            for (auto& e : rowents[s][v]) {
+                S.fwd_col.push_back(e.first);
+                S.fwd_val.push_back(e.second);
+            }
+            S.fwd_ptr.push_back((uint32_t)S.fwd_col.size());
+            S.bwd_row.push_back(slot);
+            for (auto& e : doms[s].fac.colv[v]) {
+                S.bwd_col.push_back(S.red_off[s] + e.first);
+                S.bwd_val.push_back(e.second);
+            }
+            S.bwd_ptr.push_back((uint32_t)S.bwd_col.size());
+        }
+        S.fwd_round_ptr.push_back((uint32_t)S.fwd_row.size());
+        S.bwd_round_ptr.push_back((uint32_t)S.bwd_row.size());
+    }
+    // prolongation: DOF -> local slots, in subdomain order
+    S.dof_ptr.assign(S.n_dofs + 1, 0);
+    for (uint32_t g : S.glob) ++S.dof_ptr[g + 1];
+    for (uint32_t i = 0; i < S.n_dofs; ++i) S.dof_ptr[i + 1] += S.dof_ptr[i];
+    S.dof_slot.resize(S.glob.size());
+    {
+        std::vector<uint32_t> cur(S.dof_ptr.begin(), S.dof_ptr.end() - 1);
+        for (uint32_t j = 0; j < S.glob.size(); ++j) S.dof_slot[cur[S.glob[j]]++] = j;
+    }
+    return out;
+}
+
+}  // namespace wgpu

@@ -1,0 +1,918 @@
+// kernels.cuh -- device code of the fixed-effects solve (sm_100a).
+//
+// Vector layout: K right-hand sides are interleaved, element (i, k) of an
+// observation vector lives at [i*K + k] and of a DOF vector at [j*K + k], so a
+// thread that reads one code reads every column's coefficient from one
+// contiguous K-wide run.  All reductions are formed in a fixed order (per-thread
+// strided partials, a fixed shuffle tree, per-block partials summed by the last
+// block in block order), so every result is bitwise reproducible.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+
+#include "segreduce.cuh"
+
+namespace wgpu {
+
+constexpr int MAXQ = 8, MAXC = 4, MAXS = 16;
+constexpr int RED_THREADS = 256;
+
+// Design-operator parameters (operator/design.rs:22-62), passed by value.
+struct OpParams {
+    uint32_t n;
+    int Q;
+    const uint32_t* codes[MAXQ];
+    uint32_t off[MAXQ], L[MAXQ];
+    int ncol[MAXQ];
+    int load[MAXQ][MAXC];      // -1 intercept, else loading column
+    const double* loads[MAXS];
+    const double* sqrt_w;      // nullptr = unweighted
+};
+
+// Per-column LSMR scalar state (lsmr/recurrence.rs + bidiag.rs), double
+// buffered by iteration parity.
+struct ColState {
+    double alpha, beta_prev_inv, beta;
+    double alpha_bar, phi_bar, c_bar, s_bar, zeta_bar, zeta0;
+    double prev_rho, prev_rho_bar;
+    double a_norm_sq, abs_tol, rel_tol;
+    double t_x, t_hbar, t_h, vscale;
+    double b_norm;
+    long long itn, maxiter;
+    int done, stop, upd, err;
+};
+
+struct Ctl {
+    int all_done;   // every column finished: loop kernels return at entry
+    int k5_skip;    // the vector update of this iteration has nothing to do
+    int err;        // first error code raised on the device
+    int pad;
+};
+
+enum Stop { STOP_NONE = -1, STOP_ZERO_RHS = 0, STOP_INIT_ZERO = 1, STOP_RESID = 2, STOP_NORMAL = 3,
+            STOP_MAXITER = 5 };
+
+// ---------------------------------------------------------------------------
+// fixed-order block reduction helpers
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum over the block; the result is valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double* sm /* >= 32 */) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sm[wid] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sm[w];
+    return t;
+}
+
+// Publishes NV block partials and returns true in the (single) last block to
+// finish, in which `tot` holds the grand totals summed in block order.
+template <int NV>
+__device__ bool grid_reduce(const double (&v)[NV], double* partials, unsigned* counter,
+                            double (&tot)[NV]) {
+    __shared__ double sm[32];
+    __shared__ int is_last;
+    double b[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) b[i] = block_sum(v[i], sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) partials[(size_t)blockIdx.x * NV + i] = b[i];
+        __threadfence();
+        unsigned prev = atomicAdd(counter, 1u);
+        is_last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        double a = 0;
+        for (unsigned blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
+            a += __ldcg(&partials[(size_t)blk * NV + i]);
+        tot[i] = block_sum(a, sm);
+    }
+    if (threadIdx.x == 0) *counter = 0;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// D x row sum for K columns at observation i (gather.rs:10-109).
+template <int K>
+__device__ __forceinline__ void row_dx(const OpParams& p, uint32_t i, const double* __restrict__ x,
+                                       double (&s)[K]) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) s[k] = 0.0;
+    for (int t = 0; t < p.Q; ++t) {
+        const uint32_t code = __ldg(p.codes[t] + i);
+        for (int c = 0; c < p.ncol[t]; ++c) {
+            const size_t base = ((size_t)p.off[t] + (size_t)c * p.L[t] + code) * K;
+            const int li = p.load[t][c];
+            const double ld = li < 0 ? 1.0 : __ldg(p.loads[li] + i);
+#pragma unroll
+            for (int k = 0; k < K; ++k) s[k] += __ldg(x + base + k) * ld;
+        }
+    }
+}
+
+// y = W^{1/2} D x  (Operator::apply; internal order)
+template <int K>
+__global__ void k_apply(OpParams p, const double* __restrict__ x, double* __restrict__ y) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
+        double s[K];
+        row_dx<K>(p, i, x, s);
+        const double w = p.sqrt_w ? p.sqrt_w[i] : 1.0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) y[(size_t)i * K + k] = p.sqrt_w ? w * s[k] : s[k];
+    }
+}
+
+// demeaned = y - D x (unweighted; solver.rs:468-473)
+template <int K>
+__global__ void k_demean(OpParams p, const double* __restrict__ x, const double* __restrict__ yint,
+                         double* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
+        double s[K];
+        row_dx<K>(p, i, x, s);
+#pragma unroll
+        for (int k = 0; k < K; ++k) out[(size_t)i * K + k] = yint[(size_t)i * K + k] - s[k];
+    }
+}
+
+// LSMR step, first half (bidiag.rs:278-283): u <- A v + scale u with
+// scale = -(alpha / beta_prev), beta = ||u||; fused in one row sweep.
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gather_update(OpParams p, const double* __restrict__ v, double* __restrict__ u, ColState* cur,
+                Ctl* ctl, double* partials, unsigned* counter) {
+    if (ctl->all_done) {
+        // nothing left to update this iteration either (k_alpha_step also returns)
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->k5_skip = 1;
+        return;
+    }
+    double scale[K];
+    bool act[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        act[k] = !cur[k].done;
+        scale[k] = -(cur[k].alpha * cur[k].beta_prev_inv);
+    }
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
+        double s[K];
+        row_dx<K>(p, i, v, s);
+        const double w = p.sqrt_w ? __ldg(p.sqrt_w + i) : 1.0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double av = p.sqrt_w ? w * s[k] : s[k];
+            double* up = u + (size_t)i * K + k;
+            double nu = act[k] ? av + scale[k] * (*up) : *up;
+            if (act[k]) *up = nu;
+            acc[k] += nu * nu;
+        }
+    }
+    double tot[K];
+    if (grid_reduce<K>(acc, partials, counter, tot) && threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (act[k]) cur[k].beta = sqrt(tot[k]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Scatter D^T (W^{1/2} u) as a segmented reduction (scatter.rs:14-73): one
+// problem per (term, coefficient column); segments are the term's levels,
+// positions its level-sorted observation order (identity when sorted).
+struct ScatterProb {
+    const uint32_t* seg_ptr;   // level_ptr (n_levels + 1)
+    const uint32_t* order;     // position -> observation (nullptr = identity)
+    const double* load;        // loading column (nullptr = intercept)
+    uint32_t out_off;          // DOF of level 0 of this column
+    uint32_t pad;
+};
+
+// EPI 0: out = sum (Operator::apply_adjoint)
+// EPI 1: p~ <- sum / beta - (beta / alpha) p~ (bidiag.rs:474-485), per column,
+//        skipping finished columns; beta == 0 (lucky breakdown) zeroes p~.
+template <int K, int EPI>
+struct ScatterF {
+    using Prob = ScatterProb;
+    const ScatterProb* probs;
+    const double* u;
+    const double* sqrt_w;
+    double* out;
+    const ColState* cur;
+    __device__ const uint32_t* seg_ptr(const Prob& pr) const { return pr.seg_ptr; }
+    __device__ void value(const Prob& pr, uint32_t pos, double (&v)[K]) const {
+        const uint32_t i = pr.order ? __ldg(pr.order + pos) : pos;
+        double f = pr.load ? __ldg(pr.load + i) : 1.0;
+        if (sqrt_w) f *= __ldg(sqrt_w + i);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = f * u[(size_t)i * K + k];
+    }
+    __device__ void emit(const Prob& pr, uint32_t seg, const double (&s)[K]) const {
+        double* o = out + ((size_t)pr.out_off + seg) * K;
+        if (EPI == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) o[k] = s[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (cur[k].done) continue;
+                const double beta = cur[k].beta;
+                o[k] = beta == 0.0 ? 0.0 : s[k] * (1.0 / beta) - (beta / cur[k].alpha) * o[k];
+            }
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Additive Schwarz apply (schwarz-precond executor.rs + block_elim/solver.rs),
+// all subdomains at once.  See SchwarzHost (host.hpp) for the layout.
+struct SchwarzDev {
+    uint32_t n_sub;
+    const uint32_t* loc_ptr;
+    const uint32_t* n_elim;
+    const uint32_t* red_off;
+    const uint32_t* n_kept;
+    const uint32_t* red_n;
+    const int* mode;
+    const uint32_t* glob;
+    const double* scale;
+    const uint32_t* slot_sub;
+    const double* inv_e;
+    const uint32_t* ct_col;
+    const double* ct_val;
+    const uint32_t* ct_row_slot;
+    const uint32_t* ct_row_red;
+    const uint32_t* elim_slot;
+    const uint32_t* c_col;
+    const double* c_val;
+    const uint32_t* red_sub;
+    const uint32_t* dense_row_slot;
+    const uint32_t* dense_col;
+    const double* dense_val;
+    const double* dinv;
+    const uint32_t* fwd_row;
+    const uint32_t* fwd_col;
+    const double* fwd_val;
+    const uint32_t* bwd_row;
+    const uint32_t* bwd_col;
+    const double* bwd_val;
+    const uint32_t* dof_slot;
+    const uint32_t* kept_ptr;
+    // work (K-interleaved)
+    double* rl;   // restricted, folded local rhs (per local slot)
+    double* sl;   // local solution (per local slot)
+    double* rb;   // reduced rhs
+    double* yv;   // forward-substitution values
+    double* xv;   // reduced solution
+    double* m1;   // per subdomain: mean of rl (floating) else 0
+    double* m2;   // per subdomain: mean of the reduced rhs (floating) else 0
+    double* m3;   // per subdomain: mean of the local solution (floating) else 0
+};
+
+struct SegProb {          // generic: one pointer array + a segment base
+    const uint32_t* seg_ptr;
+    uint32_t seg_base;    // added to the local segment id
+    uint32_t pad;
+};
+
+__device__ __forceinline__ int sd_mode(const SchwarzDev& S, uint32_t s) { return S.mode[s]; }
+
+// solution of kept index k (reduced slot u) after the gauge / cover read-back
+template <int K>
+__device__ __forceinline__ void kept_solution(const SchwarzDev& S, uint32_t u, double (&o)[K]) {
+    const uint32_t s = S.red_sub[u];
+    const int m = S.mode[s];
+    if (m == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) o[k] = S.xv[(size_t)u * K + k];
+    } else if (m == 1) {
+        const size_t g = (size_t)(S.red_off[s] + S.n_kept[s]) * K;
+#pragma unroll
+        for (int k = 0; k < K; ++k) o[k] = S.xv[(size_t)u * K + k] - S.xv[g + k];
+    } else {
+        const size_t w = (size_t)(u + S.n_kept[s]) * K;
+#pragma unroll
+        for (int k = 0; k < K; ++k) o[k] = 0.5 * (S.xv[(size_t)u * K + k] - S.xv[w + k]);
+    }
+}
+
+// S1: restrict + fold, per-subdomain sums -> m1 (solver.rs:445-451, domain.rs:133-152)
+template <int K>
+struct RestrictF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    const double* r;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t j, double (&v)[K]) const {
+        const uint32_t g = __ldg(S.glob + j);
+        const double sc = __ldg(S.scale + j);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            v[k] = sc * r[(size_t)g * K + k];
+            S.rl[(size_t)j * K + k] = v[k];
+        }
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t sub = p.seg_base + seg;
+        const bool fl = S.mode[sub] == 0;
+        const double inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
+#pragma unroll
+        for (int k = 0; k < K; ++k) S.m1[(size_t)sub * K + k] = fl ? s[k] * inv : 0.0;
+    }
+};
+
+// S3: reduced rhs  rhs_k + C^T D_e^-1 rhs_e  (solver.rs:360-371)
+template <int K>
+struct CtF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+        const uint32_t e = __ldg(S.ct_col + a);
+        const uint32_t s = __ldg(S.slot_sub + e);
+        const double f = __ldg(S.ct_val + a) * __ldg(S.inv_e + e);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = f * (S.rl[(size_t)e * K + k] - S.m1[(size_t)s * K + k]);
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t row = p.seg_base + seg;
+        const uint32_t slot = S.ct_row_slot[row];
+        const uint32_t sub = S.slot_sub[slot];
+        const uint32_t rbi = S.ct_row_red[row];
+        const bool cover = S.mode[sub] == 2;
+        const uint32_t nk = S.n_kept[sub];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double val = (S.rl[(size_t)slot * K + k] - S.m1[(size_t)sub * K + k]) + s[k];
+            S.rb[(size_t)rbi * K + k] = val;
+            if (cover) S.rb[(size_t)(rbi + nk) * K + k] = -val;
+        }
+    }
+};
+
+// S4: per-subdomain sum of the kept reduced rhs -> floating mean (m2) or the
+// explicit ground's rhs (solver.rs:372-384)
+template <int K>
+struct KeptSumF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t q, double (&v)[K]) const {
+        const uint32_t u = __ldg(S.ct_row_red + q);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = S.rb[(size_t)u * K + k];
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t sub = p.seg_base + seg;
+        const int m = S.mode[sub];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (m == 0) {
+                S.m2[(size_t)sub * K + k] = s[k] / (double)S.red_n[sub];
+            } else {
+                S.m2[(size_t)sub * K + k] = 0.0;
+                if (m == 1) S.rb[(size_t)(S.red_off[sub] + S.n_kept[sub]) * K + k] = -s[k];
+            }
+        }
+    }
+};
+
+template <int K>
+__device__ __forceinline__ void reduced_rhs(const SchwarzDev& S, uint32_t u, double (&b)[K]) {
+    const uint32_t s = S.red_sub[u];
+#pragma unroll
+    for (int k = 0; k < K; ++k) b[k] = S.rb[(size_t)u * K + k] - S.m2[(size_t)s * K + k];
+}
+
+// S5 (small systems): x = G b with the dense generalised inverse G
+template <int K>
+struct DenseF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+        double b[K];
+        reduced_rhs<K>(S, __ldg(S.dense_col + a), b);
+        const double g = __ldg(S.dense_val + a);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = g * b[k];
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t u = S.dense_row_slot[p.seg_base + seg];
+#pragma unroll
+        for (int k = 0; k < K; ++k) S.xv[(size_t)u * K + k] = s[k];
+    }
+};
+
+// S5 (factored systems), one round of L y = b: y_u = b_u - sum_v L[u,v] y_v,
+// and z_u = y_u / d_u for the backward pass.
+template <int K>
+struct FwdF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+        const uint32_t c = __ldg(S.fwd_col + a);
+        const double l = __ldg(S.fwd_val + a);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = l * S.yv[(size_t)c * K + k];
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t u = S.fwd_row[p.seg_base + seg];
+        double b[K];
+        reduced_rhs<K>(S, u, b);
+        const double di = S.dinv[u];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double y = b[k] - s[k];
+            S.yv[(size_t)u * K + k] = y;
+            S.xv[(size_t)u * K + k] = y * di;
+        }
+    }
+};
+
+// one round of L^T x = z: x_v = z_v - sum_u L[u,v] x_u (rounds in reverse)
+template <int K>
+struct BwdF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+        const uint32_t c = __ldg(S.bwd_col + a);
+        const double l = __ldg(S.bwd_val + a);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = l * S.xv[(size_t)c * K + k];
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t v = S.bwd_row[p.seg_base + seg];
+#pragma unroll
+        for (int k = 0; k < K; ++k) S.xv[(size_t)v * K + k] -= s[k];
+    }
+};
+
+// S6: back-substitution  x_e = D_e^-1 rhs_e + D_e^-1 C x_k  (solver.rs:41-77)
+template <int K>
+struct CF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+        double x[K];
+        kept_solution<K>(S, __ldg(S.c_col + a), x);
+        const double c = __ldg(S.c_val + a);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = c * x[k];
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t e = S.elim_slot[p.seg_base + seg];
+        const uint32_t sub = S.slot_sub[e];
+        const double ie = S.inv_e[e];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            S.sl[(size_t)e * K + k] = (S.rl[(size_t)e * K + k] - S.m1[(size_t)sub * K + k]) * ie + ie * s[k];
+    }
+};
+
+// S7: kept-block read-back and per-subdomain solution mean (floating)
+template <int K>
+struct MeanF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t j, double (&v)[K]) const {
+        const uint32_t s = __ldg(S.slot_sub + j);
+        const uint32_t kk = j - S.loc_ptr[s];
+        const uint32_t ne = S.n_elim[s];
+        if (kk < ne) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] = S.sl[(size_t)j * K + k];
+        } else {
+            kept_solution<K>(S, S.red_off[s] + (kk - ne), v);
+#pragma unroll
+            for (int k = 0; k < K; ++k) S.sl[(size_t)j * K + k] = v[k];
+        }
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t sub = p.seg_base + seg;
+        const bool fl = S.mode[sub] == 0;
+        const double inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
+#pragma unroll
+        for (int k = 0; k < K; ++k) S.m3[(size_t)sub * K + k] = fl ? s[k] * inv : 0.0;
+    }
+};
+
+// S8: unfold + prolongate  z_g = sum over subdomains of w * f * (x - mean)
+// (domain.rs:154-171), a gather per DOF in subdomain order.
+template <int K>
+struct ProlongF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    double* z;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+        const uint32_t j = __ldg(S.dof_slot + a);
+        const uint32_t s = __ldg(S.slot_sub + j);
+        const double sc = __ldg(S.scale + j);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = sc * (S.sl[(size_t)j * K + k] - S.m3[(size_t)s * K + k]);
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        double* o = z + (size_t)(p.seg_base + seg) * K;
+#pragma unroll
+        for (int k = 0; k < K; ++k) o[k] = s[k];
+    }
+};
+
+// ---------------------------------------------------------------------------
+// LSMR vector kernels over the DOF space
+
+// v = d * p~ (Diagonal, operator/schwarz.rs:64-81) or v = p~ (identity)
+template <int K>
+__global__ void k_diag_apply(uint32_t n, const double* __restrict__ d, const double* __restrict__ p,
+                             double* __restrict__ v, const Ctl* ctl) {
+    if (ctl && ctl->all_done) return;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const double dj = d ? d[j] : 1.0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[(size_t)j * K + k] = dj * p[(size_t)j * K + k];
+    }
+}
+
+__device__ __forceinline__ void givens(double a, double b, double& c, double& s, double& r) {
+    r = hypot(a, b);
+    if (r > 0.0) {
+        c = a / r;
+        s = b / r;
+    } else {
+        c = 1.0;
+        s = 0.0;
+    }
+}
+
+// alpha = sqrt(<v, p~>) with the indefinite-M check (bidiag.rs:98-111), then
+// one LsmrRecurrenceState::step, the SolutionState coefficients and the
+// convergence test (recurrence.rs:81-255), written to the next state.
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS)
+k_alpha_step(uint32_t n, const double* __restrict__ v, const double* __restrict__ p,
+             const ColState* cur, ColState* nxt, Ctl* ctl, double* partials, unsigned* counter) {
+    if (ctl->all_done) return;
+    double acc[3 * K];
+#pragma unroll
+    for (int i = 0; i < 3 * K; ++i) acc[i] = 0.0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double a = v[(size_t)j * K + k], b = p[(size_t)j * K + k];
+            acc[3 * k] += a * b;
+            acc[3 * k + 1] += a * a;
+            acc[3 * k + 2] += b * b;
+        }
+    }
+    double tot[3 * K];
+    if (!grid_reduce<3 * K>(acc, partials, counter, tot) || threadIdx.x != 0) return;
+    bool all = true;
+    for (int k = 0; k < K; ++k) {
+        ColState s = cur[k];
+        if (s.done) {
+            s.upd = 0;
+            nxt[k] = s;
+            continue;
+        }
+        const double beta = s.beta;
+        double alpha = 0.0;
+        if (beta != 0.0) {
+            const double vp = tot[3 * k];
+            if (vp < 0.0) {
+                const double bound = sqrt(DBL_EPSILON) * sqrt(tot[3 * k + 1] * tot[3 * k + 2]);
+                if (vp < -bound) {
+                    s.err = 5;
+                    s.done = 1;
+                    s.upd = 0;
+                    nxt[k] = s;
+                    atomicCAS(&ctl->err, 0, 5);
+                    continue;
+                }
+            }
+            alpha = sqrt(fmax(vp, 0.0));
+        }
+        // ConvergenceState::observe
+        s.a_norm_sq += alpha * alpha + beta * beta;
+        // LsmrRecurrenceState::step
+        double hc, hs, hr;
+        givens(s.alpha_bar, beta, hc, hs, hr);
+        const double theta_new = hs * alpha;
+        const double alpha_bar_new = -hc * alpha;
+        const double phi_bar_new = hs * s.phi_bar;
+        const double theta_bar = s.s_bar * hr;
+        double bc, bs, br;
+        givens(s.c_bar * hr, theta_new, bc, bs, br);
+        const double zeta = bc * s.zeta_bar;
+        const double zeta_bar_new = -bs * s.zeta_bar;
+        s.alpha_bar = alpha_bar_new;
+        s.phi_bar = phi_bar_new;
+        s.c_bar = bc;
+        s.s_bar = bs;
+        s.zeta_bar = zeta_bar_new;
+        // SolutionState::update coefficients
+        const double txd = hr * br;
+        s.t_x = fabs(txd) > DBL_EPSILON ? zeta / txd : 0.0;
+        const double thd = s.prev_rho * s.prev_rho_bar;
+        s.t_hbar = fabs(thd) > DBL_EPSILON ? theta_bar * hr / thd : 0.0;
+        s.t_h = fabs(hr) > DBL_EPSILON ? theta_new / hr : 0.0;
+        s.prev_rho = hr;
+        s.prev_rho_bar = br;
+        // bidiagonalisation state for the next step
+        s.vscale = alpha > 0.0 ? 1.0 / alpha : 1.0;
+        s.alpha = alpha;
+        s.beta_prev_inv = beta == 0.0 ? 0.0 : 1.0 / beta;
+        s.itn += 1;
+        s.upd = 1;
+        // ConvergenceState::check
+        const double residual = fabs(s.phi_bar);
+        if (residual <= s.abs_tol) {
+            s.done = 1;
+            s.stop = STOP_RESID;
+        } else {
+            const double an = fmax(sqrt(s.a_norm_sq), DBL_MIN);
+            if (fabs(s.zeta_bar) / (an * fmax(residual, DBL_MIN)) <= s.rel_tol) {
+                s.done = 1;
+                s.stop = STOP_NORMAL;
+            } else if (s.itn >= s.maxiter) {
+                s.done = 1;
+                s.stop = STOP_MAXITER;
+            }
+        }
+        nxt[k] = s;
+        all = all && s.done;
+    }
+    ctl->k5_skip = 0;
+    ctl->all_done = all ? 1 : 0;
+}
+
+// v <- v / alpha; h_bar, x, h update (recurrence.rs:143-191)
+template <int K>
+__global__ void k_solution_update(uint32_t n, double* __restrict__ v, double* __restrict__ h,
+                                  double* __restrict__ hb, double* __restrict__ x,
+                                  const ColState* nxt, const Ctl* ctl) {
+    if (ctl->k5_skip) return;
+    double vs[K], tx[K], thb[K], th[K];
+    bool up[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        up[k] = nxt[k].upd != 0;
+        vs[k] = nxt[k].vscale;
+        tx[k] = nxt[k].t_x;
+        thb[k] = nxt[k].t_hbar;
+        th[k] = nxt[k].t_h;
+    }
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!up[k]) continue;
+            const size_t o = (size_t)j * K + k;
+            const double vn = v[o] * vs[k];
+            v[o] = vn;
+            const double ho = h[o];
+            const double hbv = ho - thb[k] * hb[o];
+            hb[o] = hbv;
+            x[o] += tx[k] * hbv;
+            h[o] = vn - th[k] * ho;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// initialisation of a multi-RHS run (lsmr.rs:206-295, bidiag.rs:428-472)
+
+// internal-order y and b = sqrt(w) y from column-major caller-order Y; per
+// column max |b| and a non-finite flag.
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS)
+k_load_rhs(uint32_t n, uint32_t k_used, const double* __restrict__ Y, const uint32_t* __restrict__ perm,
+           const double* __restrict__ sqrt_w, double* __restrict__ yint, double* __restrict__ b,
+           double* partials, unsigned* counter, double* out_max, int* nonfinite) {
+    double mx[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) mx[k] = 0.0;
+    int bad = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t src = perm ? perm[i] : i;
+        const double w = sqrt_w ? sqrt_w[i] : 1.0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double y = (uint32_t)k < k_used ? Y[(size_t)k * n + src] : 0.0;
+            if (!isfinite(y)) bad = 1;
+            yint[(size_t)i * K + k] = y;
+            const double bv = sqrt_w ? w * y : y;
+            b[(size_t)i * K + k] = bv;
+            mx[k] = fmax(mx[k], fabs(bv));
+        }
+    }
+    if (bad) atomicExch(nonfinite, 1);
+    // max is order independent; reuse the sum machinery on per-block maxima
+    __shared__ double sm[32][K];
+    __shared__ int is_last;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double m = mx[k];
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5][k] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < K; ++k) {
+            double m = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sm[w][k]);
+            partials[(size_t)blockIdx.x * K + k] = m;
+        }
+        __threadfence();
+        is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        for (int k = 0; k < K; ++k) {
+            double m = 0;
+            for (unsigned blk = 0; blk < gridDim.x; ++blk) m = fmax(m, __ldcg(&partials[(size_t)blk * K + k]));
+            out_max[k] = m;
+        }
+        *counter = 0;
+    }
+}
+
+// beta_1 = ||b|| (max-scaled, lsmr.rs:22-36), u = b / beta_1, and the column
+// state seeded for the adjoint/preconditioner pass.
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS)
+k_norm_b(uint32_t n, const double* __restrict__ b, const double* bmax, ColState* st, double tol,
+         long long maxiter, uint32_t k_used, Ctl* ctl, double* partials, unsigned* counter) {
+    double acc[K];
+    double sc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        acc[k] = 0.0;
+        sc[k] = bmax[k] > 0.0 ? 1.0 / bmax[k] : 0.0;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double t = b[(size_t)i * K + k] * sc[k];
+            acc[k] += t * t;
+        }
+    double tot[K];
+    if (!grid_reduce<K>(acc, partials, counter, tot) || threadIdx.x != 0) return;
+    for (int k = 0; k < K; ++k) {
+        ColState s;
+        memset(&s, 0, sizeof(s));
+        const double beta = bmax[k] == 0.0 ? 0.0 : bmax[k] * sqrt(tot[k]);
+        s.beta = beta;
+        s.b_norm = beta;
+        s.maxiter = maxiter;
+        s.abs_tol = tol * beta;
+        s.rel_tol = tol;
+        s.stop = STOP_NONE;
+        s.prev_rho = 1.0;
+        s.prev_rho_bar = 1.0;
+        s.beta_prev_inv = 1.0;
+        if ((uint32_t)k >= k_used || beta == 0.0) {
+            s.done = 1;
+            s.stop = STOP_ZERO_RHS;
+        }
+        st[k] = s;
+    }
+    ctl->all_done = 0;
+    ctl->k5_skip = 0;
+}
+
+template <int K>
+__global__ void k_scale_u(uint32_t n, const double* __restrict__ b, double* __restrict__ u,
+                          const ColState* st) {
+    double inv[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) inv[k] = st[k].beta > 0.0 ? 1.0 / st[k].beta : 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) u[(size_t)i * K + k] = b[(size_t)i * K + k] * inv[k];
+}
+
+// alpha_1 from <v, p~>; LsmrRecurrenceState::init (recurrence.rs:67-78)
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS)
+k_alpha_init(uint32_t n, const double* __restrict__ v, const double* __restrict__ p, ColState* st,
+             ColState* st_other, Ctl* ctl, double* partials, unsigned* counter) {
+    double acc[3 * K];
+#pragma unroll
+    for (int i = 0; i < 3 * K; ++i) acc[i] = 0.0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double a = v[(size_t)j * K + k], b = p[(size_t)j * K + k];
+            acc[3 * k] += a * b;
+            acc[3 * k + 1] += a * a;
+            acc[3 * k + 2] += b * b;
+        }
+    double tot[3 * K];
+    if (!grid_reduce<3 * K>(acc, partials, counter, tot) || threadIdx.x != 0) return;
+    bool all = true;
+    for (int k = 0; k < K; ++k) {
+        ColState s = st[k];
+        if (!s.done) {
+            const double vp = tot[3 * k];
+            bool bad = false;
+            if (vp < 0.0) {
+                const double bound = sqrt(DBL_EPSILON) * sqrt(tot[3 * k + 1] * tot[3 * k + 2]);
+                bad = vp < -bound;
+            }
+            if (bad) {
+                s.err = 5;
+                s.done = 1;
+                atomicCAS(&ctl->err, 0, 5);
+            } else {
+                const double alpha = sqrt(fmax(vp, 0.0));
+                s.alpha = alpha;
+                if (alpha == 0.0) {
+                    s.done = 1;
+                    s.stop = STOP_INIT_ZERO;
+                    s.phi_bar = s.beta;  // residual_norm = rhs_norm
+                } else {
+                    s.vscale = 1.0 / alpha;
+                    s.a_norm_sq = alpha * alpha;
+                    s.alpha_bar = alpha;
+                    s.phi_bar = s.beta;
+                    s.c_bar = 1.0;
+                    s.s_bar = 0.0;
+                    s.zeta_bar = alpha * s.beta;
+                    s.zeta0 = fmax(fabs(s.zeta_bar), DBL_MIN);
+                    s.beta_prev_inv = 1.0;
+                }
+            }
+        }
+        s.upd = 0;
+        st[k] = s;
+        st_other[k] = s;
+        all = all && s.done;
+    }
+    ctl->all_done = all ? 1 : 0;
+    ctl->k5_skip = 0;
+}
+
+// v <- v / alpha_1, h = v, x = 0, h_bar = 0  (SolutionState::init)
+template <int K>
+__global__ void k_init_vectors(uint32_t n, double* __restrict__ v, double* __restrict__ h,
+                               double* __restrict__ hb, double* __restrict__ x, const ColState* st) {
+    double vs[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) vs[k] = (st[k].done || st[k].alpha == 0.0) ? 1.0 : st[k].vscale;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const size_t o = (size_t)j * K + k;
+            const double vn = v[o] * vs[k];
+            v[o] = vn;
+            h[o] = vn;
+            hb[o] = 0.0;
+            x[o] = 0.0;
+        }
+}
+
+// interleaved (internal order) -> column-major caller order
+template <int K>
+__global__ void k_store_obs(uint32_t n, uint32_t k_used, const double* __restrict__ src,
+                            const uint32_t* __restrict__ perm, double* __restrict__ dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t d = perm ? perm[i] : i;
+        for (uint32_t k = 0; k < k_used; ++k) dst[(size_t)k * n + d] = src[(size_t)i * K + k];
+    }
+}
+template <int K>
+__global__ void k_store_dofs(uint32_t n, uint32_t k_used, const double* __restrict__ src,
+                             double* __restrict__ dst) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        for (uint32_t k = 0; k < k_used; ++k) dst[(size_t)k * n + j] = src[(size_t)j * K + k];
+}
+
+}  // namespace wgpu

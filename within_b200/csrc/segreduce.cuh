@@ -1,0 +1,188 @@
+// segreduce.cuh -- deterministic, load-balanced segmented reduction.
+//
+// One engine serves every "sum the entries of each segment" step of the solve:
+// the adjoint scatter D^T u (segments = levels of a term, positions = the
+// term's level-sorted observation order), the cross-block SpMVs of the block
+// elimination (segments = CSR rows, positions = non-zeros), the Schwarz
+// restrict/mean/prolongation combines and the rounds of the triangular solves.
+//
+// Positions are cut into fixed tiles of T = 256*ITEMS entries, one CTA per
+// tile, so work is balanced no matter how the segment lengths are distributed
+// (a Pareto firm of 10^6 rows costs the same per row as a worker of 10).  A CTA
+// loads its tile (coalesced where the value functor reads contiguously), runs
+// a block-wide segmented inclusive scan (CUB BlockScan) and emits every segment
+// that starts and ends inside the tile.  A segment that crosses tiles leaves a
+// tail partial (its owner tile) and head partials (the tiles it continues into);
+// the last of those CTAs to finish -- decided by one atomic counter per split
+// segment, not a wait -- adds them in tile order and emits.  Every sum is
+// therefore formed in one fixed order: results are bitwise reproducible run to
+// run, with no floating-point atomics.
+//
+// The tile/split tables are built once on the host (HostPlan::add) from the
+// segment pointer arrays, which never change after set-up.
+#pragma once
+#include <cstdint>
+#include <cub/block/block_scan.cuh>
+
+#include "segplan.hpp"
+
+namespace wgpu {
+
+template <int K>
+struct SegItem {
+    double v[K];
+    int f;  // 1 = a segment starts at this position
+};
+
+template <int K>
+struct SegSumOp {
+    __device__ __forceinline__ SegItem<K> operator()(const SegItem<K>& a, const SegItem<K>& b) const {
+        if (b.f) return b;
+        SegItem<K> c;
+#pragma unroll
+        for (int k = 0; k < K; ++k) c.v[k] = a.v[k] + b.v[k];
+        c.f = a.f;
+        return c;
+    }
+};
+
+template <int K>
+constexpr int sr_items() { return K >= 8 ? 1 : (K >= 4 ? 2 : (K >= 2 ? 4 : 8)); }
+template <int K>
+constexpr int sr_tile() { return SR_THREADS * sr_items<K>(); }
+
+// F provides:
+//   using Prob = ...;                 (trivially copyable, <= 256 bytes)
+//   const Prob* probs;                (device array)
+//   __device__ const uint32_t* seg_ptr(const Prob&) const;
+//   __device__ void value(const Prob&, uint32_t pos, double (&v)[K]) const;
+//   __device__ void emit(const Prob&, uint32_t seg, const double (&s)[K]) const;
+template <class F, int K>
+__global__ void __launch_bounds__(SR_THREADS)
+segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
+                 const SRSplit* __restrict__ splits, double* __restrict__ head_buf,
+                 double* __restrict__ tail_buf, unsigned* __restrict__ counters,
+                 const int* __restrict__ skip) {
+    constexpr int ITEMS = sr_items<K>();
+    constexpr int T = SR_THREADS * ITEMS;
+    using Prob = typename F::Prob;
+    using Scan = cub::BlockScan<SegItem<K>, SR_THREADS>;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ double sv[T * K];
+    __shared__ unsigned char flags[T];
+    __shared__ SRTile tile;
+    __shared__ Prob prob;
+    __shared__ int last_split[2];
+
+    if (skip && *skip) return;
+    const int tid = threadIdx.x;
+    const uint32_t gtile = tile_base + blockIdx.x;   // global tile id
+    if (tid == 0) {
+        tile = tiles[gtile];
+        prob = f.probs[tile.problem];
+    }
+    for (int i = tid; i < T; i += SR_THREADS) flags[i] = 0;
+    __syncthreads();
+    const uint32_t p0 = tile.p0, p1 = tile.p1;
+    const uint32_t* ptr = f.seg_ptr(prob);
+    for (uint32_t s = tile.own_lo + tid; s < tile.own_hi; s += SR_THREADS) {
+        uint32_t a = ptr[s], b = ptr[s + 1];
+        if (b > a) flags[a - p0] = 1;
+    }
+    __syncthreads();
+
+    SegItem<K> it[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        uint32_t p = (uint32_t)(tid * ITEMS + i);
+        if (p0 + p < p1) {
+            double v[K];
+            f.value(prob, p0 + p, v);
+#pragma unroll
+            for (int k = 0; k < K; ++k) it[i].v[k] = v[k];
+            it[i].f = flags[p];
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) it[i].v[k] = 0.0;
+            it[i].f = 1;
+        }
+    }
+    Scan(scan_tmp).InclusiveScan(it, it, SegSumOp<K>());
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i)
+#pragma unroll
+        for (int k = 0; k < K; ++k) sv[(tid * ITEMS + i) * K + k] = it[i].v[k];
+    __syncthreads();
+
+    for (uint32_t s = tile.own_lo + tid; s < tile.own_hi; s += SR_THREADS) {
+        uint32_t a = ptr[s], b = ptr[s + 1];
+        double out[K];
+        if (b == a) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) out[k] = 0.0;
+            f.emit(prob, s, out);
+        } else if (b <= p1) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) out[k] = sv[(b - 1 - p0) * K + k];
+            f.emit(prob, s, out);
+        } else {
+            // the one owned segment that runs past the tile: tail partial
+#pragma unroll
+            for (int k = 0; k < K; ++k) tail_buf[(size_t)tile.tail_split * K + k] = sv[(p1 - 1 - p0) * K + k];
+            __threadfence();
+        }
+    }
+    if (tid == 0 && tile.cont_split >= 0) {
+        const SRSplit sp = splits[tile.cont_split];
+        uint32_t e = ptr[sp.seg + 1];
+        uint32_t last = (e < p1 ? e : p1) - 1 - p0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) head_buf[(size_t)gtile * K + k] = sv[last * K + k];
+        __threadfence();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int ids[2] = {tile.cont_split, tile.tail_split};
+        for (int j = 0; j < 2; ++j) {
+            last_split[j] = -1;
+            int id = ids[j];
+            if (id < 0) continue;
+            const SRSplit sp = splits[id];
+            unsigned total = sp.t1 - sp.t0 + 1;
+            unsigned prev = atomicAdd(&counters[id], 1u);
+            if (prev == total - 1) last_split[j] = id;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int j = 0; j < 2; ++j) {
+            int id = last_split[j];
+            if (id < 0) continue;
+            __threadfence();
+            const SRSplit sp = splits[id];
+            double acc[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = __ldcg(&tail_buf[(size_t)id * K + k]);
+            for (uint32_t t = sp.t0 + 1; t <= sp.t1; ++t)
+#pragma unroll
+                for (int k = 0; k < K; ++k) acc[k] += __ldcg(&head_buf[(size_t)t * K + k]);
+            Prob pr = (sp.problem == tile.problem) ? prob : f.probs[sp.problem];
+            f.emit(pr, sp.seg, acc);
+            counters[id] = 0;
+        }
+    }
+}
+
+// Host-side plan of one launch (device arrays).
+struct SRPlan {
+    int n_tiles = 0;
+    int n_splits = 0;
+    SRTile* tiles = nullptr;
+    SRSplit* splits = nullptr;
+    double* head_buf = nullptr;   // n_tiles * K
+    double* tail_buf = nullptr;   // n_splits * K
+    unsigned* counters = nullptr; // n_splits
+    int K = 1;
+};
+
+}  // namespace wgpu

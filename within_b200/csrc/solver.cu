@@ -1,0 +1,1007 @@
+// solver.cu -- the Solver (crates/within/src/solver.rs) on one B200: set-up,
+// the device-resident LSMR loop and the C ABI declared in include/within_gpu.h.
+//
+// A solve of k right-hand sides runs as one multi-RHS modified LSMR
+// (crates/schwarz-precond/src/lsmr.rs:206-295): every iteration is a fixed
+// sequence of kernels on one stream --
+//   gather+update (u <- A v + s u, beta)      k_gather_update
+//   scatter A^T u with the p~ epilogue       segreduce<ScatterF>, one launch
+//   preconditioner v = M^-1 p~               diagonal kernel / Schwarz chain
+//   alpha, Givens recurrences, stop test     k_alpha_step (last block)
+//   v, h, h_bar, x update                    k_solution_update
+// -- with all scalar state on the device, so the host never waits inside an
+// iteration.  Two iterations (both state parities) are captured in a CUDA
+// graph that is replayed in bursts; a finished column stops updating and once
+// every column has finished the kernels return at entry.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/within_gpu.h"
+#include "host.hpp"
+#include "kernels.cuh"
+
+using namespace wgpu;
+
+namespace {
+
+thread_local std::string g_err;
+thread_local uint64_t g_launches = 0;
+
+#define CK(x)                                                                          \
+    do {                                                                               \
+        cudaError_t e_ = (x);                                                          \
+        if (e_ != cudaSuccess)                                                         \
+            throw WError(ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int grid_for(uint64_t n, int threads, int cap) {
+    uint64_t b = (n + threads - 1) / threads;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)cap));
+}
+
+// Simple owner of device allocations.
+struct Arena {
+    std::vector<void*> ptrs;
+    template <class T>
+    T* alloc(size_t n) {
+        if (n == 0) n = 1;
+        void* p = nullptr;
+        CK(cudaMalloc(&p, n * sizeof(T)));
+        CK(cudaMemset(p, 0, n * sizeof(T)));
+        ptrs.push_back(p);
+        return (T*)p;
+    }
+    template <class T>
+    T* upload(const std::vector<T>& v) {
+        T* p = alloc<T>(v.size());
+        if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return p;
+    }
+    ~Arena() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+// A segmented-reduction launch set on device.
+struct DevPlan {
+    SRTile* tiles = nullptr;
+    SRSplit* splits = nullptr;
+    double* head = nullptr;
+    double* tail = nullptr;
+    unsigned* counters = nullptr;
+    uint32_t n_tiles = 0;
+    std::vector<uint32_t> range_lo, range_hi;   // tile ranges (per round, for round plans)
+};
+
+DevPlan make_plan(Arena& A, const HostPlan& hp, int K) {
+    DevPlan d;
+    d.n_tiles = (uint32_t)hp.tiles.size();
+    d.tiles = A.upload(hp.tiles);
+    d.splits = A.upload(hp.splits);
+    d.head = A.alloc<double>((size_t)d.n_tiles * K);
+    d.tail = A.alloc<double>(std::max<size_t>(1, hp.splits.size()) * K);
+    d.counters = A.alloc<unsigned>(std::max<size_t>(1, hp.splits.size()));
+    return d;
+}
+
+template <class F, int K>
+void launch_sr(const F& f, const DevPlan& p, uint32_t lo, uint32_t hi, const int* skip, cudaStream_t st) {
+    if (hi <= lo) return;
+    segreduce_kernel<F, K><<<hi - lo, SR_THREADS, 0, st>>>(f, p.tiles, lo, p.splits, p.head, p.tail,
+                                                           p.counters, skip);
+    ++g_launches;
+}
+
+int k_bucket(uint64_t k) { return k <= 1 ? 1 : k <= 2 ? 2 : k <= 4 ? 4 : 8; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct within_design {
+    std::vector<std::vector<uint32_t>> levels;
+    std::vector<std::vector<double>> slopes;
+    std::vector<int> intercept;
+    std::vector<std::vector<size_t>> slope_of;   // per effect: indices into slopes
+    uint64_t n_obs = 0, n_dofs = 0;
+};
+
+// Shared, immutable preconditioner state on the device.
+struct within_preconditioner {
+    int device = 0;
+    int kind = 0;   // 1 additive, 2 diagonal
+    uint32_t n = 0;
+    Arena arena;
+    double* inv_diag = nullptr;
+    SchwarzHost host;            // kept for plan building and statistics
+    SchwarzDev dev_const{};      // pointers into arena (work pointers filled per user)
+    // per-step segment problems
+    SegProb *p_restrict = nullptr, *p_ct = nullptr, *p_kept = nullptr, *p_dense = nullptr,
+            *p_fwd = nullptr, *p_bwd = nullptr, *p_c = nullptr, *p_prolong = nullptr;
+    bool has_dense = false;
+    uint32_t n_rounds = 0;
+    std::mutex mu;
+    std::atomic<int> refs{1};
+    struct SchwarzUser* standalone = nullptr;   // plans + work of Preconditioner::apply
+    ~within_preconditioner();
+};
+
+namespace {
+
+int kidx(int K) { return K == 1 ? 0 : K == 2 ? 1 : K == 4 ? 2 : 3; }
+
+void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
+    Arena& A = P.arena;
+    P.host = std::move(S);
+    SchwarzHost& H = P.host;
+    SchwarzDev& D = P.dev_const;
+    D.n_sub = H.n_sub;
+    D.loc_ptr = A.upload(H.loc_ptr);
+    D.n_elim = A.upload(H.n_elim);
+    D.red_off = A.upload(H.red_off);
+    D.n_kept = A.upload(H.n_kept);
+    D.red_n = A.upload(H.red_n);
+    D.mode = A.upload(H.mode);
+    D.glob = A.upload(H.glob);
+    D.scale = A.upload(H.scale);
+    D.slot_sub = A.upload(H.slot_sub);
+    D.inv_e = A.upload(H.inv_e);
+    D.ct_col = A.upload(H.ct_col);
+    D.ct_val = A.upload(H.ct_val);
+    D.ct_row_slot = A.upload(H.ct_row_slot);
+    D.ct_row_red = A.upload(H.ct_row_red);
+    D.elim_slot = A.upload(H.elim_slot);
+    D.c_col = A.upload(H.c_col);
+    D.c_val = A.upload(H.c_val);
+    D.red_sub = A.upload(H.red_sub);
+    D.dense_row_slot = A.upload(H.dense_row_slot);
+    D.dense_col = A.upload(H.dense_col);
+    D.dense_val = A.upload(H.dense_val);
+    D.dinv = A.upload(H.dinv);
+    D.fwd_row = A.upload(H.fwd_row);
+    D.fwd_col = A.upload(H.fwd_col);
+    D.fwd_val = A.upload(H.fwd_val);
+    D.bwd_row = A.upload(H.bwd_row);
+    D.bwd_col = A.upload(H.bwd_col);
+    D.bwd_val = A.upload(H.bwd_val);
+    D.dof_slot = A.upload(H.dof_slot);
+    D.kept_ptr = A.upload(H.kept_ptr);
+    uint32_t* loc_ptr = const_cast<uint32_t*>(D.loc_ptr);
+    uint32_t* ct_ptr = A.upload(H.ct_ptr);
+    uint32_t* kept_ptr = const_cast<uint32_t*>(D.kept_ptr);
+    uint32_t* dense_ptr = A.upload(H.dense_rows_ptr);
+    uint32_t* fwd_ptr = A.upload(H.fwd_ptr);
+    uint32_t* bwd_ptr = A.upload(H.bwd_ptr);
+    uint32_t* c_ptr = A.upload(H.c_ptr);
+    uint32_t* dof_ptr = A.upload(H.dof_ptr);
+    auto one = [&](uint32_t* ptr) { return A.upload(std::vector<SegProb>{SegProb{ptr, 0, 0}}); };
+    P.p_restrict = one(loc_ptr);
+    P.p_ct = one(ct_ptr);
+    P.p_kept = one(kept_ptr);
+    P.p_dense = one(dense_ptr);
+    P.p_c = one(c_ptr);
+    P.p_prolong = one(dof_ptr);
+    P.has_dense = H.dense_rows_ptr.size() > 1;
+    P.n_rounds = H.n_rounds;
+    std::vector<SegProb> fw, bw;
+    for (uint32_t r = 0; r < H.n_rounds; ++r) {
+        fw.push_back(SegProb{fwd_ptr + H.fwd_round_ptr[r], H.fwd_round_ptr[r], 0});
+        bw.push_back(SegProb{bwd_ptr + H.bwd_round_ptr[r], H.bwd_round_ptr[r], 0});
+    }
+    P.p_fwd = A.upload(fw);
+    P.p_bwd = A.upload(bw);
+}
+
+// Schwarz work buffers of one user (solver) for K columns.
+struct SchwarzWork {
+    double *rl = nullptr, *sl = nullptr, *rb = nullptr, *yv = nullptr, *xv = nullptr, *m1 = nullptr,
+           *m2 = nullptr, *m3 = nullptr;
+};
+
+// Everything one user of a (possibly shared) preconditioner mutates: the tile
+// plans' partial/counter buffers and the work vectors, per column bucket K.
+struct KPlans {
+    DevPlan restrict_, ct, kept, dense, fwd, bwd, c, prolong;
+    SchwarzWork w;
+    bool ready = false;
+};
+
+}  // namespace
+
+struct SchwarzUser {
+    Arena arena;
+    KPlans kp[4];
+};
+
+within_preconditioner::~within_preconditioner() { delete standalone; }
+
+namespace {
+
+KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K) {
+    KPlans& kp = U.kp[kidx(K)];
+    if (kp.ready) return kp;
+    const SchwarzHost& H = P.host;
+    Arena& A = U.arena;
+    const int T = K == 1 ? sr_tile<1>() : K == 2 ? sr_tile<2>() : K == 4 ? sr_tile<4>() : sr_tile<8>();
+    auto one = [&](const std::vector<uint32_t>& ptr) {
+        HostPlan hp;
+        hp.add(0, ptr.data(), (uint32_t)ptr.size() - 1, T);
+        DevPlan d = make_plan(A, hp, K);
+        d.range_lo = {0};
+        d.range_hi = {d.n_tiles};
+        return d;
+    };
+    kp.restrict_ = one(H.loc_ptr);
+    kp.ct = one(H.ct_ptr);
+    kp.kept = one(H.kept_ptr);
+    kp.dense = one(H.dense_rows_ptr);
+    kp.c = one(H.c_ptr);
+    kp.prolong = one(H.dof_ptr);
+    auto rounds = [&](const std::vector<uint32_t>& rptr, const std::vector<uint32_t>& ptr) {
+        HostPlan hp;
+        std::vector<uint32_t> lo, hi;
+        for (uint32_t r = 0; r + 1 < rptr.size(); ++r) {
+            lo.push_back((uint32_t)hp.tiles.size());
+            hp.add(r, ptr.data() + rptr[r], rptr[r + 1] - rptr[r], T);
+            hi.push_back((uint32_t)hp.tiles.size());
+        }
+        DevPlan d = make_plan(A, hp, K);
+        d.range_lo = lo;
+        d.range_hi = hi;
+        return d;
+    };
+    kp.fwd = rounds(H.fwd_round_ptr, H.fwd_ptr);
+    kp.bwd = rounds(H.bwd_round_ptr, H.bwd_ptr);
+    size_t nl = H.glob.size(), nr = H.n_red, ns = H.n_sub;
+    kp.w.rl = A.alloc<double>(nl * K);
+    kp.w.sl = A.alloc<double>(nl * K);
+    kp.w.rb = A.alloc<double>(nr * K);
+    kp.w.yv = A.alloc<double>(nr * K);
+    kp.w.xv = A.alloc<double>(nr * K);
+    kp.w.m1 = A.alloc<double>(ns * K);
+    kp.w.m2 = A.alloc<double>(ns * K);
+    kp.w.m3 = A.alloc<double>(ns * K);
+    kp.ready = true;
+    return kp;
+}
+
+template <int K>
+void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const double* r, double* z, const int* skip,
+                   cudaStream_t st) {
+    KPlans& kp = schwarz_user_plans(U, P, K);
+    SchwarzDev S = P.dev_const;
+    S.rl = kp.w.rl;
+    S.sl = kp.w.sl;
+    S.rb = kp.w.rb;
+    S.yv = kp.w.yv;
+    S.xv = kp.w.xv;
+    S.m1 = kp.w.m1;
+    S.m2 = kp.w.m2;
+    S.m3 = kp.w.m3;
+    launch_sr<RestrictF<K>, K>(RestrictF<K>{P.p_restrict, S, r}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
+    launch_sr<CtF<K>, K>(CtF<K>{P.p_ct, S}, kp.ct, 0, kp.ct.n_tiles, skip, st);
+    launch_sr<KeptSumF<K>, K>(KeptSumF<K>{P.p_kept, S}, kp.kept, 0, kp.kept.n_tiles, skip, st);
+    if (P.has_dense) launch_sr<DenseF<K>, K>(DenseF<K>{P.p_dense, S}, kp.dense, 0, kp.dense.n_tiles, skip, st);
+    for (uint32_t r = 0; r < P.n_rounds; ++r)
+        launch_sr<FwdF<K>, K>(FwdF<K>{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
+    for (uint32_t r = P.n_rounds; r-- > 0;)
+        launch_sr<BwdF<K>, K>(BwdF<K>{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
+    launch_sr<CF<K>, K>(CF<K>{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
+    launch_sr<MeanF<K>, K>(MeanF<K>{P.p_restrict, S}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
+    launch_sr<ProlongF<K>, K>(ProlongF<K>{P.p_prolong, S, z}, kp.prolong, 0, kp.prolong.n_tiles, skip, st);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct within_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    HostDesign design;
+    Reparam reparam;
+    uint64_t n_obs = 0, n_dofs = 0;
+    uint64_t n_warnings = 0;
+    within_preconditioner* precond = nullptr;
+    int precision = WITHIN_PRECISION_FP64;
+    std::mutex mu;
+    Arena arena;
+    // design on device
+    OpParams op{};
+    uint32_t* perm = nullptr;               // internal -> caller (nullptr = identity)
+    std::vector<ScatterProb> scatter_host;  // problems (same for all K)
+    ScatterProb* scatter_probs = nullptr;
+    std::vector<std::vector<uint32_t>> level_ptr_host;   // per term
+    DevPlan scatter_plan[4];
+    bool scatter_ready[4] = {false, false, false, false};
+    // workspaces per K
+    struct Work {
+        bool ready = false;
+        double *u, *b, *yint, *v, *p, *h, *hb, *x, *dm;
+        double* partials;
+        unsigned* counter;
+        double* bmax;
+        int* nonfinite;
+        ColState* st;   // [2][K]
+        Ctl* ctl;
+        cudaGraphExec_t graph = nullptr;
+        uint64_t graph_iters = 0;
+    } work[4];
+    // pinned staging for the host entry points
+    double* pin = nullptr;
+    size_t pin_n = 0;
+    SchwarzUser schwarz;   // this solver's plans/work for the preconditioner
+
+    ~within_solver() {
+        for (auto& w : work)
+            if (w.graph) cudaGraphExecDestroy(w.graph);
+        if (pin) cudaFreeHost(pin);
+        if (stream) cudaStreamDestroy(stream);
+        if (precond && --precond->refs == 0) delete precond;
+    }
+};
+
+namespace {
+
+constexpr int RED_GRID = 148 * 4;    // fixed reduction grid: deterministic partial order
+
+void set_device(int dev) { CK(cudaSetDevice(dev)); }
+
+void ensure_scatter(within_solver& s, int K) {
+    int ki = kidx(K);
+    if (s.scatter_ready[ki]) return;
+    const int T = K == 1 ? sr_tile<1>() : K == 2 ? sr_tile<2>() : K == 4 ? sr_tile<4>() : sr_tile<8>();
+    HostPlan hp;
+    uint32_t prob = 0;
+    for (size_t t = 0; t < s.design.terms.size(); ++t) {
+        const auto& lp = s.level_ptr_host[t];
+        for (size_t c = 0; c < s.design.terms[t].cols.size(); ++c)
+            hp.add(prob++, lp.data(), (uint32_t)lp.size() - 1, T);
+    }
+    s.scatter_plan[ki] = make_plan(s.arena, hp, K);
+    s.scatter_ready[ki] = true;
+}
+
+within_solver::Work& ensure_work(within_solver& s, int K) {
+    auto& w = s.work[kidx(K)];
+    if (w.ready) return w;
+    Arena& A = s.arena;
+    w.u = A.alloc<double>(s.n_obs * K);
+    w.b = A.alloc<double>(s.n_obs * K);
+    w.yint = A.alloc<double>(s.n_obs * K);
+    w.dm = A.alloc<double>(s.n_obs * K);
+    w.v = A.alloc<double>(s.n_dofs * K);
+    w.p = A.alloc<double>(s.n_dofs * K);
+    w.h = A.alloc<double>(s.n_dofs * K);
+    w.hb = A.alloc<double>(s.n_dofs * K);
+    w.x = A.alloc<double>(s.n_dofs * K);
+    w.partials = A.alloc<double>((size_t)RED_GRID * 3 * 8);
+    w.counter = A.alloc<unsigned>(1);
+    w.bmax = A.alloc<double>(8);
+    w.nonfinite = A.alloc<int>(1);
+    w.st = A.alloc<ColState>(2 * 8);
+    w.ctl = A.alloc<Ctl>(1);
+    if (s.precond && s.precond->kind == 1) schwarz_user_plans(s.schwarz, *s.precond, K);
+    ensure_scatter(s, K);
+    w.ready = true;
+    return w;
+}
+
+template <int K, int EPI>
+void scatter(within_solver& s, const double* u, double* out, const ColState* cur, const int* skip,
+             cudaStream_t st) {
+    const DevPlan& pl = s.scatter_plan[kidx(K)];
+    ScatterF<K, EPI> f{s.scatter_probs, u, s.op.sqrt_w, out, cur};
+    launch_sr<ScatterF<K, EPI>, K>(f, pl, 0, pl.n_tiles, skip, st);
+}
+
+template <int K>
+void precond_apply(within_solver& s, within_solver::Work& w, const double* p, double* v, const int* skip,
+                   cudaStream_t st) {
+    const uint32_t nd = (uint32_t)s.n_dofs;
+    if (!s.precond) {
+        k_diag_apply<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, nullptr, p, v, skip ? w.ctl : nullptr);
+        ++g_launches;
+    } else if (s.precond->kind == 2) {
+        k_diag_apply<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, s.precond->inv_diag, p, v,
+                                                                    skip ? w.ctl : nullptr);
+        ++g_launches;
+    } else {
+        schwarz_apply<K>(*s.precond, s.schwarz, p, v, skip, st);
+    }
+}
+
+// one LSMR iteration at state parity `par`
+template <int K>
+void iteration(within_solver& s, within_solver::Work& w, int par, cudaStream_t st) {
+    ColState* cur = w.st + (size_t)par * 8;
+    ColState* nxt = w.st + (size_t)(1 - par) * 8;
+    const uint32_t n = (uint32_t)s.n_obs, nd = (uint32_t)s.n_dofs;
+    const int* skip = &w.ctl->all_done;
+    k_gather_update<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, w.v, w.u, cur, w.ctl, w.partials, w.counter);
+    ++g_launches;
+    scatter<K, 1>(s, w.u, w.p, cur, skip, st);
+    precond_apply<K>(s, w, w.p, w.v, skip, st);
+    k_alpha_step<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, cur, nxt, w.ctl, w.partials, w.counter);
+    ++g_launches;
+    k_solution_update<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, nxt, w.ctl);
+    ++g_launches;
+    (void)n;
+}
+
+template <int K>
+void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_t k_used, double tol,
+              uint64_t maxiter, double* X_out, double* D_out, within_solve_stats* stats, cudaStream_t st,
+              double t_setup0) {
+    const uint32_t n = (uint32_t)s.n_obs, nd = (uint32_t)s.n_dofs;
+    CK(cudaMemsetAsync(w.nonfinite, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(w.ctl, 0, sizeof(Ctl), st));
+    k_load_rhs<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, k_used, Y, s.perm, s.op.sqrt_w, w.yint, w.b,
+                                                    w.partials, w.counter, w.bmax, w.nonfinite);
+    int nonfinite = 0;
+    CK(cudaMemcpyAsync(&nonfinite, w.nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (nonfinite) throw WError(ERR_INVALID, "response must be finite (a non-finite value was found)");
+    const double t_solve0 = now_s();
+    k_norm_b<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
+                                                  w.ctl, w.partials, w.counter);
+    k_scale_u<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, w.b, w.u, w.st);
+    scatter<K, 0>(s, w.u, w.p, w.st, nullptr, st);
+    precond_apply<K>(s, w, w.p, w.v, nullptr, st);
+    k_alpha_init<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, w.st, w.st + 8, w.ctl, w.partials,
+                                                      w.counter);
+    k_init_vectors<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, w.st);
+    g_launches += 6;
+    // capture two iterations once per workspace
+    if (!w.graph) {
+        cudaStream_t cs;
+        CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        uint64_t before = g_launches;
+        iteration<K>(s, w, 0, cs);
+        iteration<K>(s, w, 1, cs);
+        w.graph_iters = g_launches - before;
+        g_launches = before;
+        CK(cudaStreamEndCapture(cs, &g));
+        CK(cudaGraphInstantiate(&w.graph, g, 0));
+        CK(cudaGraphDestroy(g));
+        CK(cudaStreamDestroy(cs));
+    }
+    Ctl ctl{};
+    uint64_t done_iters = 0;
+    uint64_t burst = 2;
+    while (true) {
+        for (uint64_t b = 0; b < burst; ++b) {
+            CK(cudaGraphLaunch(w.graph, st));
+            g_launches += w.graph_iters;
+        }
+        done_iters += 2 * burst;
+        CK(cudaMemcpyAsync(&ctl, w.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (ctl.all_done || ctl.err || done_iters >= maxiter + 2) break;
+        burst = std::min<uint64_t>(burst * 2, 32);
+        uint64_t left = (maxiter + 2 - done_iters + 1) / 2;
+        burst = std::max<uint64_t>(1, std::min(burst, left));
+    }
+    if (ctl.err == 5)
+        throw WError(ERR_INDEFINITE, "mlsmr: preconditioner not positive definite (<v, Mv> < 0)");
+    const double t_solve1 = now_s();
+    // results
+    k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, w.x, w.yint, w.dm);
+    ++g_launches;
+    if (D_out) {
+        k_store_obs<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, k_used, w.dm, s.perm, D_out);
+        ++g_launches;
+    }
+    if (X_out) {
+        k_store_dofs<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, k_used, w.x, X_out);
+        ++g_launches;
+    }
+    ColState fin[8];
+    // the state parity after the loop is whichever buffer was written last:
+    // both buffers hold identical done states for finished columns, so read
+    // the one with the larger iteration count.
+    ColState a[8], b2[8];
+    CK(cudaMemcpyAsync(a, w.st, sizeof(ColState) * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(b2, w.st + 8, sizeof(ColState) * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < 8; ++k) fin[k] = a[k].itn >= b2[k].itn ? a[k] : b2[k];
+    const double t_end = now_s();
+    if (stats)
+        for (uint32_t k = 0; k < k_used; ++k) {
+            const ColState& c = fin[k];
+            within_solve_stats& o = stats[k];
+            o.converged = (c.stop == STOP_RESID || c.stop == STOP_NORMAL || c.stop == STOP_ZERO_RHS ||
+                           c.stop == STOP_INIT_ZERO) ? 1 : 0;
+            o.iterations = (uint64_t)c.itn;
+            o.residual = (c.stop == STOP_ZERO_RHS || c.stop == STOP_INIT_ZERO) ? 0.0 : fabs(c.zeta_bar) / c.zeta0;
+            o.time_setup = t_solve0 - t_setup0;
+            o.time_solve = t_solve1 - t_solve0;
+            o.time_total = t_end - t_setup0;
+        }
+}
+
+void dispatch_solve(within_solver& s, const double* Y_dev, uint64_t k, double tol, uint64_t maxiter,
+                    double* X_dev, double* D_dev, within_solve_stats* stats, cudaStream_t st) {
+    const double t0 = now_s();
+    for (uint64_t c0 = 0; c0 < k; c0 += 8) {
+        const uint32_t kk = (uint32_t)std::min<uint64_t>(8, k - c0);
+        const int K = k_bucket(kk);
+        auto& w = ensure_work(s, K);
+        const double* Y = Y_dev + c0 * s.n_obs;
+        double* X = X_dev ? X_dev + c0 * s.n_dofs : nullptr;
+        double* D = D_dev ? D_dev + c0 * s.n_obs : nullptr;
+        within_solve_stats* S = stats ? stats + c0 : nullptr;
+        switch (K) {
+            case 1: run_lsmr<1>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+            case 2: run_lsmr<2>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+            case 4: run_lsmr<4>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+            default: run_lsmr<8>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+        }
+    }
+}
+
+void validate_opts(const within_lsmr_options* o, double& tol, uint64_t& maxiter, uint64_t& local_size) {
+    tol = 1e-8;
+    maxiter = 1000;
+    local_size = 0;
+    if (o) {
+        tol = o->tol;
+        maxiter = o->maxiter;
+        local_size = o->local_size;
+    }
+    if (!std::isfinite(tol) || tol < 0.0)
+        throw WError(ERR_INVALID, "tolerance must be finite and nonnegative, got " + std::to_string(tol));
+    if (local_size != 0)
+        throw WError(ERR_UNSUPPORTED, "local_size (windowed reorthogonalisation) is not supported by this build");
+}
+
+template <class F>
+int guarded(F f) {
+    try {
+        f();
+        return WITHIN_OK;
+    } catch (const WError& e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_err = "host allocation failed";
+        return WITHIN_ERR_CUDA;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return WITHIN_ERR_CUDA;
+    }
+}
+
+within_solver* make_solver(const within_design* d, const double* weights, const within_precond_config* cfg,
+                           const within_preconditioner* prebuilt, int device) {
+    if (!d) throw WError(ERR_INVALID, "design is NULL");
+    if (device < 0) CK(cudaGetDevice(&device));
+    set_device(device);
+    auto s = std::make_unique<within_solver>();
+    s->device = device;
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    std::vector<EffectIn> effs;
+    for (size_t e = 0; e < d->levels.size(); ++e) {
+        EffectIn ef;
+        ef.levels = d->levels[e].data();
+        ef.intercept = d->intercept[e] != 0;
+        for (size_t j : d->slope_of[e]) ef.slopes.push_back(d->slopes[j].data());
+        effs.push_back(ef);
+    }
+    s->design = make_design(d->n_obs, effs);
+    HostDesign& D = s->design;
+    s->n_obs = D.n_obs;
+    s->n_dofs = D.n_dofs;
+    // Design::validate_weights (domain.rs:261-279), then permute in
+    std::vector<double> w;
+    if (weights) {
+        for (uint64_t i = 0; i < D.n_obs; ++i)
+            if (!(weights[i] >= 0.0 && std::isfinite(weights[i])))
+                throw WError(ERR_BUILD, "weight at index " + std::to_string(i) +
+                                            " must be finite and non-negative, got " + std::to_string(weights[i]));
+        w.resize(D.n_obs);
+        for (uint64_t i = 0; i < D.n_obs; ++i) w[i] = D.obs_perm.empty() ? weights[i] : weights[D.obs_perm[i]];
+    }
+    s->reparam = build_reparam(D, weights ? w.data() : nullptr);
+    // preconditioner (operator/schwarz.rs:231-270)
+    if (prebuilt) {
+        if (prebuilt->n != D.n_dofs)
+            throw WError(ERR_DIMENSION, "prebuilt preconditioner shape (" + std::to_string(prebuilt->n) + "x" +
+                                            std::to_string(prebuilt->n) + ") does not match design DOF count " +
+                                            std::to_string(D.n_dofs));
+        if (prebuilt->device != device) throw WError(ERR_INVALID, "prebuilt preconditioner lives on another device");
+        s->precond = const_cast<within_preconditioner*>(prebuilt);
+        ++s->precond->refs;
+    } else {
+        PrecondCfg pc;
+        if (cfg) {
+            pc.kind = cfg->kind;
+            pc.ac_seed = cfg->approx_chol_seed;
+            pc.ac_split = cfg->approx_chol_split;
+            pc.schur_exact = cfg->schur_exact != 0;
+            pc.schur_seed = cfg->schur_seed;
+            pc.schur_split = std::max<uint32_t>(1, cfg->schur_split);
+            pc.dense_threshold = cfg->dense_threshold;
+            pc.scaling_tol = cfg->scaling_tolerance;
+            pc.scaling_max_sweeps = cfg->scaling_max_sweeps;
+            pc.scaling_error = cfg->scaling_error != 0;
+            if (pc.kind < 0 || pc.kind > 2) throw WError(ERR_INVALID, "unknown preconditioner kind");
+        }
+        BuildResult br = build_preconditioner(D, weights ? w.data() : nullptr, pc);
+        s->n_warnings = br.n_warnings;
+        if (br.kind != 0) {
+            auto* P = new within_preconditioner();
+            P->device = device;
+            P->kind = br.kind;
+            P->n = (uint32_t)D.n_dofs;
+            try {
+                if (br.kind == 2) P->inv_diag = P->arena.upload(br.inv_diag);
+                else upload_schwarz(*P, std::move(br.schwarz));
+            } catch (...) {
+                delete P;
+                throw;
+            }
+            s->precond = P;
+        }
+    }
+    // design operator on the device
+    Arena& A = s->arena;
+    OpParams& op = s->op;
+    op.n = (uint32_t)D.n_obs;
+    op.Q = (int)D.terms.size();
+    for (size_t k = 0; k < D.loads.size(); ++k) op.loads[k] = A.upload(D.loads[k]);
+    for (int t = 0; t < op.Q; ++t) {
+        const Term& T = D.terms[t];
+        op.codes[t] = A.upload(D.codes[t]);
+        op.off[t] = T.offset;
+        op.L[t] = T.n_levels;
+        op.ncol[t] = (int)T.cols.size();
+        for (size_t c = 0; c < T.cols.size(); ++c) op.load[t][c] = T.cols[c];
+    }
+    if (weights) {
+        std::vector<double> sw(w);
+        for (double& x : sw) x = std::sqrt(x);
+        op.sqrt_w = A.upload(sw);
+    }
+    if (!D.obs_perm.empty()) s->perm = A.upload(D.obs_perm);
+    // scatter problems: level-sorted order per term (identity when sorted)
+    s->level_ptr_host.resize(op.Q);
+    for (int t = 0; t < op.Q; ++t) {
+        const Term& T = D.terms[t];
+        const auto& codes = D.codes[t];
+        std::vector<uint32_t>& lp = s->level_ptr_host[t];
+        lp.assign((size_t)T.n_levels + 1, 0);
+        for (uint32_t c : codes) ++lp[(size_t)c + 1];
+        for (uint32_t l = 0; l < T.n_levels; ++l) lp[l + 1] += lp[l];
+        uint32_t* dlp = A.upload(lp);
+        uint32_t* order = nullptr;
+        if (!T.sorted) {
+            std::vector<uint32_t> perm(D.n_obs);
+            stable_argsort_u32(codes.data(), D.n_obs, T.n_levels, perm.data());
+            order = A.upload(perm);
+        }
+        for (size_t c = 0; c < T.cols.size(); ++c) {
+            ScatterProb sp{};
+            sp.seg_ptr = dlp;
+            sp.order = order;
+            sp.load = T.cols[c] < 0 ? nullptr : op.loads[T.cols[c]];
+            sp.out_off = (uint32_t)(T.offset + c * T.n_levels);
+            s->scatter_host.push_back(sp);
+        }
+    }
+    s->scatter_probs = A.upload(s->scatter_host);
+    CK(cudaDeviceSynchronize());
+    return s.release();
+}
+
+void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr_options* opts, double* X,
+                double* Dm, within_solve_stats* stats) {
+    double tol;
+    uint64_t maxiter, ls;
+    validate_opts(opts, tol, maxiter, ls);
+    std::lock_guard<std::mutex> g(s.mu);
+    set_device(s.device);
+    const uint64_t n = s.n_obs, nd = s.n_dofs;
+    size_t need = (size_t)k * (2 * n + nd);
+    if (s.pin_n < need) {
+        if (s.pin) cudaFreeHost(s.pin);
+        s.pin = nullptr;
+        CK(cudaMallocHost(&s.pin, need * sizeof(double)));
+        s.pin_n = need;
+    }
+    double* pY = s.pin;
+    double* pD = s.pin + k * n;
+    double* pX = s.pin + 2 * k * n;
+    std::memcpy(pY, Y, k * n * sizeof(double));
+    double* dY = nullptr;
+    double* dX = nullptr;
+    double* dD = nullptr;
+    CK(cudaMallocAsync(&dY, k * n * sizeof(double), s.stream));
+    CK(cudaMallocAsync(&dX, k * nd * sizeof(double), s.stream));
+    CK(cudaMallocAsync(&dD, k * n * sizeof(double), s.stream));
+    struct Free {
+        cudaStream_t st;
+        double *a, *b, *c;
+        ~Free() {
+            cudaFreeAsync(a, st);
+            cudaFreeAsync(b, st);
+            cudaFreeAsync(c, st);
+        }
+    } fr{s.stream, dY, dX, dD};
+    CK(cudaMemcpyAsync(dY, pY, k * n * sizeof(double), cudaMemcpyHostToDevice, s.stream));
+    dispatch_solve(s, dY, k, tol, maxiter, dX, dD, stats, s.stream);
+    CK(cudaMemcpyAsync(pD, dD, k * n * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    CK(cudaMemcpyAsync(pX, dX, k * nd * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+    if (Dm) std::memcpy(Dm, pD, k * n * sizeof(double));
+    if (X) {
+        std::memcpy(X, pX, k * nd * sizeof(double));
+        if (s.reparam.active())
+            for (uint64_t j = 0; j < k; ++j) s.reparam.back_transform(X + j * nd);
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+extern "C" {
+
+const char* within_last_error(void) { return g_err.c_str(); }
+uint64_t within_launch_count(void) { return g_launches; }
+void within_launch_count_reset(void) { g_launches = 0; }
+
+void within_precond_config_default(within_precond_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->kind = WITHIN_PRECOND_ADDITIVE;
+    c->approx_chol_seed = 0;
+    c->approx_chol_split = 2;
+    c->schur_exact = 0;
+    c->schur_seed = 0;
+    c->schur_split = 1;
+    c->dense_threshold = 24;
+    c->scaling_tolerance = 1e-9;
+    c->scaling_max_sweeps = 2048;
+    c->scaling_error = 0;
+    c->reduction = 0;
+}
+
+void within_lsmr_options_default(within_lsmr_options* o) {
+    o->tol = 1e-8;
+    o->maxiter = 1000;
+    o->local_size = 0;
+}
+
+int within_design_from_categories(const uint32_t* codes, uint64_t n_obs, uint64_t n_factors,
+                                  within_design** out) {
+    *out = nullptr;
+    return guarded([&] {
+        if (!codes && n_obs * n_factors) throw WError(ERR_INVALID, "codes is NULL");
+        if (n_obs == 0) throw WError(ERR_BUILD, "no observations provided");
+        auto d = std::make_unique<within_design>();
+        d->n_obs = n_obs;
+        for (uint64_t f = 0; f < n_factors; ++f) {
+            d->levels.emplace_back(codes + f * n_obs, codes + (f + 1) * n_obs);
+            d->intercept.push_back(1);
+            d->slope_of.emplace_back();
+        }
+        uint64_t nd = 0;
+        for (auto& l : d->levels) nd += (uint64_t)*std::max_element(l.begin(), l.end()) + 1;
+        d->n_dofs = nd;
+        *out = d.release();
+    });
+}
+
+int within_design_from_effects(uint64_t n_obs, uint64_t n_effects, const uint32_t* const* levels,
+                               const int32_t* intercept, const uint64_t* n_slopes,
+                               const double* const* slopes, within_design** out) {
+    *out = nullptr;
+    return guarded([&] {
+        if (n_obs == 0) throw WError(ERR_BUILD, "no observations provided");
+        auto d = std::make_unique<within_design>();
+        d->n_obs = n_obs;
+        uint64_t si = 0, nd = 0;
+        for (uint64_t e = 0; e < n_effects; ++e) {
+            d->levels.emplace_back(levels[e], levels[e] + n_obs);
+            d->intercept.push_back(intercept[e] ? 1 : 0);
+            std::vector<size_t> idx;
+            for (uint64_t j = 0; j < n_slopes[e]; ++j, ++si) {
+                d->slopes.emplace_back(slopes[si], slopes[si] + n_obs);
+                idx.push_back(d->slopes.size() - 1);
+            }
+            if (!intercept[e] && idx.empty())
+                throw WError(ERR_BUILD, "an effect must have an intercept or at least one slope");
+            d->slope_of.push_back(idx);
+            nd += ((uint64_t)*std::max_element(levels[e], levels[e] + n_obs) + 1) *
+                  ((intercept[e] ? 1 : 0) + idx.size());
+        }
+        d->n_dofs = nd;
+        *out = d.release();
+    });
+}
+
+void within_design_free(within_design* d) { delete d; }
+uint64_t within_design_n_obs(const within_design* d) { return d ? d->n_obs : 0; }
+uint64_t within_design_n_dofs(const within_design* d) { return d ? d->n_dofs : 0; }
+
+int within_solver_new(const within_design* design, const double* weights, const within_precond_config* cfg,
+                      const within_preconditioner* prebuilt, int32_t device, within_solver** out) {
+    *out = nullptr;
+    return guarded([&] { *out = make_solver(design, weights, cfg, prebuilt, device); });
+}
+
+void within_solver_free(within_solver* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+}
+
+uint64_t within_solver_n_obs(const within_solver* s) { return s->n_obs; }
+uint64_t within_solver_n_dofs(const within_solver* s) { return s->n_dofs; }
+uint64_t within_solver_n_warnings(const within_solver* s) { return s->n_warnings; }
+uint64_t within_solver_unidentified(const within_solver* s, uint64_t* triples, uint64_t cap) {
+    const auto& u = s->reparam.unidentified;
+    uint64_t n = u.size() / 3;
+    for (uint64_t i = 0; i < n && i < cap; ++i)
+        for (int j = 0; j < 3; ++j) triples[3 * i + j] = u[3 * i + j];
+    return n;
+}
+uint64_t within_solver_n_terms(const within_solver* s) { return s->design.terms.size(); }
+int within_solver_term_layout(const within_solver* s, uint64_t term, uint64_t* n_levels, uint64_t* offset,
+                              uint64_t* n_columns) {
+    if (term >= s->design.terms.size()) {
+        g_err = "term out of range";
+        return WITHIN_ERR_INVALID_INPUT;
+    }
+    const Term& t = s->design.terms[term];
+    *n_levels = t.n_levels;
+    *offset = t.offset;
+    *n_columns = t.cols.size();
+    return WITHIN_OK;
+}
+int within_solver_obs_perm(const within_solver* s, uint32_t* out) {
+    if (s->design.obs_perm.empty()) return 0;
+    std::memcpy(out, s->design.obs_perm.data(), s->n_obs * sizeof(uint32_t));
+    return 1;
+}
+within_preconditioner* within_solver_preconditioner(const within_solver* s) {
+    if (!s->precond) return nullptr;
+    ++s->precond->refs;
+    return s->precond;
+}
+int within_solver_set_precision(within_solver* s, int32_t precision) {
+    if (precision != WITHIN_PRECISION_FP64) {
+        g_err = "only WITHIN_PRECISION_FP64 is available in this build";
+        return WITHIN_ERR_UNSUPPORTED;
+    }
+    s->precision = precision;
+    return WITHIN_OK;
+}
+
+int within_solver_solve(within_solver* s, const double* y, const within_lsmr_options* opts, double* x_out,
+                        double* demeaned_out, within_solve_stats* stats) {
+    return guarded([&] { host_solve(*s, y, 1, opts, x_out, demeaned_out, stats); });
+}
+
+int within_solver_solve_batch(within_solver* s, const double* Y, uint64_t k, const within_lsmr_options* opts,
+                              double* X_out, double* D_out, within_solve_stats* stats) {
+    return guarded([&] {
+        if (k == 0) return;
+        host_solve(*s, Y, k, opts, X_out, D_out, stats);
+    });
+}
+
+int within_solver_solve_batch_device(within_solver* s, const double* Y_dev, uint64_t k,
+                                     const within_lsmr_options* opts, double* X_dev, double* D_dev,
+                                     within_solve_stats* stats, void* stream) {
+    return guarded([&] {
+        double tol;
+        uint64_t maxiter, ls;
+        validate_opts(opts, tol, maxiter, ls);
+        if (k == 0) return;
+        std::lock_guard<std::mutex> g(s->mu);
+        set_device(s->device);
+        cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+        dispatch_solve(*s, Y_dev, k, tol, maxiter, X_dev, D_dev, stats, st);
+        if (X_dev && s->reparam.active()) {
+            std::vector<double> hx(k * s->n_dofs);
+            CK(cudaMemcpyAsync(hx.data(), X_dev, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (uint64_t j = 0; j < k; ++j) s->reparam.back_transform(hx.data() + j * s->n_dofs);
+            CK(cudaMemcpyAsync(X_dev, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+    });
+}
+
+int within_solve(const within_design* design, const double* y, const double* weights,
+                 const within_lsmr_options* opts, const within_precond_config* cfg, double* x_out,
+                 double* demeaned_out, within_solve_stats* stats) {
+    return within_solve_batch(design, y, 1, weights, opts, cfg, x_out, demeaned_out, stats);
+}
+
+int within_solve_batch(const within_design* design, const double* Y, uint64_t k, const double* weights,
+                       const within_lsmr_options* opts, const within_precond_config* cfg, double* X_out,
+                       double* D_out, within_solve_stats* stats) {
+    return guarded([&] {
+        const double t0 = now_s();
+        std::unique_ptr<within_solver> s(make_solver(design, weights, cfg, nullptr, -1));
+        const double t1 = now_s();
+        if (k == 0) return;
+        host_solve(*s, Y, k, opts, X_out, D_out, stats);
+        if (stats)
+            for (uint64_t j = 0; j < k; ++j) {
+                stats[j].time_setup += t1 - t0;
+                stats[j].time_total = now_s() - t0;
+            }
+        cudaStreamSynchronize(s->stream);
+    });
+}
+
+int within_solver_operator_apply(within_solver* s, const double* x_dev, double* y_dev, void* stream) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> g(s->mu);
+        set_device(s->device);
+        cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+        k_apply<1><<<grid_for(s->n_obs, 256, 148 * 16), 256, 0, st>>>(s->op, x_dev, y_dev);
+        ++g_launches;
+        CK(cudaGetLastError());
+        if (!stream) CK(cudaStreamSynchronize(st));
+    });
+}
+
+int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, double* y_dev, void* stream) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> g(s->mu);
+        set_device(s->device);
+        cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+        ensure_scatter(*s, 1);
+        scatter<1, 0>(*s, u_dev, y_dev, nullptr, nullptr, st);
+        CK(cudaGetLastError());
+        if (!stream) CK(cudaStreamSynchronize(st));
+    });
+}
+
+void within_preconditioner_free(within_preconditioner* p) {
+    if (p && --p->refs == 0) delete p;
+}
+uint64_t within_preconditioner_n(const within_preconditioner* p) { return p ? p->n : 0; }
+const char* within_preconditioner_variant_name(const within_preconditioner* p) {
+    return p && p->kind == 2 ? "Diagonal" : "Additive";
+}
+
+int within_preconditioner_apply(const within_preconditioner* pc, const double* x_dev, double* y_dev,
+                                void* stream) {
+    return guarded([&] {
+        auto* p = const_cast<within_preconditioner*>(pc);
+        set_device(p->device);
+        cudaStream_t st = stream ? (cudaStream_t)stream : nullptr;
+        if (p->kind == 2) {
+            k_diag_apply<1><<<grid_for(p->n, 256, 148 * 8), 256, 0, st>>>(p->n, p->inv_diag, x_dev, y_dev, nullptr);
+            ++g_launches;
+        } else {
+            std::lock_guard<std::mutex> g(p->mu);
+            if (!p->standalone) p->standalone = new SchwarzUser();
+            schwarz_apply<1>(*p, *p->standalone, x_dev, y_dev, nullptr, st);
+        }
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+    });
+}
+
+}  // extern "C"
