@@ -79,6 +79,10 @@ struct PrecondCfg {
     double scaling_tol = 1e-9;
     uint64_t scaling_max_sweeps = 2048;
     bool scaling_error = false;
+    // round-parallel factor: when to stop the rounds (host_schwarz.cpp ac_rounds)
+    uint32_t core_dense_max = 2048;
+    double core_min_frac = 0.1;
+    uint32_t max_rounds = 64;
 };
 
 // Host image of the additive Schwarz preconditioner in the layout the apply
@@ -129,6 +133,10 @@ struct SchwarzHost {
     std::vector<uint32_t> bwd_row;
     std::vector<uint32_t> bwd_ptr, bwd_col;   // pull form: L[later row, col]
     std::vector<double> bwd_val;
+    // dense cores of round-scheduled factors (x_core = G y_core after the forward pass)
+    std::vector<uint32_t> core_rows_ptr, core_row_slot, core_col;
+    std::vector<double> core_val;
+    uint32_t max_core = 0;
     // prolongation combine: DOF -> local slots
     std::vector<uint32_t> dof_ptr, dof_slot;
     // statistics

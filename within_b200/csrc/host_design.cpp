@@ -253,41 +253,55 @@ void Reparam::back_transform(double* x) const {
 // ---------------------------------------------------------------------------
 // Tile plan of one segmented-reduction problem (see segreduce.cuh).
 void HostPlan::add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, int T) {
-    // positions of this problem are [ptr[0], ptr[n_seg]); tiles start at ptr[0]
-    const uint32_t pbase = ptr[0];
-    const uint32_t npos = ptr[n_seg] - pbase;
-    const uint32_t nt = npos == 0 ? 1u : (npos + (uint32_t)T - 1) / (uint32_t)T;
+    // Positions of this problem are [ptr[0], ptr[n_seg]).  Tiles hold at most
+    // T positions and own at most T segments (a run of empty segments, e.g.
+    // the first round of a triangular solve, is spread over several CTAs; a
+    // tile may then own segments but no positions).
+    const uint32_t pbase = ptr[0], pend = ptr[n_seg];
     const uint32_t base = (uint32_t)tiles.size();
-    for (uint32_t lt = 0; lt < nt; ++lt) {
+    uint32_t p = pbase, s = 0;
+    std::vector<uint32_t> starts;  // p0 of tiles holding positions, for split lookup
+    std::vector<uint32_t> ids;
+    do {
         SRTile t{};
         t.problem = problem;
-        t.p0 = pbase + lt * (uint32_t)T;
-        t.p1 = pbase + (uint32_t)std::min<uint64_t>((uint64_t)lt * (uint32_t)T + (uint32_t)T, npos);
-        t.own_lo = t.own_hi = 0;
+        t.p0 = p;
+        t.own_lo = s;
+        uint32_t hi = (uint32_t)std::min<uint64_t>((uint64_t)p + (uint32_t)T, pend);
+        uint32_t owned = 0;
+        const bool at_end = p == pend;
+        while (s < n_seg && (ptr[s] < hi || (at_end && ptr[s] == pend)) && owned < (uint32_t)T) {
+            ++s;
+            ++owned;
+        }
+        if (owned == (uint32_t)T && s < n_seg && ptr[s] < hi) hi = ptr[s];  // segment budget spent
+        t.p1 = hi;
+        t.own_hi = s;
         t.cont_split = -1;
         t.tail_split = -1;
+        if (t.p1 > t.p0) {
+            starts.push_back(t.p0);
+            ids.push_back((uint32_t)tiles.size());
+        }
         tiles.push_back(t);
-    }
-    // owned ranges: segment s belongs to the tile holding its first position
-    // (segments starting at the end of the range belong to the last tile).
-    uint32_t s = 0;
-    for (uint32_t lt = 0; lt < nt; ++lt) {
-        SRTile& t = tiles[base + lt];
-        t.own_lo = s;
-        bool last = lt + 1 == nt;
-        while (s < n_seg && (last || ptr[s] < t.p1)) ++s;
-        t.own_hi = s;
-    }
+        p = hi;
+    } while (p < pend || s < n_seg);
+    // split segments: positions spread over more than one tile
+    auto tile_of = [&](uint32_t pos) {
+        size_t i = (size_t)(std::upper_bound(starts.begin(), starts.end(), pos) - starts.begin()) - 1;
+        return ids[i];
+    };
     for (uint32_t g = 0; g < n_seg; ++g) {
-        uint32_t a = ptr[g] - pbase, b = ptr[g + 1] - pbase;
+        uint32_t a = ptr[g], b = ptr[g + 1];
         if (b <= a) continue;
-        uint32_t t0 = a / (uint32_t)T, t1 = (b - 1) / (uint32_t)T;
+        uint32_t t0 = tile_of(a), t1 = tile_of(b - 1);
         if (t1 == t0) continue;
         int id = (int)splits.size();
-        splits.push_back(SRSplit{problem, g, base + t0, base + t1});
-        tiles[base + t0].tail_split = id;
-        for (uint32_t t = t0 + 1; t <= t1; ++t) tiles[base + t].cont_split = id;
+        splits.push_back(SRSplit{problem, g, t0, t1});
+        tiles[t0].tail_split = id;
+        for (uint32_t t = t0 + 1; t <= t1; ++t) tiles[t].cont_split = id;
     }
+    (void)base;
 }
 
 }  // namespace wgpu

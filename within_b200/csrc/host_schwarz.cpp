@@ -23,6 +23,8 @@
 #include <cfloat>
 #include <cmath>
 #include <numeric>
+#include <cstdio>
+#include <cstdlib>
 
 #include "host.hpp"
 
@@ -409,6 +411,12 @@ struct Factor {
     std::vector<double> dinv;                 // per vertex
     std::vector<std::vector<std::pair<uint32_t, double>>> colv;  // per vertex: (later row, l)
     uint32_t n_rounds = 0;
+    // the vertices left when the rounds stop (see ac_rounds): with core_dense
+    // their Schur complement is applied as a dense generalised inverse
+    // core_pinv (core.size()^2, row-major over `core`), otherwise by its diagonal.
+    std::vector<uint32_t> core;
+    bool core_dense = false;
+    std::vector<double> core_pinv;
 };
 
 // Dense LDL^T in natural order with pseudo-inverse pivots, materialised as
@@ -471,7 +479,9 @@ bool dense_pinv(const Lap& m, Factor& f) {
 // independent set: vertices whose (capped degree, hash, id) key is smaller than
 // every alive neighbour's.  Low-degree vertices therefore go first, which keeps
 // fill low; the clique of an eliminated vertex is replaced by a sampled tree.
-void ac_rounds(const Lap& m, uint64_t seed, uint32_t split, Factor& f) {
+void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
+    const uint64_t seed = cfg.ac_seed;
+    const uint32_t split = cfg.ac_split;
     const uint32_t n = m.n;
     std::vector<std::vector<std::pair<uint32_t, double>>> adj(n);
     for (uint32_t i = 0; i < n; ++i)
@@ -492,6 +502,7 @@ void ac_rounds(const Lap& m, uint64_t seed, uint32_t split, Factor& f) {
     std::vector<Edge> fill;
     std::vector<std::pair<uint32_t, double>> ent;
     uint32_t r = 0;
+    double last_frac = 1.0;
     while (!live.empty()) {
         // compact adjacency: drop dead neighbours, merge parallel edges
         for (uint32_t v : live) {
@@ -515,6 +526,54 @@ void ac_rounds(const Lap& m, uint64_t seed, uint32_t split, Factor& f) {
             }
             uint64_t deg = std::min<uint64_t>(a.size(), 255);
             key[v] = (deg << 56) | (mix64(seed ^ ((uint64_t)v << 20) ^ r) & 0x00FFFFFFFF000000ull) | 0;
+        }
+        // Stop the rounds once the remaining graph is a small or dense core:
+        // a dense core (<= core_dense_max vertices) is inverted exactly; a
+        // larger one, reached when rounds stop paying (fewer than
+        // core_min_frac of the vertices eliminated) or at max_rounds, keeps
+        // only its diagonal -- its intra-core edges are dropped, which leaves
+        // an SDD (positive semi-definite) approximation of the core.
+        const bool small = live.size() <= cfg.core_dense_max && live.size() > 1;
+        const bool stalled = last_frac < cfg.core_min_frac || r >= cfg.max_rounds;
+        if (small || (stalled && live.size() > 1)) {
+            f.core = live;
+            std::sort(f.core.begin(), f.core.end());
+            for (uint32_t v : f.core) f.round[v] = r;
+            if (small) {
+                f.core_dense = true;
+                std::vector<uint32_t> pos(n, UINT32_MAX);
+                for (uint32_t i = 0; i < f.core.size(); ++i) pos[f.core[i]] = i;
+                Lap c;
+                c.n = (uint32_t)f.core.size();
+                for (uint32_t i = 0; i < c.n; ++i) {
+                    double deg = 0;
+                    std::vector<std::pair<uint32_t, double>> row;
+                    for (auto& e : adj[f.core[i]]) {
+                        row.push_back({pos[e.first], -e.second});
+                        deg += e.second;
+                    }
+                    row.push_back({i, deg});
+                    std::sort(row.begin(), row.end());
+                    for (auto& x : row) {
+                        c.col.push_back(x.first);
+                        c.val.push_back(x.second);
+                    }
+                    c.ptr.push_back((uint32_t)c.col.size());
+                }
+                Factor cf;
+                if (!dense_pinv(c, cf)) throw WError(ERR_SINGULAR, "dense core factorisation failed");
+                f.core_pinv = std::move(cf.pinv);
+                for (uint32_t v : f.core) f.dinv[v] = 0.0;   // forward pass only; the core mat-vec writes x
+            } else {
+                f.core_dense = false;
+                for (uint32_t v : f.core) {
+                    double d = 0;
+                    for (auto& e : adj[v]) d += e.second;
+                    f.dinv[v] = d > 0.0 ? 1.0 / d : 0.0;
+                }
+            }
+            ++r;
+            break;
         }
         sel.clear();
         for (uint32_t v : live) {
@@ -553,10 +612,12 @@ void ac_rounds(const Lap& m, uint64_t seed, uint32_t split, Factor& f) {
             adj[e.lo].push_back({e.hi, e.w});
             adj[e.hi].push_back({e.lo, e.w});
         }
+        const size_t before = live.size();
         size_t w = 0;
         for (uint32_t v : live)
             if (alive[v]) live[w++] = v;
         live.resize(w);
+        last_frac = (double)sel.size() / (double)before;
         ++r;
     }
     f.n_rounds = r;
@@ -564,7 +625,7 @@ void ac_rounds(const Lap& m, uint64_t seed, uint32_t split, Factor& f) {
 
 void factor_lap(const Lap& L, const PrecondCfg& cfg, Factor& f) {
     if (L.n <= DENSE_MAX && dense_pinv(L, f)) return;
-    ac_rounds(L, cfg.ac_seed, cfg.ac_split, f);
+    ac_rounds(L, cfg, f);
 }
 
 // Gremban cover of a signed matrix (block_elim/solver.rs:220-271).
@@ -917,6 +978,25 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         }
         S.factor_nnz += (uint64_t)f.n * f.n;
     }
+    // dense cores of round-scheduled factors: x_core = G_core y_core
+    S.core_rows_ptr.push_back(0);
+    for (uint32_t s = 0; s < S.n_sub; ++s) {
+        const Factor& f = doms[s].fac;
+        if (f.dense || !f.core_dense) continue;
+        const uint32_t m = (uint32_t)f.core.size(), ro = S.red_off[s];
+        for (uint32_t i = 0; i < m; ++i) {
+            for (uint32_t j = 0; j < m; ++j) {
+                S.core_col.push_back(ro + f.core[j]);
+                S.core_val.push_back(f.core_pinv[(size_t)i * m + j]);
+            }
+            S.core_rows_ptr.push_back((uint32_t)S.core_col.size());
+            S.core_row_slot.push_back(ro + f.core[i]);
+        }
+        S.factor_nnz += (uint64_t)m * m;
+        S.max_core = std::max(S.max_core, m);
+    }
+    for (uint32_t s = 0; s < S.n_sub; ++s)
+        if (!doms[s].fac.dense) S.max_core = std::max<uint32_t>(S.max_core, (uint32_t)doms[s].fac.core.size());
     // round-scheduled factors: forward rows pull from earlier columns, backward
     // rows (= eliminated columns) pull from later rows.
     S.n_rounds = rounds;

@@ -272,6 +272,9 @@ struct SchwarzDev {
     const double* bwd_val;
     const uint32_t* dof_slot;
     const uint32_t* kept_ptr;
+    const uint32_t* core_row_slot;
+    const uint32_t* core_col;
+    const double* core_val;
     // work (K-interleaved)
     double* rl;   // restricted, folded local rhs (per local slot)
     double* sl;   // local solution (per local slot)
@@ -447,6 +450,27 @@ struct FwdF {
             S.yv[(size_t)u * K + k] = y;
             S.xv[(size_t)u * K + k] = y * di;
         }
+    }
+};
+
+// dense core of a round-scheduled factor: x_core = G_core y_core, between the
+// forward and the backward sweeps
+template <int K>
+struct CoreF {
+    using Prob = SegProb;
+    const SegProb* probs;
+    SchwarzDev S;
+    __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
+    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+        const uint32_t c = __ldg(S.core_col + a);
+        const double g = __ldg(S.core_val + a);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = g * S.yv[(size_t)c * K + k];
+    }
+    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+        const uint32_t u = S.core_row_slot[p.seg_base + seg];
+#pragma unroll
+        for (int k = 0; k < K; ++k) S.xv[(size_t)u * K + k] = s[k];
     }
 };
 

@@ -154,22 +154,41 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
         }
     }
     __syncthreads();
-    if (tid == 0) {
-        for (int j = 0; j < 2; ++j) {
-            int id = last_split[j];
-            if (id < 0) continue;
-            __threadfence();
-            const SRSplit sp = splits[id];
-            double acc[K];
+    // The finishing CTA adds the tail partial and the head partials of the
+    // split in tile order: thread i takes tiles t0+1+i, t0+1+i+256, ..., then a
+    // fixed shuffle tree -- the same order on every run.
+    for (int j = 0; j < 2; ++j) {
+        const int id = last_split[j];
+        if (id < 0) continue;   // uniform across the block (shared)
+        __threadfence();
+        const SRSplit sp = splits[id];
+        double acc[K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) acc[k] = __ldcg(&tail_buf[(size_t)id * K + k]);
-            for (uint32_t t = sp.t0 + 1; t <= sp.t1; ++t)
+        for (int k = 0; k < K; ++k) acc[k] = 0.0;
+        for (uint32_t t = sp.t0 + 1 + tid; t <= sp.t1; t += SR_THREADS)
 #pragma unroll
-                for (int k = 0; k < K; ++k) acc[k] += __ldcg(&head_buf[(size_t)t * K + k]);
+            for (int k = 0; k < K; ++k) acc[k] += __ldcg(&head_buf[(size_t)t * K + k]);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double v = acc[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if ((tid & 31) == 0) sv[(tid >> 5) * K + k] = v;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double tot[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                double v = __ldcg(&tail_buf[(size_t)id * K + k]);
+                for (int w = 0; w < SR_THREADS / 32; ++w) v += sv[w * K + k];
+                tot[k] = v;
+            }
             Prob pr = (sp.problem == tile.problem) ? prob : f.probs[sp.problem];
-            f.emit(pr, sp.seg, acc);
+            f.emit(pr, sp.seg, tot);
             counters[id] = 0;
         }
+        __syncthreads();
     }
 }
 

@@ -130,8 +130,9 @@ struct within_preconditioner {
     SchwarzDev dev_const{};      // pointers into arena (work pointers filled per user)
     // per-step segment problems
     SegProb *p_restrict = nullptr, *p_ct = nullptr, *p_kept = nullptr, *p_dense = nullptr,
-            *p_fwd = nullptr, *p_bwd = nullptr, *p_c = nullptr, *p_prolong = nullptr;
-    bool has_dense = false;
+            *p_fwd = nullptr, *p_bwd = nullptr, *p_c = nullptr, *p_prolong = nullptr,
+            *p_core = nullptr;
+    bool has_dense = false, has_core = false;
     uint32_t n_rounds = 0;
     std::mutex mu;
     std::atomic<int> refs{1};
@@ -179,6 +180,9 @@ void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
     D.bwd_val = A.upload(H.bwd_val);
     D.dof_slot = A.upload(H.dof_slot);
     D.kept_ptr = A.upload(H.kept_ptr);
+    D.core_row_slot = A.upload(H.core_row_slot);
+    D.core_col = A.upload(H.core_col);
+    D.core_val = A.upload(H.core_val);
     uint32_t* loc_ptr = const_cast<uint32_t*>(D.loc_ptr);
     uint32_t* ct_ptr = A.upload(H.ct_ptr);
     uint32_t* kept_ptr = const_cast<uint32_t*>(D.kept_ptr);
@@ -187,6 +191,7 @@ void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
     uint32_t* bwd_ptr = A.upload(H.bwd_ptr);
     uint32_t* c_ptr = A.upload(H.c_ptr);
     uint32_t* dof_ptr = A.upload(H.dof_ptr);
+    uint32_t* core_ptr = A.upload(H.core_rows_ptr);
     auto one = [&](uint32_t* ptr) { return A.upload(std::vector<SegProb>{SegProb{ptr, 0, 0}}); };
     P.p_restrict = one(loc_ptr);
     P.p_ct = one(ct_ptr);
@@ -194,7 +199,9 @@ void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
     P.p_dense = one(dense_ptr);
     P.p_c = one(c_ptr);
     P.p_prolong = one(dof_ptr);
+    P.p_core = one(core_ptr);
     P.has_dense = H.dense_rows_ptr.size() > 1;
+    P.has_core = H.core_rows_ptr.size() > 1;
     P.n_rounds = H.n_rounds;
     std::vector<SegProb> fw, bw;
     for (uint32_t r = 0; r < H.n_rounds; ++r) {
@@ -214,7 +221,7 @@ struct SchwarzWork {
 // Everything one user of a (possibly shared) preconditioner mutates: the tile
 // plans' partial/counter buffers and the work vectors, per column bucket K.
 struct KPlans {
-    DevPlan restrict_, ct, kept, dense, fwd, bwd, c, prolong;
+    DevPlan restrict_, ct, kept, dense, fwd, bwd, c, prolong, core;
     SchwarzWork w;
     bool ready = false;
 };
@@ -250,6 +257,7 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     kp.dense = one(H.dense_rows_ptr);
     kp.c = one(H.c_ptr);
     kp.prolong = one(H.dof_ptr);
+    kp.core = one(H.core_rows_ptr);
     auto rounds = [&](const std::vector<uint32_t>& rptr, const std::vector<uint32_t>& ptr) {
         HostPlan hp;
         std::vector<uint32_t> lo, hi;
@@ -297,6 +305,7 @@ void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const double* r, do
     if (P.has_dense) launch_sr<DenseF<K>, K>(DenseF<K>{P.p_dense, S}, kp.dense, 0, kp.dense.n_tiles, skip, st);
     for (uint32_t r = 0; r < P.n_rounds; ++r)
         launch_sr<FwdF<K>, K>(FwdF<K>{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
+    if (P.has_core) launch_sr<CoreF<K>, K>(CoreF<K>{P.p_core, S}, kp.core, 0, kp.core.n_tiles, skip, st);
     for (uint32_t r = P.n_rounds; r-- > 0;)
         launch_sr<BwdF<K>, K>(BwdF<K>{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
     launch_sr<CF<K>, K>(CF<K>{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
@@ -641,6 +650,10 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
             pc.scaling_error = cfg->scaling_error != 0;
             if (pc.kind < 0 || pc.kind > 2) throw WError(ERR_INVALID, "unknown preconditioner kind");
         }
+        // tuning of the round-parallel factor (see PrecondCfg)
+        if (const char* e = getenv("WITHIN_CORE_DENSE_MAX")) pc.core_dense_max = (uint32_t)atol(e);
+        if (const char* e = getenv("WITHIN_CORE_MIN_FRAC")) pc.core_min_frac = atof(e);
+        if (const char* e = getenv("WITHIN_MAX_ROUNDS")) pc.max_rounds = (uint32_t)atol(e);
         BuildResult br = build_preconditioner(D, weights ? w.data() : nullptr, pc);
         s->n_warnings = br.n_warnings;
         if (br.kind != 0) {
