@@ -1,0 +1,125 @@
+"""CPU-side checks of the product: the C ABI library loads and exports every
+entry point declared in include/*.h, the tile planner's invariants, the
+Python mirror's configuration lowering, and the multi-process (gloo) timing
+reduction used by bench.py for replicas."""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    inc = os.path.join(ROOT, "include")
+    for fn in sorted(os.listdir(inc)):
+        if fn.endswith(".h"):
+            src = open(os.path.join(inc, fn)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names += re.findall(r"\b(within_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(wb):
+    import ctypes
+    from within_b200 import _ffi
+    lib = ctypes.CDLL(_ffi.LIB_PATH)
+    decl = declared_functions()
+    assert len(decl) >= 30
+    missing = [n for n in decl if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(_ffi.exported_symbols()) == decl
+
+
+def test_library_fails_loudly_without_gpu(wb):
+    from conftest import has_gpu
+    if has_gpu():
+        pytest.skip("a GPU is present")
+    with pytest.raises(Exception):
+        wb.Solver(np.asfortranarray(np.zeros((4, 2), np.uint32)))
+
+
+def test_tile_planner_properties(tmp_path):
+    exe = tmp_path / "plan_test"
+    csrc = os.path.join(ROOT, "within_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", csrc, "-o", str(exe),
+                    os.path.join(ROOT, "tests", "cpp", "plan_test.cpp"),
+                    os.path.join(csrc, "host_design.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert "plan ok" in out
+
+
+def test_config_lowering(wb):
+    from within_b200 import _precond_config
+    from within_b200.config import (AdditiveSchwarz, ApproxCholConfig, ApproxSchurConfig,
+                                    LocalSolverConfig, ScalingConfig, Schur)
+    assert _precond_config(None) is None
+    assert _precond_config(wb.PreconditionerConfig.Off).kind == 0
+    assert _precond_config(wb.PreconditionerConfig.Diagonal).kind == 2
+    d = _precond_config(wb.PreconditionerConfig.Additive)
+    assert (d.kind, d.dense_threshold, d.approx_chol_split, d.schur_split) == (1, 24, 2, 1)
+    c = _precond_config(AdditiveSchwarz(local_solver=LocalSolverConfig(
+        approx_chol=ApproxCholConfig(seed=3, split_merge=4),
+        schur=Schur.approximate(ApproxSchurConfig(seed=5, split=2)), dense_threshold=7,
+        scaling=ScalingConfig(tolerance=1e-6, max_sweeps=9, on_failure="error"))))
+    assert (c.approx_chol_seed, c.approx_chol_split, c.schur_seed, c.schur_split) == (3, 4, 5, 2)
+    assert (c.dense_threshold, c.scaling_tolerance, c.scaling_max_sweeps, c.scaling_error) == (7, 1e-6, 9, 1)
+    assert _precond_config(AdditiveSchwarz(local_solver=LocalSolverConfig(schur=Schur.exact()))).schur_exact == 1
+    with pytest.raises(ValueError):
+        ApproxSchurConfig(split=0)
+    with pytest.raises(TypeError):
+        _precond_config("nope")
+
+
+def test_layout_and_effect_validation(wb):
+    lay = wb.CoefficientLayout([(0, 3, 1), (3, 4, 2)], 11)
+    for i in range(11):
+        assert lay.index(*lay.address(i)) == i
+    with pytest.raises(IndexError):
+        lay.index(1, 0, 2)
+    with pytest.raises(IndexError):
+        lay.address(11)
+    with pytest.raises(ValueError):
+        wb.Effect(np.zeros(4, np.uint32), False)
+    with pytest.raises(ValueError):
+        wb.Effect(np.zeros(4, np.uint32), True, [np.zeros(3)])
+    with pytest.raises(TypeError):
+        wb.Effect(np.zeros(4, np.float64), True)
+
+
+def _replica_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    sys.path.insert(0, ROOT)
+    import bench
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    t = bench.max_over_ranks(1.0 + rank, world)
+    q.put((rank, t, bench.dist_env()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_timing_is_max_over_ranks_gloo():
+    import multiprocessing as mp
+    import socket
+    ctx = mp.get_context("spawn")
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_replica_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[1] for r in res] == [2.0, 2.0]
+    assert [r[2][:2] for r in res] == [(0, 2), (1, 2)]
