@@ -168,6 +168,34 @@ int within_solver_operator_apply(within_solver* s, const double* x_dev, double* 
 int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, double* y_dev,
                                          void* stream);
 
+/* Allocation-free variant of within_solver_operator_apply_adjoint.  It has
+ * no counterpart in the reference.  It serves callers that cannot allocate
+ * device memory while they run -- code recording a CUDA stream capture (an
+ * allocation is not capturable), runtimes that own all device memory through
+ * their own arena, and latency-critical paths that cannot afford an
+ * allocation's implicit synchronisation or failure.  It computes the same
+ * D^T (W^{1/2} u) on device buffers in the internal observation order, but
+ * the reduction's scratch (per-tile partial sums, per-split completion
+ * counters) lives in one 8 MiB static device array of the library instead of
+ * solver-owned memory, and the call allocates nothing.
+ *  - The solver's single-column tile plan must already exist: the solver's
+ *    first single-RHS solve or within_solver_operator_apply_adjoint builds
+ *    it; before that the call returns WITHIN_ERR_INVALID_INPUT.
+ *  - A design whose reduction needs more than 8 MiB of scratch (about
+ *    700,000 tiles of 2,048 observations, i.e. more than 10^9 observation x
+ *    term pairs) is rejected with WITHIN_ERR_UNSUPPORTED and a message giving
+ *    the size needed.
+ *  - The first call on a device looks up the array's device address (with
+ *    that device current) and caches it; make that first call before any
+ *    stream capture that includes this entry point.
+ *  - Every call on a device shares the one array and leaves its contents
+ *    behind; the call clears the counters it needs.  Calls that overlap on
+ *    the GPU (other streams, other threads, other solvers) race on it and
+ *    must be serialised by the caller.
+ *  - stream NULL = the solver's stream, and the call waits for completion. */
+int within_solver_operator_apply_adjoint_noalloc(within_solver* s, const double* u_dev,
+                                                 double* y_dev, void* stream);
+
 /* ---- Preconditioner handle (operator/schwarz.rs:115-183) ---- */
 void within_preconditioner_free(within_preconditioner* p);
 uint64_t within_preconditioner_n(const within_preconditioner* p);

@@ -89,6 +89,7 @@ _SIGNATURES = [
     ("within_solve_batch", C.c_int, [P, P, U64, P, P, P, P, P, P]),
     ("within_solver_operator_apply", C.c_int, [P, P, P, P]),
     ("within_solver_operator_apply_adjoint", C.c_int, [P, P, P, P]),
+    ("within_solver_operator_apply_adjoint_noalloc", C.c_int, [P, P, P, P]),
     ("within_preconditioner_free", None, [P]),
     ("within_preconditioner_n", U64, [P]),
     ("within_preconditioner_variant_name", C.c_char_p, [P]),

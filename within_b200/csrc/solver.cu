@@ -84,12 +84,14 @@ struct DevPlan {
     double* tail = nullptr;
     unsigned* counters = nullptr;
     uint32_t n_tiles = 0;
+    uint32_t n_splits = 0;
     std::vector<uint32_t> range_lo, range_hi;   // tile ranges (per round, for round plans)
 };
 
 DevPlan make_plan(Arena& A, const HostPlan& hp, int K) {
     DevPlan d;
     d.n_tiles = (uint32_t)hp.tiles.size();
+    d.n_splits = (uint32_t)hp.splits.size();
     d.tiles = A.upload(hp.tiles);
     d.splits = A.upload(hp.splits);
     d.head = A.alloc<double>((size_t)d.n_tiles * K);
@@ -1018,3 +1020,80 @@ int within_preconditioner_apply(const within_preconditioner* pc, const double* x
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free variant of within_solver_operator_apply_adjoint.
+//
+// Some callers cannot allocate device memory while they run: code executing
+// under a CUDA stream capture (allocations are not capturable), runtimes that
+// own all device memory through their own arena and forbid cudaMalloc from
+// libraries, and real-time paths where an allocation's implicit
+// synchronisation or failure is unacceptable.  This entry point computes the
+// same D^T (W^{1/2} u) as within_solver_operator_apply_adjoint, but the
+// segmented reduction's scratch -- the per-tile partial sums and the per-split
+// completion counters -- lives in the file-scope device array below instead of
+// solver-owned allocations, and nothing is allocated during the call.
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)8 << 20;   // 8 MiB
+// Present on every device that loads this library, for the process lifetime.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_dev_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_noalloc_scratch on `dev` (which must be current).  On the
+// host the array's name only identifies the symbol; the address is looked up
+// once per device and cached.
+void* noalloc_scratch(int dev) {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw WError(ERR_UNSUPPORTED, "device ordinal out of range");
+    if (!g_noalloc_dev_ptr[dev]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_dev_ptr[dev] = p;
+    }
+    return g_noalloc_dev_ptr[dev];
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int within_solver_operator_apply_adjoint_noalloc(within_solver* s, const double* u_dev,
+                                                            double* y_dev, void* stream) {
+    return guarded([&] {
+        if (!s) throw WError(ERR_INVALID, "solver is NULL");
+        std::lock_guard<std::mutex> g(s->mu);
+        set_device(s->device);
+        if (!s->scatter_ready[0])
+            throw WError(ERR_INVALID,
+                         "within_solver_operator_apply_adjoint_noalloc: the solver's single-column tile plan "
+                         "does not exist yet; it is built by the solver's first single-RHS solve or "
+                         "within_solver_operator_apply_adjoint call");
+        const DevPlan& pl = s->scatter_plan[0];
+        const size_t head_b = align256((size_t)pl.n_tiles * sizeof(double));
+        const size_t tail_b = align256((size_t)std::max<uint32_t>(1, pl.n_splits) * sizeof(double));
+        const size_t cnt_b = align256((size_t)std::max<uint32_t>(1, pl.n_splits) * sizeof(unsigned));
+        const size_t need = head_b + tail_b + cnt_b;
+        if (need > NOALLOC_SCRATCH_BYTES)
+            throw WError(ERR_UNSUPPORTED,
+                         "within_solver_operator_apply_adjoint_noalloc: this design needs " + std::to_string(need) +
+                         " bytes of scratch (" + std::to_string(pl.n_tiles) + " tiles, " +
+                         std::to_string(pl.n_splits) + " split segments); the static maximum is " +
+                         std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes");
+        char* base = (char*)noalloc_scratch(s->device);
+        DevPlan p = pl;
+        p.head = (double*)base;
+        p.tail = (double*)(base + head_b);
+        p.counters = (unsigned*)(base + head_b + tail_b);
+        cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+        // the completion counters must start at zero; partials are written before they are read
+        CK(cudaMemsetAsync(p.counters, 0, cnt_b, st));
+        ScatterF<1, 0> f{s->scatter_probs, u_dev, s->op.sqrt_w, y_dev, nullptr};
+        launch_sr<ScatterF<1, 0>, 1>(f, p, 0, p.n_tiles, nullptr, st);
+        CK(cudaGetLastError());
+        if (!stream) CK(cudaStreamSynchronize(st));
+    });
+}
