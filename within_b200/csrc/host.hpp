@@ -105,14 +105,17 @@ struct SchwarzHost {
     std::vector<double> scale;            // partition weight * coordinate factor
     std::vector<uint32_t> slot_sub;       // owning subdomain
     std::vector<double> inv_e;            // 1/D_e for eliminated slots (0 for kept)
-    // C^T rows: one per kept slot, columns = local slot of the eliminated entry
+    // C^T rows: one per kept slot, columns = local slot of the eliminated entry,
+    // values C^T[k,e] / D_e[e]; ct_rowsum[k] = sum of the row's values
     std::vector<uint32_t> ct_ptr, ct_col;
-    std::vector<double> ct_val;
+    std::vector<double> ct_val, ct_rowsum;
     std::vector<uint32_t> ct_row_slot;    // kept local slot of each C^T row
     std::vector<uint32_t> ct_row_red;     // reduced slot of each C^T row
     // C rows: one per eliminated slot (in local-slot order of eliminated slots)
     std::vector<uint32_t> elim_slot;      // local slot of each C row
-    std::vector<uint32_t> c_ptr, c_col;   // columns = reduced slot of the kept entry
+    // columns = reduced slot of the kept entry (bit 31 set when the kept
+    // solution needs the ground gauge or the cover read-back); values C[e,k] / D_e[e]
+    std::vector<uint32_t> c_ptr, c_col;
     std::vector<double> c_val;
     // reduced slots
     uint32_t n_red = 0;

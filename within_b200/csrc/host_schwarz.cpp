@@ -934,24 +934,31 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             S.inv_e.push_back(j < ne ? dm.inv_e[j] : 0.0);
         }
         S.loc_ptr.push_back(lo + nloc);
-        // C^T rows (kept), columns = local slots of eliminated entries
+        // C^T rows (kept), columns = local slots of eliminated entries, values
+        // pre-divided by D_e (solver.rs:360-371 scales rhs_e by 1/D_e first)
         for (uint32_t k = 0; k < nk; ++k) {
             const Csr& ct = dm.comp.m.ct;
+            double rs = 0.0;
             for (uint32_t a = ct.ptr[k]; a < ct.ptr[k + 1]; ++a) {
+                const double v = ct.val[a] * dm.inv_e[ct.col[a]];
                 S.ct_col.push_back(lo + ct.col[a]);
-                S.ct_val.push_back(ct.val[a]);
+                S.ct_val.push_back(v);
+                rs += v;
             }
             S.ct_ptr.push_back((uint32_t)S.ct_col.size());
+            S.ct_rowsum.push_back(rs);
             S.ct_row_slot.push_back(lo + ne + k);
             S.ct_row_red.push_back(red + k);
         }
         S.kept_ptr.push_back(S.kept_ptr.back() + nk);
-        // C rows (eliminated), columns = reduced slot of the kept entry
+        // C rows (eliminated), columns = reduced slot of the kept entry (bit 31:
+        // gauge/cover read-back needed), values pre-divided by D_e (solver.rs:41-77)
+        const uint32_t flag = dm.mode == 0 ? 0u : 0x80000000u;
         for (uint32_t e = 0; e < ne; ++e) {
             const Csr& c = dm.comp.m.c;
             for (uint32_t a = c.ptr[e]; a < c.ptr[e + 1]; ++a) {
-                S.c_col.push_back(red + c.col[a]);
-                S.c_val.push_back(c.val[a]);
+                S.c_col.push_back((red + c.col[a]) | flag);
+                S.c_val.push_back(c.val[a] * dm.inv_e[e]);
             }
             S.c_ptr.push_back((uint32_t)S.c_col.size());
             S.elim_slot.push_back(lo + e);

@@ -106,20 +106,37 @@ __device__ bool grid_reduce(const double (&v)[NV], double* partials, unsigned* c
 }
 
 // ---------------------------------------------------------------------------
-// D x row sum for K columns at observation i (gather.rs:10-109).
+// D x rows (gather.rs:10-109): term sums accumulate in term order from 0.
+// D x for 4 consecutive observations [base, base+nr) per call: the code loads
+// are one 16-byte vector per term and all coefficient gathers of the 4 rows
+// are independent, so a thread keeps several memory requests in flight.
 template <int K>
-__device__ __forceinline__ void row_dx(const OpParams& p, uint32_t i, const double* __restrict__ x,
-                                       double (&s)[K]) {
+__device__ __forceinline__ void rows4_dx(const OpParams& p, uint32_t base, int nr,
+                                         const double* __restrict__ x, double (&s)[4][K]) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) s[k] = 0.0;
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int k = 0; k < K; ++k) s[r][k] = 0.0;
     for (int t = 0; t < p.Q; ++t) {
-        const uint32_t code = __ldg(p.codes[t] + i);
-        for (int c = 0; c < p.ncol[t]; ++c) {
-            const size_t base = ((size_t)p.off[t] + (size_t)c * p.L[t] + code) * K;
-            const int li = p.load[t][c];
-            const double ld = li < 0 ? 1.0 : __ldg(p.loads[li] + i);
+        uint32_t code[4];
+        if (nr == 4) {
+            const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(p.codes[t] + base));
+            code[0] = c4.x; code[1] = c4.y; code[2] = c4.z; code[3] = c4.w;
+        } else {
 #pragma unroll
-            for (int k = 0; k < K; ++k) s[k] += __ldg(x + base + k) * ld;
+            for (int r = 0; r < 4; ++r) code[r] = r < nr ? __ldg(p.codes[t] + base + r) : 0u;
+        }
+        for (int c = 0; c < p.ncol[t]; ++c) {
+            const size_t col = (size_t)p.off[t] + (size_t)c * p.L[t];
+            const int li = p.load[t][c];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (r >= nr) continue;
+                const double ld = li < 0 ? 1.0 : __ldg(p.loads[li] + base + r);
+                const double* xr = x + (col + code[r]) * K;
+#pragma unroll
+                for (int k = 0; k < K; ++k) s[r][k] += __ldg(xr + k) * ld;
+            }
         }
     }
 }
@@ -127,12 +144,18 @@ __device__ __forceinline__ void row_dx(const OpParams& p, uint32_t i, const doub
 // y = W^{1/2} D x  (Operator::apply; internal order)
 template <int K>
 __global__ void k_apply(OpParams p, const double* __restrict__ x, double* __restrict__ y) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
-        double s[K];
-        row_dx<K>(p, i, x, s);
-        const double w = p.sqrt_w ? p.sqrt_w[i] : 1.0;
+    const uint32_t stride = gridDim.x * blockDim.x * 4;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * 4; base < p.n; base += stride) {
+        const int nr = (int)min(4u, p.n - base);
+        double s[4][K];
+        rows4_dx<K>(p, base, nr, x, s);
 #pragma unroll
-        for (int k = 0; k < K; ++k) y[(size_t)i * K + k] = p.sqrt_w ? w * s[k] : s[k];
+        for (int r = 0; r < 4; ++r) {
+            if (r >= nr) continue;
+            const double w = p.sqrt_w ? p.sqrt_w[base + r] : 1.0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) y[(size_t)(base + r) * K + k] = p.sqrt_w ? w * s[r][k] : s[r][k];
+        }
     }
 }
 
@@ -140,11 +163,18 @@ __global__ void k_apply(OpParams p, const double* __restrict__ x, double* __rest
 template <int K>
 __global__ void k_demean(OpParams p, const double* __restrict__ x, const double* __restrict__ yint,
                          double* __restrict__ out) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
-        double s[K];
-        row_dx<K>(p, i, x, s);
+    const uint32_t stride = gridDim.x * blockDim.x * 4;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * 4; base < p.n; base += stride) {
+        const int nr = (int)min(4u, p.n - base);
+        double s[4][K];
+        rows4_dx<K>(p, base, nr, x, s);
 #pragma unroll
-        for (int k = 0; k < K; ++k) out[(size_t)i * K + k] = yint[(size_t)i * K + k] - s[k];
+        for (int r = 0; r < 4; ++r) {
+            if (r >= nr) continue;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                out[(size_t)(base + r) * K + k] = yint[(size_t)(base + r) * K + k] - s[r][k];
+        }
     }
 }
 
@@ -169,17 +199,23 @@ k_gather_update(OpParams p, const double* __restrict__ v, double* __restrict__ u
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
-        double s[K];
-        row_dx<K>(p, i, v, s);
-        const double w = p.sqrt_w ? __ldg(p.sqrt_w + i) : 1.0;
+    const uint32_t stride = gridDim.x * blockDim.x * 4;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * 4; base < p.n; base += stride) {
+        const int nr = (int)min(4u, p.n - base);
+        double s[4][K];
+        rows4_dx<K>(p, base, nr, v, s);
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            double av = p.sqrt_w ? w * s[k] : s[k];
-            double* up = u + (size_t)i * K + k;
-            double nu = act[k] ? av + scale[k] * (*up) : *up;
-            if (act[k]) *up = nu;
-            acc[k] += nu * nu;
+        for (int r = 0; r < 4; ++r) {
+            if (r >= nr) continue;
+            const double w = p.sqrt_w ? __ldg(p.sqrt_w + base + r) : 1.0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const double av = p.sqrt_w ? w * s[r][k] : s[r][k];
+                double* up = u + (size_t)(base + r) * K + k;
+                const double nu = act[k] ? av + scale[k] * (*up) : *up;
+                if (act[k]) *up = nu;
+                acc[k] += nu * nu;
+            }
         }
     }
     double tot[K];
@@ -253,7 +289,8 @@ struct SchwarzDev {
     const uint32_t* slot_sub;
     const double* inv_e;
     const uint32_t* ct_col;
-    const double* ct_val;
+    const double* ct_val;       // C^T / D_e
+    const double* ct_rowsum;
     const uint32_t* ct_row_slot;
     const uint32_t* ct_row_red;
     const uint32_t* elim_slot;
@@ -339,7 +376,8 @@ struct RestrictF {
     }
 };
 
-// S3: reduced rhs  rhs_k + C^T D_e^-1 rhs_e  (solver.rs:360-371)
+// S3: reduced rhs  rhs_k + C^T D_e^-1 rhs_e  (solver.rs:360-371).  With the
+// floating mean m: sum_e (C^T/D_e)[k,e] (r_e - m) = sum_e (C^T/D_e) r_e - m * rowsum_k.
 template <int K>
 struct CtF {
     using Prob = SegProb;
@@ -348,10 +386,9 @@ struct CtF {
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         const uint32_t e = __ldg(S.ct_col + a);
-        const uint32_t s = __ldg(S.slot_sub + e);
-        const double f = __ldg(S.ct_val + a) * __ldg(S.inv_e + e);
+        const double f = __ldg(S.ct_val + a);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = f * (S.rl[(size_t)e * K + k] - S.m1[(size_t)s * K + k]);
+        for (int k = 0; k < K; ++k) v[k] = f * S.rl[(size_t)e * K + k];
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t row = p.seg_base + seg;
@@ -360,9 +397,11 @@ struct CtF {
         const uint32_t rbi = S.ct_row_red[row];
         const bool cover = S.mode[sub] == 2;
         const uint32_t nk = S.n_kept[sub];
+        const double rsum = S.ct_rowsum[row];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const double val = (S.rl[(size_t)slot * K + k] - S.m1[(size_t)sub * K + k]) + s[k];
+            const double m = S.m1[(size_t)sub * K + k];
+            const double val = (S.rl[(size_t)slot * K + k] - m) + (s[k] - m * rsum);
             S.rb[(size_t)rbi * K + k] = val;
             if (cover) S.rb[(size_t)(rbi + nk) * K + k] = -val;
         }
@@ -494,7 +533,9 @@ struct BwdF {
     }
 };
 
-// S6: back-substitution  x_e = D_e^-1 rhs_e + D_e^-1 C x_k  (solver.rs:41-77)
+// S6: back-substitution  x_e = D_e^-1 rhs_e + D_e^-1 C x_k  (solver.rs:41-77);
+// C is stored pre-divided by D_e, and a column with bit 31 clear reads the
+// reduced solution directly (floating subdomain).
 template <int K>
 struct CF {
     using Prob = SegProb;
@@ -502,9 +543,15 @@ struct CF {
     SchwarzDev S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
-        double x[K];
-        kept_solution<K>(S, __ldg(S.c_col + a), x);
+        const uint32_t cc = __ldg(S.c_col + a);
         const double c = __ldg(S.c_val + a);
+        double x[K];
+        if (cc & 0x80000000u) {
+            kept_solution<K>(S, cc & 0x7fffffffu, x);
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) x[k] = S.xv[(size_t)cc * K + k];
+        }
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = c * x[k];
     }
@@ -514,7 +561,7 @@ struct CF {
         const double ie = S.inv_e[e];
 #pragma unroll
         for (int k = 0; k < K; ++k)
-            S.sl[(size_t)e * K + k] = (S.rl[(size_t)e * K + k] - S.m1[(size_t)sub * K + k]) * ie + ie * s[k];
+            S.sl[(size_t)e * K + k] = (S.rl[(size_t)e * K + k] - S.m1[(size_t)sub * K + k]) * ie + s[k];
     }
 };
 

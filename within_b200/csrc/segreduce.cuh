@@ -31,25 +31,28 @@ namespace wgpu {
 template <int K>
 struct SegItem {
     double v[K];
-    int f;  // 1 = a segment starts at this position
+    int sid;  // id of the segment that starts here (scan: the segment this position belongs to), -1 = none
 };
 
 template <int K>
 struct SegSumOp {
     __device__ __forceinline__ SegItem<K> operator()(const SegItem<K>& a, const SegItem<K>& b) const {
-        if (b.f) return b;
+        if (b.sid >= 0) return b;
         SegItem<K> c;
 #pragma unroll
         for (int k = 0; k < K; ++k) c.v[k] = a.v[k] + b.v[k];
-        c.f = a.f;
+        c.sid = a.sid;
         return c;
     }
 };
 
 template <int K>
-constexpr int sr_items() { return K >= 8 ? 1 : (K >= 4 ? 2 : (K >= 2 ? 4 : 8)); }
+constexpr int sr_items() { return K >= 4 ? 1 : (K >= 2 ? 2 : 4); }
 template <int K>
 constexpr int sr_tile() { return SR_THREADS * sr_items<K>(); }
+// resident CTAs per SM the register budget is sized for (no spills at K = 8)
+template <int K>
+constexpr int sr_min_blocks() { return K >= 8 ? 2 : (K >= 4 ? 3 : (K >= 2 ? 4 : 6)); }
 
 // F provides:
 //   using Prob = ...;                 (trivially copyable, <= 256 bytes)
@@ -57,8 +60,12 @@ constexpr int sr_tile() { return SR_THREADS * sr_items<K>(); }
 //   __device__ const uint32_t* seg_ptr(const Prob&) const;
 //   __device__ void value(const Prob&, uint32_t pos, double (&v)[K]) const;
 //   __device__ void emit(const Prob&, uint32_t seg, const double (&s)[K]) const;
+//
+// The block scan carries, for every position, the id of the segment it belongs
+// to, so the thread holding a segment's last position emits it straight from
+// registers; only the 2048-entry head table lives in shared memory.
 template <class F, int K>
-__global__ void __launch_bounds__(SR_THREADS)
+__global__ void __launch_bounds__(SR_THREADS, sr_min_blocks<K>())
 segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
                  const SRSplit* __restrict__ splits, double* __restrict__ head_buf,
                  double* __restrict__ tail_buf, unsigned* __restrict__ counters,
@@ -68,8 +75,8 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     using Prob = typename F::Prob;
     using Scan = cub::BlockScan<SegItem<K>, SR_THREADS>;
     __shared__ typename Scan::TempStorage scan_tmp;
-    __shared__ double sv[T * K];
-    __shared__ unsigned char flags[T];
+    __shared__ int headseg[T + 1];
+    __shared__ double wsum[(SR_THREADS / 32) * K];
     __shared__ SRTile tile;
     __shared__ Prob prob;
     __shared__ int last_split[2];
@@ -81,13 +88,20 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
         tile = tiles[gtile];
         prob = f.probs[tile.problem];
     }
-    for (int i = tid; i < T; i += SR_THREADS) flags[i] = 0;
+    for (int i = tid; i <= T; i += SR_THREADS) headseg[i] = -1;
     __syncthreads();
     const uint32_t p0 = tile.p0, p1 = tile.p1;
     const uint32_t* ptr = f.seg_ptr(prob);
     for (uint32_t s = tile.own_lo + tid; s < tile.own_hi; s += SR_THREADS) {
         uint32_t a = ptr[s], b = ptr[s + 1];
-        if (b > a) flags[a - p0] = 1;
+        if (b > a) {
+            headseg[a - p0] = (int)s;
+        } else {
+            double z[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) z[k] = 0.0;
+            f.emit(prob, s, z);   // empty segment
+        }
     }
     __syncthreads();
 
@@ -100,45 +114,40 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
             f.value(prob, p0 + p, v);
 #pragma unroll
             for (int k = 0; k < K; ++k) it[i].v[k] = v[k];
-            it[i].f = flags[p];
+            it[i].sid = headseg[p];
         } else {
 #pragma unroll
             for (int k = 0; k < K; ++k) it[i].v[k] = 0.0;
-            it[i].f = 1;
+            it[i].sid = -2;   // past the tile end: never emitted
         }
     }
     Scan(scan_tmp).InclusiveScan(it, it, SegSumOp<K>());
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i)
-#pragma unroll
-        for (int k = 0; k < K; ++k) sv[(tid * ITEMS + i) * K + k] = it[i].v[k];
-    __syncthreads();
 
-    for (uint32_t s = tile.own_lo + tid; s < tile.own_hi; s += SR_THREADS) {
-        uint32_t a = ptr[s], b = ptr[s + 1];
-        double out[K];
-        if (b == a) {
+    // emit at the last position of each segment piece held by this thread
 #pragma unroll
-            for (int k = 0; k < K; ++k) out[k] = 0.0;
-            f.emit(prob, s, out);
-        } else if (b <= p1) {
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t p = (uint32_t)(tid * ITEMS + i);
+        const uint32_t P = p0 + p;
+        if (P >= p1) continue;
+        const bool last = (P + 1 == p1) || headseg[p + 1] >= 0;
+        if (!last) continue;
+        const int sid = it[i].sid;
+        double o[K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) out[k] = sv[(b - 1 - p0) * K + k];
-            f.emit(prob, s, out);
-        } else {
-            // the one owned segment that runs past the tile: tail partial
+        for (int k = 0; k < K; ++k) o[k] = it[i].v[k];
+        if (sid >= 0) {
+            if (ptr[sid + 1] <= p1) {
+                f.emit(prob, (uint32_t)sid, o);
+            } else {   // the owned segment that runs past the tile: tail partial
 #pragma unroll
-            for (int k = 0; k < K; ++k) tail_buf[(size_t)tile.tail_split * K + k] = sv[(p1 - 1 - p0) * K + k];
+                for (int k = 0; k < K; ++k) tail_buf[(size_t)tile.tail_split * K + k] = o[k];
+                __threadfence();
+            }
+        } else {       // the segment continuing into this tile: head partial
+#pragma unroll
+            for (int k = 0; k < K; ++k) head_buf[(size_t)gtile * K + k] = o[k];
             __threadfence();
         }
-    }
-    if (tid == 0 && tile.cont_split >= 0) {
-        const SRSplit sp = splits[tile.cont_split];
-        uint32_t e = ptr[sp.seg + 1];
-        uint32_t last = (e < p1 ? e : p1) - 1 - p0;
-#pragma unroll
-        for (int k = 0; k < K; ++k) head_buf[(size_t)gtile * K + k] = sv[last * K + k];
-        __threadfence();
     }
     __syncthreads();
     if (tid == 0) {
@@ -173,7 +182,7 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
             double v = acc[k];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if ((tid & 31) == 0) sv[(tid >> 5) * K + k] = v;
+            if ((tid & 31) == 0) wsum[(tid >> 5) * K + k] = v;
         }
         __syncthreads();
         if (tid == 0) {
@@ -181,7 +190,7 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 double v = __ldcg(&tail_buf[(size_t)id * K + k]);
-                for (int w = 0; w < SR_THREADS / 32; ++w) v += sv[w * K + k];
+                for (int w = 0; w < SR_THREADS / 32; ++w) v += wsum[w * K + k];
                 tot[k] = v;
             }
             Prob pr = (sp.problem == tile.problem) ? prob : f.probs[sp.problem];

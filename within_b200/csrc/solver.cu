@@ -164,6 +164,7 @@ void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
     D.inv_e = A.upload(H.inv_e);
     D.ct_col = A.upload(H.ct_col);
     D.ct_val = A.upload(H.ct_val);
+    D.ct_rowsum = A.upload(H.ct_rowsum);
     D.ct_row_slot = A.upload(H.ct_row_slot);
     D.ct_row_red = A.upload(H.ct_row_red);
     D.elim_slot = A.upload(H.elim_slot);
@@ -366,7 +367,7 @@ struct within_solver {
 
 namespace {
 
-constexpr int RED_GRID = 148 * 4;    // fixed reduction grid: deterministic partial order
+constexpr int RED_GRID = 148 * 8;    // fixed reduction grid: deterministic partial order
 
 void set_device(int dev) { CK(cudaSetDevice(dev)); }
 
