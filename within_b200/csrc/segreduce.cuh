@@ -47,12 +47,14 @@ struct SegSumOp {
 };
 
 template <int K>
-constexpr int sr_items() { return K >= 4 ? 1 : (K >= 2 ? 2 : 4); }
+constexpr int sr_items() { return K >= 4 ? 2 : 4; }
 template <int K>
 constexpr int sr_tile() { return SR_THREADS * sr_items<K>(); }
 // resident CTAs per SM the register budget is sized for (no spills at K = 8)
 template <int K>
 constexpr int sr_min_blocks() { return K >= 8 ? 2 : (K >= 4 ? 3 : (K >= 2 ? 4 : 6)); }
+// the scan runs one column at a time over the positions' K-wide values
+using SegItem1 = SegItem<1>;
 
 // F provides:
 //   using Prob = ...;                 (trivially copyable, <= 256 bytes)
@@ -73,7 +75,7 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     constexpr int ITEMS = sr_items<K>();
     constexpr int T = SR_THREADS * ITEMS;
     using Prob = typename F::Prob;
-    using Scan = cub::BlockScan<SegItem<K>, SR_THREADS>;
+    using Scan = cub::BlockScan<SegItem1, SR_THREADS>;
     __shared__ typename Scan::TempStorage scan_tmp;
     __shared__ int headseg[T + 1];
     __shared__ double wsum[(SR_THREADS / 32) * K];
@@ -105,23 +107,39 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     }
     __syncthreads();
 
-    SegItem<K> it[ITEMS];
+    // values of this thread's positions, all K columns (index loads shared)
+    double val[ITEMS][K];
+    int sid[ITEMS];
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         uint32_t p = (uint32_t)(tid * ITEMS + i);
         if (p0 + p < p1) {
-            double v[K];
-            f.value(prob, p0 + p, v);
-#pragma unroll
-            for (int k = 0; k < K; ++k) it[i].v[k] = v[k];
-            it[i].sid = headseg[p];
+            f.value(prob, p0 + p, val[i]);
+            sid[i] = headseg[p];
         } else {
 #pragma unroll
-            for (int k = 0; k < K; ++k) it[i].v[k] = 0.0;
-            it[i].sid = -2;   // past the tile end: never emitted
+            for (int k = 0; k < K; ++k) val[i][k] = 0.0;
+            sid[i] = -2;   // past the tile end: never emitted
         }
     }
-    Scan(scan_tmp).InclusiveScan(it, it, SegSumOp<K>());
+    // one segmented inclusive scan per column; the carried segment id is the
+    // same for every column
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        SegItem1 it[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            it[i].v[0] = val[i][k];
+            it[i].sid = sid[i];
+        }
+        if (k > 0) __syncthreads();   // scan_tmp reuse
+        Scan(scan_tmp).InclusiveScan(it, it, SegSumOp<1>());
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            val[i][k] = it[i].v[0];
+            if (k == K - 1) sid[i] = it[i].sid;
+        }
+    }
 
     // emit at the last position of each segment piece held by this thread
 #pragma unroll
@@ -131,13 +149,13 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
         if (P >= p1) continue;
         const bool last = (P + 1 == p1) || headseg[p + 1] >= 0;
         if (!last) continue;
-        const int sid = it[i].sid;
+        const int sg = sid[i];
         double o[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = it[i].v[k];
-        if (sid >= 0) {
-            if (ptr[sid + 1] <= p1) {
-                f.emit(prob, (uint32_t)sid, o);
+        for (int k = 0; k < K; ++k) o[k] = val[i][k];
+        if (sg >= 0) {
+            if (ptr[sg + 1] <= p1) {
+                f.emit(prob, (uint32_t)sg, o);
             } else {   // the owned segment that runs past the tile: tail partial
 #pragma unroll
                 for (int k = 0; k < K; ++k) tail_buf[(size_t)tile.tail_split * K + k] = o[k];
