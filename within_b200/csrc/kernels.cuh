@@ -232,9 +232,12 @@ k_gather_update(OpParams p, const double* __restrict__ v, double* __restrict__ u
 // positions its level-sorted observation order (identity when sorted).
 struct ScatterProb {
     const uint32_t* seg_ptr;   // level_ptr (n_levels + 1)
-    const uint32_t* order;     // position -> observation (nullptr = identity)
+    const uint32_t* order;     // position -> observation, or -> run (nullptr = identity)
     const double* load;        // loading column (nullptr = intercept)
     uint32_t out_off;          // DOF of level 0 of this column
+    uint32_t ncol;             // run-sum problems: columns of the term
+    const double* run_sum;     // non-null: positions are runs, values run_sum[(run*ncol+col)*K+k]
+    uint32_t col;              // run-sum problems: this problem's column
     uint32_t pad;
 };
 
@@ -252,6 +255,12 @@ struct ScatterF {
     __device__ const uint32_t* seg_ptr(const Prob& pr) const { return pr.seg_ptr; }
     __device__ void value(const Prob& pr, uint32_t pos, double (&v)[K]) const {
         const uint32_t i = pr.order ? __ldg(pr.order + pos) : pos;
+        if (pr.run_sum) {   // combine of run sums formed by the row sweep (sweep.cuh)
+            const double* rs = pr.run_sum + ((size_t)i * pr.ncol + pr.col) * K;
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] = __ldg(rs + k);
+            return;
+        }
         double f = pr.load ? __ldg(pr.load + i) : 1.0;
         if (sqrt_w) f *= __ldg(sqrt_w + i);
 #pragma unroll
