@@ -205,6 +205,22 @@ const char* within_preconditioner_variant_name(const within_preconditioner* p);
 int within_preconditioner_apply(const within_preconditioner* p, const double* x_dev,
                                 double* y_dev, void* stream);
 
+/* ---- Demeaning adjoint (no counterpart in the reference, which has no
+ * differentiation; it differentiates the demeaned output of Solver::solve,
+ * solver.rs:468-473).  For r = demeaned(z) with weights w, a loss gradient v
+ * on r pulls back through one more solve with the same solver:
+ *   a = v / w            within_adjoint_rhs
+ *   s = demeaned(a)      within_solver_solve_batch_device on a
+ *   dL/dz = w * s,  dL/dw = -sum_columns r * (a - s)   within_demean_vjp
+ * Device buffers are column-major (n, k); w NULL means unit weights (then
+ * a = v); the weights must be positive.  grad_z / grad_w may be NULL to skip
+ * them (r and a are then not read for grad_w).  Asynchronous on `stream`. */
+int within_adjoint_rhs(uint64_t n, uint64_t k, const double* v_dev, const double* w_dev,
+                       double* a_dev, void* stream);
+int within_demean_vjp(uint64_t n, uint64_t k, const double* r_dev, const double* a_dev,
+                      const double* s_dev, const double* w_dev, double* grad_z_dev,
+                      double* grad_w_dev, void* stream);
+
 /* ---- diagnostics ---- */
 const char* within_last_error(void);
 /* Kernel launches issued by this library on the calling thread since the last

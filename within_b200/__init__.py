@@ -40,6 +40,7 @@ __all__ = [
     "UnidentifiedDirection",
     "solve",
     "solve_batch",
+    "demean",
     "config",
 ]
 
@@ -486,3 +487,6 @@ def solve_batch(design, Y, weights=None, options: LsmrOptions | None = None,
     r.time_setup = t1 - t0
     r.time_total = time.perf_counter() - t0
     return r
+
+
+from .autograd import demean  # noqa: E402  (differentiable demeaning; imports torch lazily)

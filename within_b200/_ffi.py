@@ -94,6 +94,8 @@ _SIGNATURES = [
     ("within_preconditioner_n", U64, [P]),
     ("within_preconditioner_variant_name", C.c_char_p, [P]),
     ("within_preconditioner_apply", C.c_int, [P, P, P, P]),
+    ("within_adjoint_rhs", C.c_int, [U64, U64, P, P, P, P]),
+    ("within_demean_vjp", C.c_int, [U64, U64, P, P, P, P, P, P, P]),
     ("within_last_error", C.c_char_p, []),
     ("within_launch_count", U64, []),
     ("within_launch_count_reset", None, []),

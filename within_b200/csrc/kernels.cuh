@@ -8,6 +8,7 @@
 // block in block order), so every result is bitwise reproducible.
 #pragma once
 #include <cfloat>
+#include <climits>
 #include <cstdint>
 
 #include "segreduce.cuh"
@@ -43,11 +44,23 @@ struct ColState {
 };
 
 struct Ctl {
-    int all_done;   // every column finished: loop kernels return at entry
-    int k5_skip;    // the vector update of this iteration has nothing to do
-    int err;        // first error code raised on the device
-    int pad;
+    int all_done;     // every column finished: loop kernels return at entry
+    int k5_skip;      // the vector update of this iteration has nothing to do
+    int err;          // first error code raised on the device
+    int bodies_left;  // device-side graph loop: bodies (2 iterations each) still allowed
+    int bodies_run;   // device-side graph loop: bodies executed
+    int pad[3];
 };
+
+// End of one body (two LSMR iterations) of the device-side graph loop: run
+// the body again while a column is active, no error was raised and the body
+// budget (set from maxiter by k_norm_b) is not spent.
+__global__ void k_loop_cond(Ctl* ctl, cudaGraphConditionalHandle h) {
+    const int left = ctl->bodies_left - 1;
+    ctl->bodies_left = left;
+    ctl->bodies_run += 1;
+    cudaGraphSetConditional(h, (!ctl->all_done && !ctl->err && left > 0) ? 1u : 0u);
+}
 
 enum Stop { STOP_NONE = -1, STOP_ZERO_RHS = 0, STOP_INIT_ZERO = 1, STOP_RESID = 2, STOP_NORMAL = 3,
             STOP_MAXITER = 5 };
@@ -886,6 +899,8 @@ k_norm_b(uint32_t n, const double* __restrict__ b, const double* bmax, ColState*
     }
     ctl->all_done = 0;
     ctl->k5_skip = 0;
+    ctl->bodies_left = (int)min((long long)maxiter / 2 + 2, (long long)INT_MAX);
+    ctl->bodies_run = 0;
 }
 
 template <int K>
@@ -993,6 +1008,36 @@ __global__ void k_store_dofs(uint32_t n, uint32_t k_used, const double* __restri
                              double* __restrict__ dst) {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
         for (uint32_t k = 0; k < k_used; ++k) dst[(size_t)k * n + j] = src[(size_t)j * K + k];
+}
+
+// ---------------------------------------------------------------------------
+// Demeaning adjoint (vector-Jacobian product of z -> z - D x*(z, w)).
+// With r = demeaned(z), a = v / w and s = demeaned(a) (one more solve with the
+// same weights and preconditioner):  dL/dz = w * s  and
+// dL/dw = -sum_columns r * (a - s).  Column-major (n, k) buffers.
+
+__global__ void k_adjoint_rhs(uint64_t n, uint32_t k, const double* __restrict__ v,
+                              const double* __restrict__ w, double* __restrict__ a) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double wi = w ? w[i] : 1.0;
+        for (uint32_t c = 0; c < k; ++c) a[(size_t)c * n + i] = w ? v[(size_t)c * n + i] / wi : v[(size_t)c * n + i];
+    }
+}
+
+__global__ void k_demean_vjp(uint64_t n, uint32_t k, const double* __restrict__ r, const double* __restrict__ a,
+                             const double* __restrict__ s, const double* __restrict__ w,
+                             double* __restrict__ gz, double* __restrict__ gw) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double wi = w ? w[i] : 1.0;
+        double g = 0.0;
+        for (uint32_t c = 0; c < k; ++c) {
+            const size_t o = (size_t)c * n + i;
+            const double sv = s[o];
+            if (gz) gz[o] = wi * sv;
+            if (gw) g -= r[o] * (a[o] - sv);
+        }
+        if (gw) gw[i] = g;
+    }
 }
 
 }  // namespace wgpu

@@ -10,9 +10,10 @@
 //   alpha, Givens recurrences, stop test     k_alpha_step (last block)
 //   v, h, h_bar, x update                    k_solution_update
 // -- with all scalar state on the device, so the host never waits inside an
-// iteration.  Two iterations (both state parities) are captured in a CUDA
-// graph that is replayed in bursts; a finished column stops updating and once
-// every column has finished the kernels return at entry.
+// iteration.  Two iterations (both state parities) form the body of a CUDA
+// graph with a conditional WHILE node, so a solve is one graph launch and one
+// host wait; a finished column stops updating and once every column has
+// finished the kernels return at entry.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -349,8 +350,10 @@ struct within_solver {
         int* nonfinite;
         ColState* st;   // [2][K]
         Ctl* ctl;
-        cudaGraphExec_t graph = nullptr;
+        cudaGraphExec_t graph = nullptr;       // two iterations, replayed in bursts
         uint64_t graph_iters = 0;
+        cudaGraphExec_t loop_graph = nullptr;  // the whole loop: a device-side while node
+        bool loop_failed = false;
     } work[4];
     // pinned staging for the host entry points
     double* pin = nullptr;
@@ -371,8 +374,10 @@ struct within_solver {
     bool use_sweep[4] = {false, false, false, false};
 
     ~within_solver() {
-        for (auto& w : work)
+        for (auto& w : work) {
             if (w.graph) cudaGraphExecDestroy(w.graph);
+            if (w.loop_graph) cudaGraphExecDestroy(w.loop_graph);
+        }
         if (pin) cudaFreeHost(pin);
         if (stream) cudaStreamDestroy(stream);
         if (precond && --precond->refs == 0) delete precond;
@@ -616,6 +621,60 @@ void iteration(within_solver& s, within_solver::Work& w, int par, cudaStream_t s
     (void)n;
 }
 
+// The LSMR loop as one graph: a conditional WHILE node whose body is two
+// iterations (both state parities) followed by k_loop_cond, which keeps the
+// loop going while any column is active.  One launch and one host wait per
+// solve, and no iterations run past convergence.  Returns false (and the
+// caller replays the two-iteration graph in bursts) if the runtime refuses
+// conditional nodes.
+template <int K>
+bool build_loop_graph(within_solver& s, within_solver::Work& w) {
+    if (w.loop_graph) return true;
+    if (w.loop_failed) return false;
+    if (const char* e = getenv("WITHIN_GRAPH_LOOP"))
+        if (atoi(e) == 0) {
+            w.loop_failed = true;
+            return false;
+        }
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        w.loop_failed = true;
+        return false;
+    }
+    alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(np_raw);
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &np) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        w.loop_failed = true;
+        return false;
+    }
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    uint64_t before = g_launches;
+    iteration<K>(s, w, 0, cs);
+    iteration<K>(s, w, 1, cs);
+    k_loop_cond<<<1, 1, 0, cs>>>(w.ctl, h);
+    w.graph_iters = g_launches - before + 1;
+    g_launches = before;
+    CK(cudaStreamEndCapture(cs, &body));
+    CK(cudaStreamDestroy(cs));
+    CK(cudaGraphInstantiate(&w.loop_graph, g, 0));
+    CK(cudaGraphDestroy(g));
+    return true;
+}
+
 template <int K>
 void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_t k_used, double tol,
               uint64_t maxiter, double* X_out, double* D_out, within_solve_stats* stats, cudaStream_t st,
@@ -639,6 +698,13 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
                                                       w.counter);
     k_init_vectors<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, w.st);
     g_launches += 6;
+    Ctl ctl{};
+    if (build_loop_graph<K>(s, w)) {
+        CK(cudaGraphLaunch(w.loop_graph, st));
+        CK(cudaMemcpyAsync(&ctl, w.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        g_launches += (uint64_t)ctl.bodies_run * w.graph_iters;
+    } else {
     // capture two iterations once per workspace
     if (!w.graph) {
         cudaStream_t cs;
@@ -655,7 +721,6 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
         CK(cudaGraphDestroy(g));
         CK(cudaStreamDestroy(cs));
     }
-    Ctl ctl{};
     uint64_t done_iters = 0;
     uint64_t burst = 2;
     while (true) {
@@ -670,6 +735,7 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
         burst = std::min<uint64_t>(burst * 2, 32);
         uint64_t left = (maxiter + 2 - done_iters + 1) / 2;
         burst = std::max<uint64_t>(1, std::min(burst, left));
+    }
     }
     if (ctl.err == 5)
         throw WError(ERR_INDEFINITE, "mlsmr: preconditioner not positive definite (<v, Mv> < 0)");
@@ -1195,6 +1261,32 @@ int within_preconditioner_apply(const within_preconditioner* pc, const double* x
         }
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(st));
+    });
+}
+
+int within_adjoint_rhs(uint64_t n, uint64_t k, const double* v_dev, const double* w_dev, double* a_dev,
+                       void* stream) {
+    return guarded([&] {
+        if (n == 0 || k == 0) return;
+        if (!v_dev || !a_dev) throw WError(ERR_INVALID, "adjoint rhs: null buffer");
+        cudaStream_t st = (cudaStream_t)stream;
+        k_adjoint_rhs<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, (uint32_t)k, v_dev, w_dev, a_dev);
+        ++g_launches;
+        CK(cudaGetLastError());
+    });
+}
+
+int within_demean_vjp(uint64_t n, uint64_t k, const double* r_dev, const double* a_dev, const double* s_dev,
+                      const double* w_dev, double* grad_z_dev, double* grad_w_dev, void* stream) {
+    return guarded([&] {
+        if (n == 0 || k == 0) return;
+        if (!s_dev || (grad_w_dev && (!r_dev || !a_dev)))
+            throw WError(ERR_INVALID, "demean vjp: null buffer");
+        cudaStream_t st = (cudaStream_t)stream;
+        k_demean_vjp<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, (uint32_t)k, r_dev, a_dev, s_dev, w_dev,
+                                                                  grad_z_dev, grad_w_dev);
+        ++g_launches;
+        CK(cudaGetLastError());
     });
 }
 
