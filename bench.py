@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--rows", type=int, default=10_000_000)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision batched section")
     ap.add_argument("--cpu-sample-iters", type=int, default=3)
     return ap.parse_args()
 
@@ -187,6 +188,54 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def mixed_section(W, codes, dev, stream, args):
+    """The mixed-precision batched solve on the weighted variant of the same
+    panel (weights lognormal(0, 1), k = 4 right-hand sides) against the plain
+    FP64 single-RHS solve of the same weighted design; errors of both against
+    the FP64 GPU solve at tol 1e-12."""
+    import torch
+    n = codes.shape[0]
+    rng = np.random.default_rng(4)
+    w = rng.lognormal(0.0, 1.0, n)
+    k = 4
+    Y = torch.tensor(np.asfortranarray(rng.standard_normal((n, k))), device=dev).t().contiguous().t()
+    y1 = Y[:, 0].contiguous()
+    s = W.Solver(codes, weights=w, device=dev.index)
+    opts = W.LsmrOptions(tol=args.tol)
+    _, Dref, _ = s.solve_device(Y, W.LsmrOptions(tol=1e-12, maxiter=20000))
+
+    def timed(fn, reps):
+        fn()
+        fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            out = fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / 1e3 / reps, out
+
+    reps = max(2, args.steps // 2)
+    t_plain, (_, Dp, stp) = timed(lambda: s.solve_device(y1, opts), reps)
+    s.set_precision("mixed")
+    t_mx, (_, Dm, stm) = timed(lambda: s.solve_device(Y, opts), reps)
+
+    def err(D, cols):
+        return max(float((D[:, c] - Dref[:, c]).abs().max() / Y[:, c].abs().max()) for c in cols)
+    plain_v = 1.0 / t_plain
+    mixed_v = k / t_mx
+    out = {"k": k, "weights": "lognormal(0,1)", "value": mixed_v, "unit": UNIT, "ms_per_batch": t_mx * 1e3,
+           "iterations_max": max(x[1] for x in stm), "converged": all(x[0] for x in stm),
+           "demeaned_err_vs_fp64_tol1e-12": err(Dm, range(k)),
+           "plain_fp64_k1": {"value": plain_v, "unit": UNIT, "iterations": stp[0][1],
+                             "demeaned_err_vs_fp64_tol1e-12": err(Dp.reshape(-1, 1), [0])},
+           "speedup_vs_plain_fp64": mixed_v / plain_v,
+           "note": "error = max |demeaned - FP64 tol 1e-12 demeaned| / max |y| per column"}
+    del s
+    return out
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
@@ -263,6 +312,7 @@ def run_ours(args):
     batched = {"k": kb, "value": kb / t_b, "unit": UNIT, "ms_per_batch": t_b * 1e3,
                "iterations_max": max(s_[1] for s_ in stb), "demeaned_err_vs_fp64_tol1e-12": err_b,
                "speedup_vs_single": (kb / t_b) / value * world}
+    mixed = None if args.no_mixed else mixed_section(W, codes, dev, stream, args)
     # e2e through the host API (numpy in, numpy out)
     for _ in range(1):
         solver.solve(y, opts)
@@ -312,7 +362,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(n, nd),
         "iterations": it, "lsmr_iters_per_s": world * sum(iters) / t_max, "setup_s": t_setup,
-        "demeaned_err_vs_fp64_tol1e-12": err, "batched_fp64": batched, "roofline": roof,
+        "demeaned_err_vs_fp64_tol1e-12": err, "batched_fp64": batched, "mixed_batched": mixed,
+        "roofline": roof,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * (n + nd)},
         "gpu_launches": launches, "clocks": clk.summary(),

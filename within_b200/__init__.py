@@ -332,7 +332,8 @@ def _as_f64_2d(name, a):
 class Solver:
     """Persistent solver owning its preconditioner (crates/within/src/solver.rs:295-593)."""
 
-    def __init__(self, design, weights=None, preconditioner=None, device: int = -1):
+    def __init__(self, design, weights=None, preconditioner=None, device: int = -1,
+                 precision: str = "fp64"):
         L = _ffi.lib()
         d = _Design(design)
         w = None if weights is None else _as_f64_1d("weights", weights)
@@ -352,6 +353,8 @@ class Solver:
             _ffi.check(L.within_solver_term_layout(h, t, C.byref(nl), C.byref(off), C.byref(nc)))
             terms.append((off.value, nl.value, nc.value))
         self._layout = CoefficientLayout(terms, self._n_dofs)
+        self._precision = "fp64"
+        self.set_precision(precision)
         cap = 1 << 16
         buf = np.zeros(3 * cap, np.uint64)
         k = int(L.within_solver_unidentified(h, _ffi.ptr(buf), cap))
@@ -371,6 +374,20 @@ class Solver:
     @property
     def n_dofs(self) -> int:
         return self._n_dofs
+
+    @property
+    def precision(self) -> str:
+        return self._precision
+
+    def set_precision(self, precision: str) -> None:
+        """"fp64" (default, the reference's arithmetic) or "mixed": FP64
+        iterative refinement on the normal-equation residual around an inner
+        solve whose vectors, operator data and factors are stored in FP32."""
+        code = {"fp64": _ffi.PRECISION_FP64, "mixed": _ffi.PRECISION_MIXED}.get(precision)
+        if code is None:
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        _ffi.check(_ffi.lib().within_solver_set_precision(self._h, code))
+        self._precision = precision
 
     @property
     def n_obs(self) -> int:

@@ -19,16 +19,20 @@ constexpr int MAXQ = 8, MAXC = 4, MAXS = 16;
 constexpr int RED_THREADS = 256;
 
 // Design-operator parameters (operator/design.rs:22-62), passed by value.
-struct OpParams {
+// T is the storage type of the floating operands (double; float for the
+// mixed-precision inner solve); sums are always formed in double.
+template <class T>
+struct OpParamsT {
     uint32_t n;
     int Q;
     const uint32_t* codes[MAXQ];
     uint32_t off[MAXQ], L[MAXQ];
     int ncol[MAXQ];
     int load[MAXQ][MAXC];      // -1 intercept, else loading column
-    const double* loads[MAXS];
-    const double* sqrt_w;      // nullptr = unweighted
+    const T* loads[MAXS];
+    const T* sqrt_w;           // nullptr = unweighted
 };
+using OpParams = OpParamsT<double>;
 
 // Per-column LSMR scalar state (lsmr/recurrence.rs + bidiag.rs), double
 // buffered by iteration parity.
@@ -123,9 +127,9 @@ __device__ bool grid_reduce(const double (&v)[NV], double* partials, unsigned* c
 // D x for 4 consecutive observations [base, base+nr) per call: the code loads
 // are one 16-byte vector per term and all coefficient gathers of the 4 rows
 // are independent, so a thread keeps several memory requests in flight.
-template <int K>
-__device__ __forceinline__ void rows4_dx(const OpParams& p, uint32_t base, int nr,
-                                         const double* __restrict__ x, double (&s)[4][K]) {
+template <int K, class T = double>
+__device__ __forceinline__ void rows4_dx(const OpParamsT<T>& p, uint32_t base, int nr,
+                                         const T* __restrict__ x, double (&s)[4][K]) {
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -145,29 +149,30 @@ __device__ __forceinline__ void rows4_dx(const OpParams& p, uint32_t base, int n
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 if (r >= nr) continue;
-                const double ld = li < 0 ? 1.0 : __ldg(p.loads[li] + base + r);
-                const double* xr = x + (col + code[r]) * K;
+                const double ld = li < 0 ? 1.0 : (double)__ldg(p.loads[li] + base + r);
+                const T* xr = x + (col + code[r]) * K;
 #pragma unroll
-                for (int k = 0; k < K; ++k) s[r][k] += __ldg(xr + k) * ld;
+                for (int k = 0; k < K; ++k) s[r][k] += (double)__ldg(xr + k) * ld;
             }
         }
     }
 }
 
 // y = W^{1/2} D x  (Operator::apply; internal order)
-template <int K>
-__global__ void k_apply(OpParams p, const double* __restrict__ x, double* __restrict__ y) {
+template <int K, class T = double>
+__global__ void k_apply(OpParamsT<T> p, const T* __restrict__ x, T* __restrict__ y, const int* skip = nullptr) {
+    if (skip && *skip) return;
     const uint32_t stride = gridDim.x * blockDim.x * 4;
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * 4; base < p.n; base += stride) {
         const int nr = (int)min(4u, p.n - base);
         double s[4][K];
-        rows4_dx<K>(p, base, nr, x, s);
+        rows4_dx<K, T>(p, base, nr, x, s);
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             if (r >= nr) continue;
-            const double w = p.sqrt_w ? p.sqrt_w[base + r] : 1.0;
+            const double w = p.sqrt_w ? (double)p.sqrt_w[base + r] : 1.0;
 #pragma unroll
-            for (int k = 0; k < K; ++k) y[(size_t)(base + r) * K + k] = p.sqrt_w ? w * s[r][k] : s[r][k];
+            for (int k = 0; k < K; ++k) y[(size_t)(base + r) * K + k] = (T)(p.sqrt_w ? w * s[r][k] : s[r][k]);
         }
     }
 }
@@ -247,6 +252,7 @@ struct ScatterProb {
     const uint32_t* seg_ptr;   // level_ptr (n_levels + 1)
     const uint32_t* order;     // position -> observation, or -> run (nullptr = identity)
     const double* load;        // loading column (nullptr = intercept)
+    const float* load_f;       // the same column in float (mixed-precision inner solve)
     uint32_t out_off;          // DOF of level 0 of this column
     uint32_t ncol;             // run-sum problems: columns of the term
     const double* run_sum;     // non-null: positions are runs, values run_sum[(run*ncol+col)*K+k]
@@ -257,13 +263,13 @@ struct ScatterProb {
 // EPI 0: out = sum (Operator::apply_adjoint)
 // EPI 1: p~ <- sum / beta - (beta / alpha) p~ (bidiag.rs:474-485), per column,
 //        skipping finished columns; beta == 0 (lucky breakdown) zeroes p~.
-template <int K, int EPI>
+template <int K, int EPI, class T = double>
 struct ScatterF {
     using Prob = ScatterProb;
     const ScatterProb* probs;
-    const double* u;
-    const double* sqrt_w;
-    double* out;
+    const T* u;
+    const T* sqrt_w;
+    T* out;
     const ColState* cur;
     __device__ const uint32_t* seg_ptr(const Prob& pr) const { return pr.seg_ptr; }
     __device__ void value(const Prob& pr, uint32_t pos, double (&v)[K]) const {
@@ -274,16 +280,21 @@ struct ScatterF {
             for (int k = 0; k < K; ++k) v[k] = __ldg(rs + k);
             return;
         }
-        double f = pr.load ? __ldg(pr.load + i) : 1.0;
-        if (sqrt_w) f *= __ldg(sqrt_w + i);
+        double f = 1.0;
+        if constexpr (sizeof(T) == 8) {
+            if (pr.load) f = __ldg(pr.load + i);
+        } else {
+            if (pr.load_f) f = (double)__ldg(pr.load_f + i);
+        }
+        if (sqrt_w) f *= (double)__ldg(sqrt_w + i);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = f * u[(size_t)i * K + k];
+        for (int k = 0; k < K; ++k) v[k] = f * (double)u[(size_t)i * K + k];
     }
     __device__ void emit(const Prob& pr, uint32_t seg, const double (&s)[K]) const {
-        double* o = out + ((size_t)pr.out_off + seg) * K;
+        T* o = out + ((size_t)pr.out_off + seg) * K;
         if (EPI == 0) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) o[k] = s[k];
+            for (int k = 0; k < K; ++k) o[k] = (T)s[k];
         } else {
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -298,7 +309,8 @@ struct ScatterF {
 // ---------------------------------------------------------------------------
 // Additive Schwarz apply (schwarz-precond executor.rs + block_elim/solver.rs),
 // all subdomains at once.  See SchwarzHost (host.hpp) for the layout.
-struct SchwarzDev {
+template <class T>
+struct SchwarzDevT {
     uint32_t n_sub;
     const uint32_t* loc_ptr;
     const uint32_t* n_elim;
@@ -307,43 +319,44 @@ struct SchwarzDev {
     const uint32_t* red_n;
     const int* mode;
     const uint32_t* glob;
-    const double* scale;
+    const T* scale;
     const uint32_t* slot_sub;
-    const double* inv_e;
+    const T* inv_e;
     const uint32_t* ct_col;
-    const double* ct_val;       // C^T / D_e
-    const double* ct_rowsum;
+    const T* ct_val;       // C^T / D_e
+    const T* ct_rowsum;
     const uint32_t* ct_row_slot;
     const uint32_t* ct_row_red;
     const uint32_t* elim_slot;
     const uint32_t* c_col;
-    const double* c_val;
+    const T* c_val;
     const uint32_t* red_sub;
     const uint32_t* dense_row_slot;
     const uint32_t* dense_col;
-    const double* dense_val;
-    const double* dinv;
+    const T* dense_val;
+    const T* dinv;
     const uint32_t* fwd_row;
     const uint32_t* fwd_col;
-    const double* fwd_val;
+    const T* fwd_val;
     const uint32_t* bwd_row;
     const uint32_t* bwd_col;
-    const double* bwd_val;
+    const T* bwd_val;
     const uint32_t* dof_slot;
     const uint32_t* kept_ptr;
     const uint32_t* core_row_slot;
     const uint32_t* core_col;
-    const double* core_val;
+    const T* core_val;
     // work (K-interleaved)
-    double* rl;   // restricted, folded local rhs (per local slot)
-    double* sl;   // local solution (per local slot)
-    double* rb;   // reduced rhs
-    double* yv;   // forward-substitution values
-    double* xv;   // reduced solution
-    double* m1;   // per subdomain: mean of rl (floating) else 0
-    double* m2;   // per subdomain: mean of the reduced rhs (floating) else 0
-    double* m3;   // per subdomain: mean of the local solution (floating) else 0
+    T* rl;   // restricted, folded local rhs (per local slot)
+    T* sl;   // local solution (per local slot)
+    T* rb;   // reduced rhs
+    T* yv;   // forward-substitution values
+    T* xv;   // reduced solution
+    T* m1;   // per subdomain: mean of rl (floating) else 0
+    T* m2;   // per subdomain: mean of the reduced rhs (floating) else 0
+    T* m3;   // per subdomain: mean of the local solution (floating) else 0
 };
+using SchwarzDev = SchwarzDevT<double>;
 
 struct SegProb {          // generic: one pointer array + a segment base
     const uint32_t* seg_ptr;
@@ -351,11 +364,9 @@ struct SegProb {          // generic: one pointer array + a segment base
     uint32_t pad;
 };
 
-__device__ __forceinline__ int sd_mode(const SchwarzDev& S, uint32_t s) { return S.mode[s]; }
-
 // solution of kept index k (reduced slot u) after the gauge / cover read-back
-template <int K>
-__device__ __forceinline__ void kept_solution(const SchwarzDev& S, uint32_t u, double (&o)[K]) {
+template <int K, class T = double>
+__device__ __forceinline__ void kept_solution(const SchwarzDevT<T>& S, uint32_t u, double (&o)[K]) {
     const uint32_t s = S.red_sub[u];
     const int m = S.mode[s];
     if (m == 0) {
@@ -373,12 +384,12 @@ __device__ __forceinline__ void kept_solution(const SchwarzDev& S, uint32_t u, d
 }
 
 // S1: restrict + fold, per-subdomain sums -> m1 (solver.rs:445-451, domain.rs:133-152)
-template <int K>
+template <int K, class T = double>
 struct RestrictF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
-    const double* r;
+    SchwarzDevT<T> S;
+    const T* r;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t j, double (&v)[K]) const {
         const uint32_t g = __ldg(S.glob + j);
@@ -400,11 +411,11 @@ struct RestrictF {
 
 // S3: reduced rhs  rhs_k + C^T D_e^-1 rhs_e  (solver.rs:360-371).  With the
 // floating mean m: sum_e (C^T/D_e)[k,e] (r_e - m) = sum_e (C^T/D_e) r_e - m * rowsum_k.
-template <int K>
+template <int K, class T = double>
 struct CtF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         const uint32_t e = __ldg(S.ct_col + a);
@@ -432,11 +443,11 @@ struct CtF {
 
 // S4: per-subdomain sum of the kept reduced rhs -> floating mean (m2) or the
 // explicit ground's rhs (solver.rs:372-384)
-template <int K>
+template <int K, class T = double>
 struct KeptSumF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t q, double (&v)[K]) const {
         const uint32_t u = __ldg(S.ct_row_red + q);
@@ -458,23 +469,23 @@ struct KeptSumF {
     }
 };
 
-template <int K>
-__device__ __forceinline__ void reduced_rhs(const SchwarzDev& S, uint32_t u, double (&b)[K]) {
+template <int K, class T = double>
+__device__ __forceinline__ void reduced_rhs(const SchwarzDevT<T>& S, uint32_t u, double (&b)[K]) {
     const uint32_t s = S.red_sub[u];
 #pragma unroll
     for (int k = 0; k < K; ++k) b[k] = S.rb[(size_t)u * K + k] - S.m2[(size_t)s * K + k];
 }
 
 // S5 (small systems): x = G b with the dense generalised inverse G
-template <int K>
+template <int K, class T = double>
 struct DenseF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         double b[K];
-        reduced_rhs<K>(S, __ldg(S.dense_col + a), b);
+        reduced_rhs<K, T>(S, __ldg(S.dense_col + a), b);
         const double g = __ldg(S.dense_val + a);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = g * b[k];
@@ -488,11 +499,11 @@ struct DenseF {
 
 // S5 (factored systems), one round of L y = b: y_u = b_u - sum_v L[u,v] y_v,
 // and z_u = y_u / d_u for the backward pass.
-template <int K>
+template <int K, class T = double>
 struct FwdF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         const uint32_t c = __ldg(S.fwd_col + a);
@@ -503,7 +514,7 @@ struct FwdF {
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t u = S.fwd_row[p.seg_base + seg];
         double b[K];
-        reduced_rhs<K>(S, u, b);
+        reduced_rhs<K, T>(S, u, b);
         const double di = S.dinv[u];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -516,11 +527,11 @@ struct FwdF {
 
 // dense core of a round-scheduled factor: x_core = G_core y_core, between the
 // forward and the backward sweeps
-template <int K>
+template <int K, class T = double>
 struct CoreF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         const uint32_t c = __ldg(S.core_col + a);
@@ -536,11 +547,11 @@ struct CoreF {
 };
 
 // one round of L^T x = z: x_v = z_v - sum_u L[u,v] x_u (rounds in reverse)
-template <int K>
+template <int K, class T = double>
 struct BwdF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         const uint32_t c = __ldg(S.bwd_col + a);
@@ -558,18 +569,18 @@ struct BwdF {
 // S6: back-substitution  x_e = D_e^-1 rhs_e + D_e^-1 C x_k  (solver.rs:41-77);
 // C is stored pre-divided by D_e, and a column with bit 31 clear reads the
 // reduced solution directly (floating subdomain).
-template <int K>
+template <int K, class T = double>
 struct CF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         const uint32_t cc = __ldg(S.c_col + a);
         const double c = __ldg(S.c_val + a);
         double x[K];
         if (cc & 0x80000000u) {
-            kept_solution<K>(S, cc & 0x7fffffffu, x);
+            kept_solution<K, T>(S, cc & 0x7fffffffu, x);
         } else {
 #pragma unroll
             for (int k = 0; k < K; ++k) x[k] = S.xv[(size_t)cc * K + k];
@@ -588,11 +599,11 @@ struct CF {
 };
 
 // S7: kept-block read-back and per-subdomain solution mean (floating)
-template <int K>
+template <int K, class T = double>
 struct MeanF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
+    SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t j, double (&v)[K]) const {
         const uint32_t s = __ldg(S.slot_sub + j);
@@ -602,7 +613,7 @@ struct MeanF {
 #pragma unroll
             for (int k = 0; k < K; ++k) v[k] = S.sl[(size_t)j * K + k];
         } else {
-            kept_solution<K>(S, S.red_off[s] + (kk - ne), v);
+            kept_solution<K, T>(S, S.red_off[s] + (kk - ne), v);
 #pragma unroll
             for (int k = 0; k < K; ++k) S.sl[(size_t)j * K + k] = v[k];
         }
@@ -618,12 +629,12 @@ struct MeanF {
 
 // S8: unfold + prolongate  z_g = sum over subdomains of w * f * (x - mean)
 // (domain.rs:154-171), a gather per DOF in subdomain order.
-template <int K>
+template <int K, class T = double>
 struct ProlongF {
     using Prob = SegProb;
     const SegProb* probs;
-    SchwarzDev S;
-    double* z;
+    SchwarzDevT<T> S;
+    T* z;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
     __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
         const uint32_t j = __ldg(S.dof_slot + a);
@@ -633,9 +644,9 @@ struct ProlongF {
         for (int k = 0; k < K; ++k) v[k] = sc * (S.sl[(size_t)j * K + k] - S.m3[(size_t)s * K + k]);
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
-        double* o = z + (size_t)(p.seg_base + seg) * K;
+        T* o = z + (size_t)(p.seg_base + seg) * K;
 #pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = s[k];
+        for (int k = 0; k < K; ++k) o[k] = (T)s[k];
     }
 };
 
@@ -643,14 +654,14 @@ struct ProlongF {
 // LSMR vector kernels over the DOF space
 
 // v = d * p~ (Diagonal, operator/schwarz.rs:64-81) or v = p~ (identity)
-template <int K>
-__global__ void k_diag_apply(uint32_t n, const double* __restrict__ d, const double* __restrict__ p,
-                             double* __restrict__ v, const Ctl* ctl) {
+template <int K, class T = double>
+__global__ void k_diag_apply(uint32_t n, const T* __restrict__ d, const T* __restrict__ p,
+                             T* __restrict__ v, const Ctl* ctl) {
     if (ctl && ctl->all_done) return;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const double dj = d ? d[j] : 1.0;
+        const double dj = d ? (double)d[j] : 1.0;
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[(size_t)j * K + k] = dj * p[(size_t)j * K + k];
+        for (int k = 0; k < K; ++k) v[(size_t)j * K + k] = (T)(dj * (double)p[(size_t)j * K + k]);
     }
 }
 

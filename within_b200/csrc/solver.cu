@@ -30,6 +30,7 @@
 #include "../../include/within_gpu.h"
 #include "host.hpp"
 #include "kernels.cuh"
+#include "refine.cuh"
 #include "sweep.cuh"
 
 using namespace wgpu;
@@ -131,7 +132,12 @@ struct within_preconditioner {
     Arena arena;
     double* inv_diag = nullptr;
     SchwarzHost host;            // kept for plan building and statistics
+    std::vector<double> host_inv_diag;
     SchwarzDev dev_const{};      // pointers into arena (work pointers filled per user)
+    // FP32 copies of the factor values (mixed-precision inner solve), built on first use
+    SchwarzDevT<float> dev_const_f{};
+    float* inv_diag_f = nullptr;
+    bool has_f = false;
     // per-step segment problems
     SegProb *p_restrict = nullptr, *p_ct = nullptr, *p_kept = nullptr, *p_dense = nullptr,
             *p_fwd = nullptr, *p_bwd = nullptr, *p_c = nullptr, *p_prolong = nullptr,
@@ -218,16 +224,74 @@ void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
 }
 
 // Schwarz work buffers of one user (solver) for K columns.
-struct SchwarzWork {
-    double *rl = nullptr, *sl = nullptr, *rb = nullptr, *yv = nullptr, *xv = nullptr, *m1 = nullptr,
-           *m2 = nullptr, *m3 = nullptr;
+template <class T>
+struct SchwarzWorkT {
+    T *rl = nullptr, *sl = nullptr, *rb = nullptr, *yv = nullptr, *xv = nullptr, *m1 = nullptr, *m2 = nullptr,
+      *m3 = nullptr;
 };
+using SchwarzWork = SchwarzWorkT<double>;
+
+template <class T>
+std::vector<T> cast_vec(const std::vector<double>& v) {
+    return std::vector<T>(v.begin(), v.end());
+}
+
+// FP32 factor values for the mixed-precision inner solve (index arrays shared).
+void ensure_precond_f(within_preconditioner& P) {
+    std::lock_guard<std::mutex> g(P.mu);
+    if (P.has_f) return;
+    Arena& A = P.arena;
+    if (P.kind == 2) {
+        P.inv_diag_f = A.upload(cast_vec<float>(P.host_inv_diag));
+    } else {
+        const SchwarzHost& H = P.host;
+        const SchwarzDev& D = P.dev_const;
+        SchwarzDevT<float>& F = P.dev_const_f;
+        F.n_sub = D.n_sub;
+        F.loc_ptr = D.loc_ptr;
+        F.n_elim = D.n_elim;
+        F.red_off = D.red_off;
+        F.n_kept = D.n_kept;
+        F.red_n = D.red_n;
+        F.mode = D.mode;
+        F.glob = D.glob;
+        F.slot_sub = D.slot_sub;
+        F.ct_col = D.ct_col;
+        F.ct_row_slot = D.ct_row_slot;
+        F.ct_row_red = D.ct_row_red;
+        F.elim_slot = D.elim_slot;
+        F.c_col = D.c_col;
+        F.red_sub = D.red_sub;
+        F.dense_row_slot = D.dense_row_slot;
+        F.dense_col = D.dense_col;
+        F.fwd_row = D.fwd_row;
+        F.fwd_col = D.fwd_col;
+        F.bwd_row = D.bwd_row;
+        F.bwd_col = D.bwd_col;
+        F.dof_slot = D.dof_slot;
+        F.kept_ptr = D.kept_ptr;
+        F.core_row_slot = D.core_row_slot;
+        F.core_col = D.core_col;
+        F.scale = A.upload(cast_vec<float>(H.scale));
+        F.inv_e = A.upload(cast_vec<float>(H.inv_e));
+        F.ct_val = A.upload(cast_vec<float>(H.ct_val));
+        F.ct_rowsum = A.upload(cast_vec<float>(H.ct_rowsum));
+        F.c_val = A.upload(cast_vec<float>(H.c_val));
+        F.dense_val = A.upload(cast_vec<float>(H.dense_val));
+        F.dinv = A.upload(cast_vec<float>(H.dinv));
+        F.fwd_val = A.upload(cast_vec<float>(H.fwd_val));
+        F.bwd_val = A.upload(cast_vec<float>(H.bwd_val));
+        F.core_val = A.upload(cast_vec<float>(H.core_val));
+    }
+    P.has_f = true;
+}
 
 // Everything one user of a (possibly shared) preconditioner mutates: the tile
 // plans' partial/counter buffers and the work vectors, per column bucket K.
 struct KPlans {
     DevPlan restrict_, ct, kept, dense, fwd, bwd, c, prolong, core;
     SchwarzWork w;
+    SchwarzWorkT<float> wf;   // mixed-precision inner solve, allocated on first use
     bool ready = false;
 };
 
@@ -291,31 +355,67 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     return kp;
 }
 
-template <int K>
-void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const double* r, double* z, const int* skip,
+// FP32 work vectors of one user (allocated outside any stream capture).
+SchwarzWorkT<float>& schwarz_user_work_f(SchwarzUser& U, const within_preconditioner& P, int K) {
+    KPlans& kp = schwarz_user_plans(U, P, K);
+    if (!kp.wf.rl) {
+        const SchwarzHost& H = P.host;
+        size_t nl = H.glob.size(), nr = H.n_red, ns = H.n_sub;
+        kp.wf.rl = U.arena.alloc<float>(nl * K);
+        kp.wf.sl = U.arena.alloc<float>(nl * K);
+        kp.wf.rb = U.arena.alloc<float>(nr * K);
+        kp.wf.yv = U.arena.alloc<float>(nr * K);
+        kp.wf.xv = U.arena.alloc<float>(nr * K);
+        kp.wf.m1 = U.arena.alloc<float>(ns * K);
+        kp.wf.m2 = U.arena.alloc<float>(ns * K);
+        kp.wf.m3 = U.arena.alloc<float>(ns * K);
+    }
+    return kp.wf;
+}
+
+template <int K, class T = double>
+void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const T* r, T* z, const int* skip,
                    cudaStream_t st) {
     KPlans& kp = schwarz_user_plans(U, P, K);
-    SchwarzDev S = P.dev_const;
-    S.rl = kp.w.rl;
-    S.sl = kp.w.sl;
-    S.rb = kp.w.rb;
-    S.yv = kp.w.yv;
-    S.xv = kp.w.xv;
-    S.m1 = kp.w.m1;
-    S.m2 = kp.w.m2;
-    S.m3 = kp.w.m3;
-    launch_sr<RestrictF<K>, K>(RestrictF<K>{P.p_restrict, S, r}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
-    launch_sr<CtF<K>, K>(CtF<K>{P.p_ct, S}, kp.ct, 0, kp.ct.n_tiles, skip, st);
-    launch_sr<KeptSumF<K>, K>(KeptSumF<K>{P.p_kept, S}, kp.kept, 0, kp.kept.n_tiles, skip, st);
-    if (P.has_dense) launch_sr<DenseF<K>, K>(DenseF<K>{P.p_dense, S}, kp.dense, 0, kp.dense.n_tiles, skip, st);
+    SchwarzDevT<T> S;
+    SchwarzWorkT<T>* w;
+    if constexpr (sizeof(T) == 8) {
+        S = P.dev_const;
+        w = &kp.w;
+    } else {
+        S = P.dev_const_f;
+        w = &schwarz_user_work_f(U, P, K);
+    }
+    S.rl = w->rl;
+    S.sl = w->sl;
+    S.rb = w->rb;
+    S.yv = w->yv;
+    S.xv = w->xv;
+    S.m1 = w->m1;
+    S.m2 = w->m2;
+    S.m3 = w->m3;
+    using RF = RestrictF<K, T>;
+    using CtFT = CtF<K, T>;
+    using KS = KeptSumF<K, T>;
+    using DF = DenseF<K, T>;
+    using FF = FwdF<K, T>;
+    using CoF = CoreF<K, T>;
+    using BF = BwdF<K, T>;
+    using CFT = CF<K, T>;
+    using MF = MeanF<K, T>;
+    using PF = ProlongF<K, T>;
+    launch_sr<RF, K>(RF{P.p_restrict, S, r}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
+    launch_sr<CtFT, K>(CtFT{P.p_ct, S}, kp.ct, 0, kp.ct.n_tiles, skip, st);
+    launch_sr<KS, K>(KS{P.p_kept, S}, kp.kept, 0, kp.kept.n_tiles, skip, st);
+    if (P.has_dense) launch_sr<DF, K>(DF{P.p_dense, S}, kp.dense, 0, kp.dense.n_tiles, skip, st);
     for (uint32_t r = 0; r < P.n_rounds; ++r)
-        launch_sr<FwdF<K>, K>(FwdF<K>{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
-    if (P.has_core) launch_sr<CoreF<K>, K>(CoreF<K>{P.p_core, S}, kp.core, 0, kp.core.n_tiles, skip, st);
+        launch_sr<FF, K>(FF{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
+    if (P.has_core) launch_sr<CoF, K>(CoF{P.p_core, S}, kp.core, 0, kp.core.n_tiles, skip, st);
     for (uint32_t r = P.n_rounds; r-- > 0;)
-        launch_sr<BwdF<K>, K>(BwdF<K>{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
-    launch_sr<CF<K>, K>(CF<K>{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
-    launch_sr<MeanF<K>, K>(MeanF<K>{P.p_restrict, S}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
-    launch_sr<ProlongF<K>, K>(ProlongF<K>{P.p_prolong, S, z}, kp.prolong, 0, kp.prolong.n_tiles, skip, st);
+        launch_sr<BF, K>(BF{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
+    launch_sr<CFT, K>(CFT{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
+    launch_sr<MF, K>(MF{P.p_restrict, S}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
+    launch_sr<PF, K>(PF{P.p_prolong, S, z}, kp.prolong, 0, kp.prolong.n_tiles, skip, st);
 }
 
 }  // namespace
@@ -337,6 +437,10 @@ struct within_solver {
     uint32_t* perm = nullptr;               // internal -> caller (nullptr = identity)
     std::vector<ScatterProb> scatter_host;  // problems (same for all K)
     ScatterProb* scatter_probs = nullptr;
+    // mixed precision: FP32 copies of sqrt(w) and the loading columns
+    OpParamsT<float> op_f{};
+    ScatterProb* scatter_probs_f = nullptr;
+    bool has_f = false;
     std::vector<std::vector<uint32_t>> level_ptr_host;   // per term
     DevPlan scatter_plan[4];
     bool scatter_ready[4] = {false, false, false, false};
@@ -355,6 +459,16 @@ struct within_solver {
         cudaGraphExec_t loop_graph = nullptr;  // the whole loop: a device-side while node
         bool loop_failed = false;
     } work[4];
+    // mixed-precision workspaces per K (refine.cuh)
+    struct MixedWork {
+        bool ready = false;
+        double *r64, *g64, *x64;
+        float *res, *z, *p, *q, *t, *d;
+        CgCol* st;
+        Ctl* ctl;
+        cudaGraphExec_t loop_graph = nullptr;
+        uint64_t body_launches = 0;
+    } mixed[4];
     // pinned staging for the host entry points
     double* pin = nullptr;
     size_t pin_n = 0;
@@ -378,6 +492,8 @@ struct within_solver {
             if (w.graph) cudaGraphExecDestroy(w.graph);
             if (w.loop_graph) cudaGraphExecDestroy(w.loop_graph);
         }
+        for (auto& m : mixed)
+            if (m.loop_graph) cudaGraphExecDestroy(m.loop_graph);
         if (pin) cudaFreeHost(pin);
         if (stream) cudaStreamDestroy(stream);
         if (precond && --precond->refs == 0) delete precond;
@@ -571,27 +687,32 @@ within_solver::Work& ensure_work(within_solver& s, int K) {
     return w;
 }
 
-template <int K, int EPI>
-void scatter(within_solver& s, const double* u, double* out, const ColState* cur, const int* skip,
-             cudaStream_t st) {
+template <int K, int EPI, class T = double>
+void scatter(within_solver& s, const T* u, T* out, const ColState* cur, const int* skip, cudaStream_t st) {
     const DevPlan& pl = s.scatter_plan[kidx(K)];
-    ScatterF<K, EPI> f{s.scatter_probs, u, s.op.sqrt_w, out, cur};
-    launch_sr<ScatterF<K, EPI>, K>(f, pl, 0, pl.n_tiles, skip, st);
+    if constexpr (sizeof(T) == 8) {
+        ScatterF<K, EPI> f{s.scatter_probs, u, s.op.sqrt_w, out, cur};
+        launch_sr<ScatterF<K, EPI>, K>(f, pl, 0, pl.n_tiles, skip, st);
+    } else {
+        ScatterF<K, EPI, float> f{s.scatter_probs_f, u, s.op_f.sqrt_w, out, cur};
+        launch_sr<ScatterF<K, EPI, float>, K>(f, pl, 0, pl.n_tiles, skip, st);
+    }
 }
 
-template <int K>
-void precond_apply(within_solver& s, within_solver::Work& w, const double* p, double* v, const int* skip,
-                   cudaStream_t st) {
+template <int K, class T = double>
+void precond_apply(within_solver& s, Ctl* ctl, const T* p, T* v, const int* skip, cudaStream_t st) {
     const uint32_t nd = (uint32_t)s.n_dofs;
     if (!s.precond) {
-        k_diag_apply<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, nullptr, p, v, skip ? w.ctl : nullptr);
+        k_diag_apply<K, T><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, nullptr, p, v, skip ? ctl : nullptr);
         ++g_launches;
     } else if (s.precond->kind == 2) {
-        k_diag_apply<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, s.precond->inv_diag, p, v,
-                                                                    skip ? w.ctl : nullptr);
+        const T* d;
+        if constexpr (sizeof(T) == 8) d = s.precond->inv_diag;
+        else d = s.precond->inv_diag_f;
+        k_diag_apply<K, T><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, d, p, v, skip ? ctl : nullptr);
         ++g_launches;
     } else {
-        schwarz_apply<K>(*s.precond, s.schwarz, p, v, skip, st);
+        schwarz_apply<K, T>(*s.precond, s.schwarz, p, v, skip, st);
     }
 }
 
@@ -613,7 +734,7 @@ void iteration(within_solver& s, within_solver::Work& w, int par, cudaStream_t s
         ++g_launches;
         scatter<K, 1>(s, w.u, w.p, cur, skip, st);
     }
-    precond_apply<K>(s, w, w.p, w.v, skip, st);
+    precond_apply<K>(s, w.ctl, w.p, w.v, skip, st);
     k_alpha_step<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, cur, nxt, w.ctl, w.partials, w.counter);
     ++g_launches;
     k_solution_update<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, nxt, w.ctl);
@@ -693,7 +814,7 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
                                                   w.ctl, w.partials, w.counter);
     k_scale_u<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, w.b, w.u, w.st);
     scatter<K, 0>(s, w.u, w.p, w.st, nullptr, st);
-    precond_apply<K>(s, w, w.p, w.v, nullptr, st);
+    precond_apply<K>(s, w.ctl, w.p, w.v, nullptr, st);
     k_alpha_init<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, w.st, w.st + 8, w.ctl, w.partials,
                                                       w.counter);
     k_init_vectors<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, w.st);
@@ -775,6 +896,181 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
         }
 }
 
+// ---------------------------------------------------------------------------
+// mixed precision (refine.cuh): FP32 copies of the operator's floating data,
+// of the preconditioner's factor values and FP32 inner-solve workspaces.
+void ensure_mixed_data(within_solver& s) {
+    if (s.has_f) return;
+    Arena& A = s.arena;
+    const HostDesign& D = s.design;
+    s.op_f.n = s.op.n;
+    s.op_f.Q = s.op.Q;
+    for (int t = 0; t < MAXQ; ++t) {
+        s.op_f.codes[t] = s.op.codes[t];
+        s.op_f.off[t] = s.op.off[t];
+        s.op_f.L[t] = s.op.L[t];
+        s.op_f.ncol[t] = s.op.ncol[t];
+        for (int c = 0; c < MAXC; ++c) s.op_f.load[t][c] = s.op.load[t][c];
+    }
+    for (size_t k = 0; k < D.loads.size(); ++k) s.op_f.loads[k] = A.upload(cast_vec<float>(D.loads[k]));
+    if (s.op.sqrt_w) {
+        std::vector<double> sw(s.n_obs);
+        CK(cudaMemcpy(sw.data(), s.op.sqrt_w, s.n_obs * sizeof(double), cudaMemcpyDeviceToHost));
+        s.op_f.sqrt_w = A.upload(cast_vec<float>(sw));
+    }
+    std::vector<ScatterProb> pf = s.scatter_host;
+    size_t i = 0;
+    for (size_t t = 0; t < D.terms.size(); ++t)
+        for (size_t c = 0; c < D.terms[t].cols.size(); ++c, ++i)
+            pf[i].load_f = D.terms[t].cols[c] < 0 ? nullptr : s.op_f.loads[D.terms[t].cols[c]];
+    s.scatter_probs_f = A.upload(pf);
+    if (s.precond) ensure_precond_f(*s.precond);
+    s.has_f = true;
+}
+
+within_solver::MixedWork& ensure_mixed(within_solver& s, int K) {
+    auto& m = s.mixed[kidx(K)];
+    if (m.ready) return m;
+    ensure_work(s, K);   // FP64 rhs staging, reduction scratch, plans
+    ensure_mixed_data(s);
+    Arena& A = s.arena;
+    m.r64 = A.alloc<double>(s.n_obs * K);
+    m.g64 = A.alloc<double>(s.n_dofs * K);
+    m.x64 = A.alloc<double>(s.n_dofs * K);
+    m.t = A.alloc<float>(s.n_obs * K);
+    m.res = A.alloc<float>(s.n_dofs * K);
+    m.z = A.alloc<float>(s.n_dofs * K);
+    m.p = A.alloc<float>(s.n_dofs * K);
+    m.q = A.alloc<float>(s.n_dofs * K);
+    m.d = A.alloc<float>(s.n_dofs * K);
+    m.st = A.alloc<CgCol>(8);
+    m.ctl = A.alloc<Ctl>(1);
+    if (s.precond && s.precond->kind == 1) schwarz_user_work_f(s.schwarz, *s.precond, K);
+    m.ready = true;
+    return m;
+}
+
+// one inner CG iteration in FP32 storage
+template <int K>
+void cg_iteration(within_solver& s, within_solver::Work& w, within_solver::MixedWork& m, cudaStream_t st) {
+    const uint32_t nd = (uint32_t)s.n_dofs;
+    const int* skip = &m.ctl->all_done;
+    k_apply<K, float><<<grid_for(s.n_obs, 256 * 4, 148 * 8), 256, 0, st>>>(s.op_f, m.p, m.t, skip);
+    scatter<K, 0, float>(s, m.t, m.q, nullptr, skip, st);
+    k_cg_alpha<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.p, m.q, m.st, m.ctl, w.partials, w.counter);
+    k_cg_update<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.p, m.q, m.d, m.res, m.st, m.ctl);
+    g_launches += 3;
+    precond_apply<K, float>(s, m.ctl, m.res, m.z, skip, st);
+    k_cg_beta<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.st, m.ctl, w.partials, w.counter);
+    k_cg_dir<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.z, m.p, m.st, m.ctl);
+    g_launches += 2;
+}
+
+template <int K>
+void build_cg_loop(within_solver& s, within_solver::Work& w, within_solver::MixedWork& m) {
+    if (m.loop_graph) return;
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(np_raw);
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = g_launches;
+    cg_iteration<K>(s, w, m, cs);
+    k_loop_cond<<<1, 1, 0, cs>>>(m.ctl, h);
+    m.body_launches = g_launches - before + 1;
+    g_launches = before;
+    CK(cudaStreamEndCapture(cs, &body));
+    CK(cudaStreamDestroy(cs));
+    CK(cudaGraphInstantiate(&m.loop_graph, g, 0));
+    CK(cudaGraphDestroy(g));
+}
+
+// Mixed-precision solve of K columns: FP64 refinement steps around FP32-storage
+// CG on the normal equations (refine.cuh); same outputs as run_lsmr.
+template <int K>
+void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, uint64_t maxiter, double* X_out,
+               double* D_out, within_solve_stats* stats, cudaStream_t st, double t_setup0) {
+    auto& w = ensure_work(s, K);
+    auto& m = ensure_mixed(s, K);
+    const uint32_t n = (uint32_t)s.n_obs, nd = (uint32_t)s.n_dofs;
+    CK(cudaMemsetAsync(w.nonfinite, 0, sizeof(int), st));
+    k_load_rhs<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, k_used, Y, s.perm, s.op.sqrt_w, w.yint, w.b, w.partials,
+                                                    w.counter, w.bmax, w.nonfinite);
+    ++g_launches;
+    int nonfinite = 0;
+    CK(cudaMemcpyAsync(&nonfinite, w.nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (nonfinite) throw WError(ERR_INVALID, "response must be finite (a non-finite value was found)");
+    const double t_solve0 = now_s();
+    build_cg_loop<K>(s, w, m);
+    CK(cudaMemsetAsync(m.x64, 0, (size_t)nd * K * sizeof(double), st));
+    k_cg_setup<<<1, 1, 0, st>>>(m.st, (int)k_used, tol, (long long)std::min<uint64_t>(maxiter, (uint64_t)1 << 40),
+                                m.ctl);
+    ++g_launches;
+    CgCol fin[8];
+    Ctl ctl{};
+    for (int outer = 0;; ++outer) {
+        k_resid64<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, m.x64, w.b, m.r64, m.st, w.partials, w.counter);
+        scatter<K, 0>(s, m.r64, m.g64, nullptr, nullptr, st);
+        k_cg_start<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.g64, m.res, m.d);
+        precond_apply<K, float>(s, m.ctl, m.res, m.z, nullptr, st);
+        k_cg_init<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.p, m.st, m.ctl, outer == 0 ? 1 : 0,
+                                                               w.partials, w.counter);
+        g_launches += 3;
+        CK(cudaMemcpyAsync(&ctl, m.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (ctl.all_done || ctl.err) break;
+        const int runs0 = ctl.bodies_run;
+        CK(cudaGraphLaunch(m.loop_graph, st));
+        k_add_delta<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.d, m.x64);
+        ++g_launches;
+        CK(cudaMemcpyAsync(&ctl, m.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        g_launches += (uint64_t)(ctl.bodies_run - runs0) * m.body_launches;
+        if (ctl.err || outer > 64) break;
+    }
+    CK(cudaMemcpyAsync(fin, m.st, sizeof(CgCol) * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (ctl.err == 5)
+        throw WError(ERR_INDEFINITE, "mixed solve: preconditioner not positive definite (<g, M g> < 0)");
+    const double t_solve1 = now_s();
+    k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, m.x64, w.yint, w.dm);
+    ++g_launches;
+    if (D_out) {
+        k_store_obs<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, k_used, w.dm, s.perm, D_out);
+        ++g_launches;
+    }
+    if (X_out) {
+        k_store_dofs<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, k_used, m.x64, X_out);
+        ++g_launches;
+    }
+    CK(cudaStreamSynchronize(st));
+    const double t_end = now_s();
+    if (stats)
+        for (uint32_t k = 0; k < k_used; ++k) {
+            const CgCol& c = fin[k];
+            within_solve_stats& o = stats[k];
+            o.converged = (c.stop == STOP_RESID || c.stop == STOP_NORMAL || c.stop == STOP_ZERO_RHS ||
+                           c.stop == STOP_INIT_ZERO) ? 1 : 0;
+            o.iterations = (uint64_t)c.itn;
+            o.residual = c.bnorm > 0.0 ? sqrt(c.rnorm2) / c.bnorm : 0.0;
+            o.time_setup = t_solve0 - t_setup0;
+            o.time_solve = t_solve1 - t_solve0;
+            o.time_total = t_end - t_setup0;
+        }
+}
+
 void dispatch_solve(within_solver& s, const double* Y_dev, uint64_t k, double tol, uint64_t maxiter,
                     double* X_dev, double* D_dev, within_solve_stats* stats, cudaStream_t st) {
     const double t0 = now_s();
@@ -786,6 +1082,15 @@ void dispatch_solve(within_solver& s, const double* Y_dev, uint64_t k, double to
         double* X = X_dev ? X_dev + c0 * s.n_dofs : nullptr;
         double* D = D_dev ? D_dev + c0 * s.n_obs : nullptr;
         within_solve_stats* S = stats ? stats + c0 : nullptr;
+        if (s.precision == WITHIN_PRECISION_MIXED) {
+            switch (K) {
+                case 1: run_mixed<1>(s, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+                case 2: run_mixed<2>(s, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+                case 4: run_mixed<4>(s, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+                default: run_mixed<8>(s, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+            }
+            continue;
+        }
         switch (K) {
             case 1: run_lsmr<1>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
             case 2: run_lsmr<2>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
@@ -894,7 +1199,10 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
             P->kind = br.kind;
             P->n = (uint32_t)D.n_dofs;
             try {
-                if (br.kind == 2) P->inv_diag = P->arena.upload(br.inv_diag);
+                if (br.kind == 2) {
+                    P->inv_diag = P->arena.upload(br.inv_diag);
+                    P->host_inv_diag = br.inv_diag;
+                }
                 else upload_schwarz(*P, std::move(br.schwarz));
             } catch (...) {
                 delete P;
@@ -1130,10 +1438,11 @@ within_preconditioner* within_solver_preconditioner(const within_solver* s) {
     return s->precond;
 }
 int within_solver_set_precision(within_solver* s, int32_t precision) {
-    if (precision != WITHIN_PRECISION_FP64) {
-        g_err = "only WITHIN_PRECISION_FP64 is available in this build";
-        return WITHIN_ERR_UNSUPPORTED;
+    if (precision != WITHIN_PRECISION_FP64 && precision != WITHIN_PRECISION_MIXED) {
+        g_err = "unknown precision " + std::to_string(precision);
+        return WITHIN_ERR_INVALID_INPUT;
     }
+    std::lock_guard<std::mutex> g(s->mu);
     s->precision = precision;
     return WITHIN_OK;
 }
