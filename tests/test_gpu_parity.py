@@ -204,15 +204,16 @@ def test_input_errors(wb):
         s.solve(y.astype(np.float32))
 
 
-@pytest.mark.parametrize("path", ["0", "1"])
+@pytest.mark.parametrize("path", ["0", "1", "2"])
 @pytest.mark.parametrize("seed", [0, 1])
 def test_adjoint_sweep_classes_match_oracle(wb, oracle, seed, path, monkeypatch):
-    """Both adjoint paths (WITHIN_SWEEP=1: the fused row sweep, =0: gather plus
-    segmented reduction) against the restatement's scatter: a worker-sorted
-    term whose levels span many 1024-row tiles, a firm term with runs along
-    the worker order (and a slope), a 12-level term summed in per-thread
-    histograms, weights, and an observation count that is not a multiple of
-    the tile; single and 3-column solves go through the same path."""
+    """Every operator path (WITHIN_SWEEP=0: gather plus segmented reduction,
+    =1: tile sweep, =2: warp-range row sweep) against the restatement's
+    scatter: a worker-sorted term whose levels span many tiles and warp
+    ranges, a firm term with runs along the worker order (and a slope), a
+    12-level histogram term, weights, and an observation count that is not a
+    multiple of any tile or chunk; single and 3-column solves go through the
+    same path."""
     import torch
     monkeypatch.setenv("WITHIN_SWEEP", path)
     rng = np.random.default_rng(100 + seed)
@@ -248,3 +249,44 @@ def test_adjoint_sweep_classes_match_oracle(wb, oracle, seed, path, monkeypatch)
     for k in range(3):
         refk = o.solve(np.ascontiguousarray(Y[:, k]), tol=1e-10, maxiter=3000)
         assert rel_inf(b.demeaned[:, k], refk.demeaned, Y[:, k]) < DEMEAN_TOL
+
+
+@pytest.fixture(scope="module")
+def multi_k_case(oracle):
+    """A worker-sorted panel with a firm slope and a year term, weights, and 5
+    right-hand sides with their restatement solutions."""
+    rng = np.random.default_rng(77)
+    n_w = 4000
+    counts = rng.integers(1, 400, n_w)
+    worker = np.repeat(np.arange(n_w), counts).astype(np.uint32)
+    n = worker.size
+    firm = np.empty(n, np.uint32)
+    cur = 0
+    for i in range(n):
+        if i == 0 or worker[i] != worker[i - 1] or rng.random() < 0.05:
+            cur = rng.integers(0, 3000)
+        firm[i] = cur
+    year = rng.integers(0, 30, n).astype(np.uint32)
+    z = rng.standard_normal(n)
+    w = rng.lognormal(0, 0.7, n)
+    Y = np.asfortranarray(rng.standard_normal((n, 5)))
+    o = oracle.OracleSolver([oracle.Effect(worker, True), oracle.Effect(firm, True, (z,)),
+                             oracle.Effect(year, True)], weights=w, cfg=oracle.precond_cfg("diagonal"))
+    refs = [o.solve(np.ascontiguousarray(Y[:, c]), tol=1e-11, maxiter=20000).demeaned for c in range(5)]
+    return worker, firm, year, z, w, Y, refs
+
+
+@pytest.mark.parametrize("path", ["0", "1", "2"])
+def test_every_column_bucket_on_every_path(wb, multi_k_case, path, monkeypatch):
+    """Solves of 1, 2, 3 and 5 columns (the K = 1, 2, 4 and 8 kernels) on each
+    operator path against the restatement, diagonal preconditioner."""
+    monkeypatch.setenv("WITHIN_SWEEP", path)
+    worker, firm, year, z, w, Y, refs = multi_k_case
+    s = wb.Solver([wb.Effect(worker, True), wb.Effect(firm, True, [z]), wb.Effect(year, True)], weights=w,
+                  preconditioner=wb.PreconditionerConfig.Diagonal)
+    opts = wb.LsmrOptions(tol=1e-10, maxiter=20000)
+    for k in (1, 2, 3, 5):
+        b = s.solve_batch(np.asfortranarray(Y[:, :k]), opts)
+        for c in range(k):
+            assert b.converged[c]
+            assert rel_inf(b.demeaned[:, c], refs[c], Y[:, c]) < DEMEAN_TOL, (k, c)

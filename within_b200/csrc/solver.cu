@@ -31,6 +31,7 @@
 #include "host.hpp"
 #include "kernels.cuh"
 #include "refine.cuh"
+#include "rowsweep.cuh"
 #include "sweep.cuh"
 
 using namespace wgpu;
@@ -483,9 +484,24 @@ struct within_solver {
         uint32_t n_rest = 0;
         double* atu = nullptr;        // n_dofs * K raw A^T u
     } sweep[4];
-    // per column bucket: run the fused row sweep (true) or the separate
-    // gather + full segmented-reduction scatter (false)
-    bool use_sweep[4] = {false, false, false, false};
+    // warp-range row sweep (rowsweep.cuh), per column bucket K
+    struct RowSweepK {
+        bool ready = false;
+        RwParams rp{};
+        size_t smem = 0;
+        std::vector<ScatterProb> rest_host;   // run combines + full-resolution rest terms
+        std::vector<std::vector<uint32_t>> rest_ptrs;
+        DevPlan rest;
+        ScatterProb* rest_probs = nullptr;
+        ScatterProb* rest_probs_f = nullptr;
+        uint32_t n_rest = 0;
+        bool rest_needs_rows = false;        // a full-resolution rest term reads the row vector
+        double* atu = nullptr;               // n_dofs * K raw A^T u (LSMR)
+    } rsw[4];
+    // per column bucket, the LSMR step's operator path:
+    // 0 gather + full segmented-reduction scatter, 1 tile sweep (sweep.cuh),
+    // 2 warp-range row sweep (rowsweep.cuh)
+    int path[4] = {0, 0, 0, 0};
 
     ~within_solver() {
         for (auto& w : work) {
@@ -655,6 +671,176 @@ void sweep_adjoint_rest(within_solver& s, within_solver::SweepK& sk, const doubl
     launch_sr<ScatterF<K, 0>, K>(f, sk.rest, 0, sk.rest.n_tiles, skip, st);
 }
 
+// Classifies the terms for the warp-range row sweep and builds its tables
+// (rowsweep.cuh): range bases of the run ordinals, the crossing-run fix-ups,
+// the level-sorted run combines and the remaining full-resolution terms.
+template <int K>
+within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
+    auto& rk = s.rsw[kidx(K)];
+    if (rk.ready) return rk;
+    const HostDesign& D = s.design;
+    const uint64_t n = D.n_obs;
+    Arena& A = s.arena;
+    RwParams& rp = rk.rp;
+    const uint64_t G = (uint64_t)rw_grid<K>() * RW_WARPS;
+    const uint64_t CH = rw_chunk<K>();
+    uint64_t rpr = (n + G - 1) / G;
+    rpr = std::max<uint64_t>(CH, (rpr + CH - 1) / CH * CH);
+    rp.rows_per_range = (uint32_t)rpr;
+    std::vector<RwFix> fixes;
+    size_t first_prob = 0;
+    for (int t = 0; t < (int)D.terms.size(); ++t) {
+        const Term& T = D.terms[t];
+        const auto& codes = D.codes[t];
+        const int ncol = (int)T.cols.size();
+        const size_t probs_before = first_prob;
+        first_prob += (size_t)ncol;
+        if (rp.n_hist < RW_MAX_HIST && (uint64_t)rp.n_buckets + (uint64_t)T.n_levels * ncol <= RW_MAX_BUCKETS) {
+            rp.hist[rp.n_hist++] = RwHist{t, rp.n_buckets};
+            rp.n_buckets += (int)(T.n_levels * ncol);
+            continue;
+        }
+        // run heads per range
+        std::vector<uint32_t> cnt(G, 0);
+        uint64_t runs = 0;
+        for (uint64_t i = 0; i < n; ++i)
+            if (i == 0 || codes[i] != codes[i - 1]) {
+                ++cnt[i / rpr];
+                ++runs;
+            }
+        const bool sorted_runs = T.sorted != 0;
+        if (rp.n_run < RW_MAX_RUN && ncol <= rw_max_cols<K>() && (sorted_runs || runs * 3 <= n)) {
+            const int j = rp.n_run++;
+            RwRun& rr = rp.run[j];
+            rr.term = t;
+            rr.direct = sorted_runs ? 1 : 0;
+            std::vector<uint32_t> base(G, 0);
+            for (uint64_t g = 1; g < G; ++g) base[g] = base[g - 1] + cnt[g - 1];
+            for (uint64_t g = 0; g < G; ++g) {
+                const uint64_t r0 = g * rpr, r1 = std::min<uint64_t>(r0 + rpr, n);
+                if (r0 >= n) break;
+                if (cnt[g] == 0 || r1 >= n || codes[r1] != codes[r1 - 1]) continue;
+                uint64_t h = g + 1;
+                while (true) {
+                    const uint64_t h0 = h * rpr, h1 = std::min<uint64_t>(h0 + rpr, n);
+                    if (cnt[h] > 0 || h1 >= n || codes[h1] != codes[h1 - 1]) break;
+                    (void)h0;
+                    ++h;
+                }
+                RwFix f;
+                f.g0 = (uint32_t)g;
+                f.g1 = (uint32_t)h;
+                f.id = rr.direct ? codes[r1 - 1] : base[g] + cnt[g] - 1;
+                f.run = (uint32_t)j;
+                fixes.push_back(f);
+            }
+            rr.head = A.alloc<double>(G * ncol * K);
+            rr.tail = A.alloc<double>(G * ncol * K);
+            rr.range_base = nullptr;
+            rr.run_sum = nullptr;
+            if (!rr.direct) {
+                rr.range_base = A.upload(base);
+                rr.run_sum = A.alloc<double>(runs * ncol * K);
+                // combine: run sums grouped by level (stable in run order)
+                std::vector<uint32_t> run_level;
+                run_level.reserve(runs);
+                for (uint64_t i = 0; i < n; ++i)
+                    if (i == 0 || codes[i] != codes[i - 1]) run_level.push_back(codes[i]);
+                std::vector<uint32_t> perm(runs);
+                stable_argsort_u32(run_level.data(), runs, T.n_levels, perm.data());
+                std::vector<uint32_t> lp((size_t)T.n_levels + 1, 0);
+                for (uint32_t l : run_level) ++lp[(size_t)l + 1];
+                for (uint32_t l = 0; l < T.n_levels; ++l) lp[l + 1] += lp[l];
+                uint32_t* dlp = A.upload(lp);
+                uint32_t* dperm = A.upload(perm);
+                for (int c = 0; c < ncol; ++c) {
+                    ScatterProb pr{};
+                    pr.seg_ptr = dlp;
+                    pr.order = dperm;
+                    pr.out_off = (uint32_t)(T.offset + c * T.n_levels);
+                    pr.ncol = (uint32_t)ncol;
+                    pr.run_sum = rr.run_sum;
+                    pr.col = (uint32_t)c;
+                    rk.rest_host.push_back(pr);
+                    rk.rest_ptrs.push_back(lp);
+                }
+            }
+            continue;
+        }
+        for (int c = 0; c < ncol; ++c) {
+            rk.rest_host.push_back(s.scatter_host[probs_before + c]);
+            rk.rest_ptrs.push_back(s.level_ptr_host[t]);
+            rk.rest_needs_rows = true;
+        }
+    }
+    rp.fix = A.upload(fixes);
+    rp.n_fix = (uint32_t)fixes.size();
+    rp.part = A.alloc<double>((size_t)rw_grid<K>() * (K + (size_t)rp.n_buckets * K));
+    rp.counter = A.alloc<unsigned>(1);
+    rk.smem = rp.n_hist > 0 ? (size_t)RW_WARPS * ((size_t)rp.n_buckets * K + 32 * K) * sizeof(double) : 0;
+    rk.atu = A.alloc<double>(s.n_dofs * K);
+    rk.n_rest = (uint32_t)rk.rest_host.size();
+    if (rk.n_rest) {
+        const int Ttile = sr_tile<K>();
+        HostPlan hp;
+        for (size_t i = 0; i < rk.rest_host.size(); ++i)
+            hp.add((uint32_t)i, rk.rest_ptrs[i].data(), (uint32_t)rk.rest_ptrs[i].size() - 1, Ttile);
+        rk.rest = make_plan(A, hp, K);
+        rk.rest_probs = A.upload(rk.rest_host);
+    }
+    // dynamic shared memory above the default needs the opt-in (set outside any capture)
+    if (rk.smem > 40 * 1024) {
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
+    }
+    rk.ready = true;
+    return rk;
+}
+
+// FP32 loading columns in the rest problems (mixed-precision inner solve)
+template <int K>
+void ensure_rowsweep_f(within_solver& s) {
+    auto& rk = ensure_rowsweep<K>(s);
+    if (rk.rest_probs_f || !rk.n_rest) return;
+    std::vector<ScatterProb> pf = rk.rest_host;
+    for (auto& pr : pf) {
+        pr.load_f = nullptr;
+        if (pr.load)
+            for (size_t k = 0; k < s.design.loads.size(); ++k)
+                if (pr.load == s.op.loads[k]) pr.load_f = s.op_f.loads[k];
+    }
+    rk.rest_probs_f = s.arena.upload(pf);
+}
+
+template <int K, int MODE, class T>
+void launch_rowsweep(within_solver& s, within_solver::RowSweepK& rk, const OpParamsT<T>& op, void* atu, const T* v,
+                     T* u, ColState* cur, Ctl* ctl, const int* skip, int store, cudaStream_t st) {
+    RwParams rp = rk.rp;
+    rp.atu = atu;
+    k_rowsweep<K, MODE, T><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip, store);
+    ++g_launches;
+}
+
+// the run combines and full-resolution rest terms of A^T u, raw sums into out
+template <int K, class T>
+void rowsweep_rest(within_solver& s, within_solver::RowSweepK& rk, const T* u, T* out, const int* skip,
+                   cudaStream_t st) {
+    if (!rk.n_rest) return;
+    if constexpr (sizeof(T) == 8) {
+        ScatterF<K, 0> f{rk.rest_probs, u, s.op.sqrt_w, out, nullptr};
+        launch_sr<ScatterF<K, 0>, K>(f, rk.rest, 0, rk.rest.n_tiles, skip, st);
+    } else {
+        ScatterF<K, 0, float> f{rk.rest_probs_f, u, s.op_f.sqrt_w, out, nullptr};
+        launch_sr<ScatterF<K, 0, float>, K>(f, rk.rest, 0, rk.rest.n_tiles, skip, st);
+    }
+}
+
+int env_path(int dflt) {
+    if (const char* e = getenv("WITHIN_SWEEP")) return std::max(0, std::min(2, atoi(e)));
+    return dflt;
+}
+
 within_solver::Work& ensure_work(within_solver& s, int K) {
     auto& w = s.work[kidx(K)];
     if (w.ready) return w;
@@ -677,12 +863,16 @@ within_solver::Work& ensure_work(within_solver& s, int K) {
     if (s.precond && s.precond->kind == 1) schwarz_user_plans(s.schwarz, *s.precond, K);
     ensure_scatter(s, K);
     // Path choice per column count, fixed per process so results stay bitwise
-    // reproducible: measured on the 10M-row panel the sweep pays off from 4
-    // columns up.  WITHIN_SWEEP=0/1 forces either path.
-    bool sweep = K >= 4;
-    if (const char* e = getenv("WITHIN_SWEEP")) sweep = atoi(e) != 0;
-    s.use_sweep[kidx(K)] = sweep;
-    if (sweep) ensure_sweep(s, K);
+    // reproducible.  WITHIN_SWEEP=0/1/2 forces a path.
+    const int path = env_path(2);
+    s.path[kidx(K)] = path;
+    if (path == 1) ensure_sweep(s, K);
+    if (path == 2) {
+        if (K == 1) ensure_rowsweep<1>(s);
+        else if (K == 2) ensure_rowsweep<2>(s);
+        else if (K == 4) ensure_rowsweep<4>(s);
+        else ensure_rowsweep<8>(s);
+    }
     w.ready = true;
     return w;
 }
@@ -723,7 +913,13 @@ void iteration(within_solver& s, within_solver::Work& w, int par, cudaStream_t s
     ColState* nxt = w.st + (size_t)(1 - par) * 8;
     const uint32_t n = (uint32_t)s.n_obs, nd = (uint32_t)s.n_dofs;
     const int* skip = &w.ctl->all_done;
-    if (s.use_sweep[kidx(K)]) {
+    if (s.path[kidx(K)] == 2) {
+        auto& rk = s.rsw[kidx(K)];
+        launch_rowsweep<K, 1, double>(s, rk, s.op, rk.atu, w.v, w.u, cur, w.ctl, nullptr, 0, st);
+        rowsweep_rest<K, double>(s, rk, w.u, rk.atu, skip, st);
+        k_ptilde<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, rk.atu, w.p, cur, w.ctl);
+        ++g_launches;
+    } else if (s.path[kidx(K)] == 1) {
         auto& sk = s.sweep[kidx(K)];
         launch_sweep<K, true>(s, sk, w.v, w.u, cur, w.ctl, st);
         sweep_adjoint_rest<K>(s, sk, w.u, sk.atu, skip, st);
@@ -946,6 +1142,12 @@ within_solver::MixedWork& ensure_mixed(within_solver& s, int K) {
     m.st = A.alloc<CgCol>(8);
     m.ctl = A.alloc<Ctl>(1);
     if (s.precond && s.precond->kind == 1) schwarz_user_work_f(s.schwarz, *s.precond, K);
+    if (s.path[kidx(K)] == 2) {
+        if (K == 1) ensure_rowsweep_f<1>(s);
+        else if (K == 2) ensure_rowsweep_f<2>(s);
+        else if (K == 4) ensure_rowsweep_f<4>(s);
+        else ensure_rowsweep_f<8>(s);
+    }
     m.ready = true;
     return m;
 }
@@ -955,11 +1157,19 @@ template <int K>
 void cg_iteration(within_solver& s, within_solver::Work& w, within_solver::MixedWork& m, cudaStream_t st) {
     const uint32_t nd = (uint32_t)s.n_dofs;
     const int* skip = &m.ctl->all_done;
-    k_apply<K, float><<<grid_for(s.n_obs, 256 * 4, 148 * 8), 256, 0, st>>>(s.op_f, m.p, m.t, skip);
-    scatter<K, 0, float>(s, m.t, m.q, nullptr, skip, st);
+    if (s.path[kidx(K)] == 2) {
+        auto& rk = s.rsw[kidx(K)];
+        launch_rowsweep<K, 2, float>(s, rk, s.op_f, m.q, m.p, m.t, nullptr, m.ctl, skip, rk.rest_needs_rows ? 1 : 0,
+                                     st);
+        rowsweep_rest<K, float>(s, rk, m.t, m.q, skip, st);
+    } else {
+        k_apply<K, float><<<grid_for(s.n_obs, 256 * 4, 148 * 8), 256, 0, st>>>(s.op_f, m.p, m.t, skip);
+        ++g_launches;
+        scatter<K, 0, float>(s, m.t, m.q, nullptr, skip, st);
+    }
     k_cg_alpha<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.p, m.q, m.st, m.ctl, w.partials, w.counter);
     k_cg_update<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.p, m.q, m.d, m.res, m.st, m.ctl);
-    g_launches += 3;
+    g_launches += 2;
     precond_apply<K, float>(s, m.ctl, m.res, m.z, skip, st);
     k_cg_beta<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.st, m.ctl, w.partials, w.counter);
     k_cg_dir<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.z, m.p, m.st, m.ctl);
@@ -1525,9 +1735,18 @@ int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, 
         set_device(s->device);
         cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
         ensure_scatter(*s, 1);
-        bool use = false;
-        if (const char* e = getenv("WITHIN_SWEEP")) use = atoi(e) != 0;
-        if (!use) {
+        const int path = env_path(2);
+        if (path == 2) {
+            auto& rk = ensure_rowsweep<1>(*s);
+            CK(cudaMemsetAsync(y_dev, 0, s->n_dofs * sizeof(double), st));   // levels no row reaches stay 0
+            launch_rowsweep<1, 0, double>(*s, rk, s->op, y_dev, nullptr, const_cast<double*>(u_dev), nullptr,
+                                          nullptr, nullptr, 0, st);
+            rowsweep_rest<1, double>(*s, rk, u_dev, y_dev, nullptr, st);
+            CK(cudaGetLastError());
+            if (!stream) CK(cudaStreamSynchronize(st));
+            return;
+        }
+        if (path == 0) {
             scatter<1, 0>(*s, u_dev, y_dev, nullptr, nullptr, st);
             CK(cudaGetLastError());
             if (!stream) CK(cudaStreamSynchronize(st));
