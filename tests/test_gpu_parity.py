@@ -204,11 +204,11 @@ def test_input_errors(wb):
         s.solve(y.astype(np.float32))
 
 
-@pytest.mark.parametrize("path", ["0", "1", "2"])
+@pytest.mark.parametrize("path", ["0", "2"])
 @pytest.mark.parametrize("seed", [0, 1])
 def test_adjoint_sweep_classes_match_oracle(wb, oracle, seed, path, monkeypatch):
-    """Every operator path (WITHIN_SWEEP=0: gather plus segmented reduction,
-    =1: tile sweep, =2: warp-range row sweep) against the restatement's
+    """Both operator paths (WITHIN_SWEEP=0: gather plus segmented reduction,
+    =2: warp-range row sweep) against the restatement's
     scatter: a worker-sorted term whose levels span many tiles and warp
     ranges, a firm term with runs along the worker order (and a slope), a
     12-level histogram term, weights, and an observation count that is not a
@@ -276,7 +276,7 @@ def multi_k_case(oracle):
     return worker, firm, year, z, w, Y, refs
 
 
-@pytest.mark.parametrize("path", ["0", "1", "2"])
+@pytest.mark.parametrize("path", ["0", "2"])
 def test_every_column_bucket_on_every_path(wb, multi_k_case, path, monkeypatch):
     """Solves of 1, 2, 3 and 5 columns (the K = 1, 2, 4 and 8 kernels) on each
     operator path against the restatement, diagonal preconditioner."""

@@ -78,6 +78,16 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Column i of a [nblk][stride] table of block partials, summed in one fixed
+// order by a whole warp: lane l adds rows l, l+32, ..., then a fixed shuffle
+// tree; every lane returns the total.
+__device__ __forceinline__ double warp_col_sum(const double* part, unsigned nblk, size_t stride, size_t i) {
+    const int lane = threadIdx.x & 31;
+    double a = 0.0;
+    for (unsigned blk = lane; blk < nblk; blk += 32) a += __ldcg(&part[(size_t)blk * stride + i]);
+    return warp_sum(a);
+}
+
 // Sum over the block; the result is valid in thread 0.
 __device__ __forceinline__ double block_sum(double v, double* sm /* >= 32 */) {
     v = warp_sum(v);
@@ -274,7 +284,7 @@ struct ScatterF {
     __device__ const uint32_t* seg_ptr(const Prob& pr) const { return pr.seg_ptr; }
     __device__ void value(const Prob& pr, uint32_t pos, double (&v)[K]) const {
         const uint32_t i = pr.order ? __ldg(pr.order + pos) : pos;
-        if (pr.run_sum) {   // combine of run sums formed by the row sweep (sweep.cuh)
+        if (pr.run_sum) {   // combine of run sums formed by the row sweep (rowsweep.cuh)
             const double* rs = pr.run_sum + ((size_t)i * pr.ncol + pr.col) * K;
 #pragma unroll
             for (int k = 0; k < K; ++k) v[k] = __ldg(rs + k);
@@ -857,14 +867,16 @@ k_load_rhs(uint32_t n, uint32_t k_used, const double* __restrict__ Y, const uint
         is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (is_last && threadIdx.x == 0) {
+    if (is_last) {
         __threadfence();
-        for (int k = 0; k < K; ++k) {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (int k = wid; k < K; k += (int)(blockDim.x >> 5)) {
             double m = 0;
-            for (unsigned blk = 0; blk < gridDim.x; ++blk) m = fmax(m, __ldcg(&partials[(size_t)blk * K + k]));
-            out_max[k] = m;
+            for (unsigned blk = lane; blk < gridDim.x; blk += 32) m = fmax(m, __ldcg(&partials[(size_t)blk * K + k]));
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) out_max[k] = m;
         }
-        *counter = 0;
+        if (threadIdx.x == 0) *counter = 0;
     }
 }
 

@@ -21,10 +21,12 @@
 //               leaves a tail partial (range where it starts) and head
 //               partials (ranges it continues into); the last block adds them
 //               in range order.
-//   hist terms  few coefficients (levels x columns <= 64): per-warp bins in
-//               shared memory, each 32-row step grouped by level with
-//               __match_any_sync and summed by the group's first lane in lane
-//               order; bins are then reduced over warps and blocks in order.
+//   hist terms  few coefficients (levels x columns <= 64): bins in shared
+//               memory -- per lane when they fit (each lane adds its rows in
+//               order), else per warp with each 32-row step grouped by level
+//               (__match_any_sync) and summed by the group's first lane in lane
+//               order; bins are then reduced over lanes, warps and blocks in
+//               order.
 //   rest terms  left to the segmented reduction over the level-sorted
 //               observation permutation (segreduce.cuh).
 // Modes: 0 -- A^T u of a given u (Operator::apply_adjoint);  1 -- LSMR step
@@ -46,11 +48,11 @@ constexpr int RW_MAX_BUCKETS = 64;   // levels x columns over all hist terms
 constexpr int RW_RUN_VALS = 8;       // columns x K of a run term (register carry)
 
 template <int K>
-__host__ __device__ constexpr int rw_rows() { return K >= 4 ? 2 : 4; }
+__host__ __device__ constexpr int rw_rows() { return K >= 4 ? 2 : K == 2 ? 4 : 8; }
 template <int K>
 __host__ __device__ constexpr int rw_chunk() { return 32 * rw_rows<K>(); }
 template <int K>
-__host__ __device__ constexpr int rw_min_blocks() { return K >= 8 ? 2 : 3; }
+__host__ __device__ constexpr int rw_min_blocks() { return K >= 8 || K == 1 ? 2 : 3; }
 // fixed grid: 148 SMs x resident blocks per SM
 template <int K>
 __host__ __device__ constexpr int rw_grid() { return 148 * rw_min_blocks<K>(); }
@@ -81,6 +83,7 @@ struct RwHist {
 struct RwParams {
     uint32_t rows_per_range;     // multiple of the chunk
     int n_run, n_hist, n_buckets;
+    int hist_private;            // bins per lane (bins x K x 32 doubles per warp), else match-grouped
     RwRun run[RW_MAX_RUN];
     RwHist hist[RW_MAX_HIST];
     const RwFix* fix;
@@ -100,7 +103,18 @@ template <int R>
 __device__ __forceinline__ void rw_load_codes(const uint32_t* __restrict__ c, uint32_t row0, int nr,
                                               uint32_t (&cd)[R]) {
     if (nr == R) {
-        if constexpr (R == 4) {
+        if constexpr (R == 8) {
+            const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(c + row0));
+            const uint4 q1 = __ldg(reinterpret_cast<const uint4*>(c + row0 + 4));
+            cd[0] = q0.x;
+            cd[1] = q0.y;
+            cd[2] = q0.z;
+            cd[3] = q0.w;
+            cd[4] = q1.x;
+            cd[5] = q1.y;
+            cd[6] = q1.z;
+            cd[7] = q1.w;
+        } else if constexpr (R == 4) {
             const uint4 q = __ldg(reinterpret_cast<const uint4*>(c + row0));
             cd[0] = q.x;
             cd[1] = q.y;
@@ -142,9 +156,10 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nb = rw.n_buckets * K;
-    double* bins = rw_sm + (size_t)wid * nb;
-    double* stage = rw_sm + (size_t)RW_WARPS * nb + (size_t)wid * 32 * K;
-    for (int i = lane; i < nb; i += 32) bins[i] = 0.0;
+    const int bw = rw.hist_private ? nb * 32 : nb;   // bin doubles per warp
+    double* bins = rw_sm + (size_t)wid * bw;
+    double* stage = rw_sm + (size_t)RW_WARPS * bw + (size_t)wid * 32 * K;
+    for (int i = lane; i < bw; i += 32) bins[i] = 0.0;
     __syncwarp();
     TO* atu = reinterpret_cast<TO*>(rw.atu);
 
@@ -242,12 +257,25 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             }
         }
 
-        // ---- hist terms: per-warp bins, grouped by level per 32-row step
+        // ---- hist terms: per-lane bins, or per-warp bins grouped by level per 32-row step
         for (int hh = 0; hh < rw.n_hist; ++hh) {
             const int t = rw.hist[hh].term;
             const int ncol = p.ncol[t];
             uint32_t hc[R];
             rw_load_codes<R>(p.codes[t], row0, nr, hc);
+            if (rw.hist_private) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (r >= nr) break;
+                    for (int c = 0; c < ncol; ++c) {
+                        const double ld = rw_load(p, t, c, row0 + r);
+                        const int bk = rw.hist[hh].bucket0 + (int)hc[r] * ncol + c;
+#pragma unroll
+                        for (int k = 0; k < K; ++k) bins[(bk * K + k) * 32 + lane] += ld * b[r][k];
+                    }
+                }
+                continue;
+            }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const uint32_t key = r < nr ? hc[r] : 0xffffffffu;
@@ -442,6 +470,14 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
 
     // ---- block partials: ||u||^2 (mode 1) and the bins, in warp order
     const int stride = K + nb;
+    if (rw.hist_private) {   // lanes of each warp in order, into the lane-0 slot
+        __syncwarp();
+        for (int i = lane; i < nb; i += 32) {
+            double s = 0.0;
+            for (int l = 0; l < 32; ++l) s += bins[i * 32 + l];
+            bins[i * 32] = s;
+        }
+    }
     if (MODE == 1) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -457,8 +493,9 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
         mypart[threadIdx.x] = s;
     }
     for (int i = threadIdx.x; i < nb; i += RW_THREADS) {
+        const size_t slot = rw.hist_private ? (size_t)i * 32 : (size_t)i;
         double s = 0.0;
-        for (int w = 0; w < RW_WARPS; ++w) s += rw_sm[(size_t)w * nb + i];
+        for (int w = 0; w < RW_WARPS; ++w) s += rw_sm[(size_t)w * bw + slot];
         mypart[K + i] = s;
     }
     __syncthreads();
@@ -470,10 +507,10 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     if (!is_last) return;
     __threadfence();
     // ---- last block: grand totals in block order, bins -> A^T u, crossing runs
-    for (int i = threadIdx.x; i < stride; i += RW_THREADS) {
+    for (int i = wid; i < stride; i += RW_WARPS) {
         if (i < K && MODE != 1) continue;
-        double a = 0.0;
-        for (unsigned blk = 0; blk < gridDim.x; ++blk) a += __ldcg(&rw.part[(size_t)blk * stride + i]);
+        const double a = warp_col_sum(rw.part, gridDim.x, stride, i);
+        if (lane != 0) continue;
         if (i < K) {
             if (act[i]) cur[i].beta = sqrt(a);
             continue;
@@ -509,6 +546,30 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             }
     }
     if (threadIdx.x == 0) *rw.counter = 0;
+}
+
+// p~ <- A^T u / beta - (beta / alpha) p~ over all DOFs (bidiag.rs:474-485),
+// skipping finished columns; beta == 0 (lucky breakdown) zeroes p~.
+template <int K>
+__global__ void k_ptilde(uint32_t nd, const double* __restrict__ atu, double* __restrict__ pt,
+                         const ColState* cur, const Ctl* ctl) {
+    if (ctl->all_done) return;
+    double inv[K], coef[K];
+    bool act[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        act[k] = !cur[k].done;
+        const double beta = cur[k].beta;
+        inv[k] = beta == 0.0 ? 0.0 : 1.0 / beta;
+        coef[k] = beta == 0.0 ? 0.0 : beta / cur[k].alpha;
+    }
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nd; j += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (act[k]) {
+                const size_t o = (size_t)j * K + k;
+                pt[o] = atu[o] * inv[k] - coef[k] * pt[o];
+            }
 }
 
 }  // namespace wgpu

@@ -32,7 +32,6 @@
 #include "kernels.cuh"
 #include "refine.cuh"
 #include "rowsweep.cuh"
-#include "sweep.cuh"
 
 using namespace wgpu;
 
@@ -474,16 +473,6 @@ struct within_solver {
     double* pin = nullptr;
     size_t pin_n = 0;
     SchwarzUser schwarz;   // this solver's plans/work for the preconditioner
-    // fused row sweep (sweep.cuh), per column bucket K
-    struct SweepK {
-        bool ready = false;
-        SweepParams sp{};
-        size_t hist_bytes = 0;
-        DevPlan rest;                 // segmented reduction of the remaining terms / run combines
-        ScatterProb* rest_probs = nullptr;
-        uint32_t n_rest = 0;
-        double* atu = nullptr;        // n_dofs * K raw A^T u
-    } sweep[4];
     // warp-range row sweep (rowsweep.cuh), per column bucket K
     struct RowSweepK {
         bool ready = false;
@@ -499,8 +488,7 @@ struct within_solver {
         double* atu = nullptr;               // n_dofs * K raw A^T u (LSMR)
     } rsw[4];
     // per column bucket, the LSMR step's operator path:
-    // 0 gather + full segmented-reduction scatter, 1 tile sweep (sweep.cuh),
-    // 2 warp-range row sweep (rowsweep.cuh)
+    // 0 gather + full segmented-reduction scatter, 2 warp-range row sweep (rowsweep.cuh)
     int path[4] = {0, 0, 0, 0};
 
     ~within_solver() {
@@ -535,140 +523,6 @@ void ensure_scatter(within_solver& s, int K) {
     }
     s.scatter_plan[ki] = make_plan(s.arena, hp, K);
     s.scatter_ready[ki] = true;
-}
-
-constexpr int SWEEP_GRID = 148 * 4;   // fixed: deterministic block partials
-
-// Classifies the terms for the row sweep and builds its tables (sweep.cuh).
-within_solver::SweepK& ensure_sweep(within_solver& s, int K) {
-    auto& sk = s.sweep[kidx(K)];
-    if (sk.ready) return sk;
-    const HostDesign& D = s.design;
-    const uint64_t n = D.n_obs;
-    const uint32_t n_tiles = (uint32_t)((n + SW_TILE - 1) / SW_TILE);
-    Arena& A = s.arena;
-    SweepParams& sp = sk.sp;
-    sp.n_tiles = n_tiles;
-    int hist_used = 0;
-    std::vector<ScatterProb> rest;
-    std::vector<std::vector<uint32_t>> rest_ptrs;
-    for (int t = 0; t < (int)D.terms.size(); ++t) {
-        const Term& T = D.terms[t];
-        const auto& codes = D.codes[t];
-        const int ncol = (int)T.cols.size();
-        const uint64_t cap = (uint64_t)T.n_levels * ncol * K;
-        if (sp.n_hist < SW_MAX_HIST && hist_used + (int)cap <= SW_HIST_CAP) {
-            sp.hist[sp.n_hist] = SweepHist{t, sp.n_buckets};
-            sp.n_buckets += (int)(T.n_levels * ncol);
-            hist_used += (int)cap;
-            ++sp.n_hist;
-            continue;
-        }
-        std::vector<uint32_t> run_ptr{0};
-        for (uint64_t i = 1; i < n; ++i)
-            if (codes[i] != codes[i - 1]) run_ptr.push_back((uint32_t)i);
-        run_ptr.push_back((uint32_t)n);
-        const uint64_t R = run_ptr.size() - 1;
-        if (sp.n_run < SW_MAX_RUN && R * 3 <= n) {
-            SweepRun& rr = sp.run[sp.n_run++];
-            rr.term = t;
-            rr.direct = T.sorted ? 1 : 0;
-            // runs crossing tile boundaries: per tile, the start tile of the run
-            // continuing into it and the last tile of the run leaving it
-            std::vector<uint32_t> cont_t0(n_tiles, UINT32_MAX), leave_t1(n_tiles, UINT32_MAX),
-                leave_a(n_tiles, 0);
-            for (uint64_t r = 0; r < R; ++r) {
-                const uint32_t a = run_ptr[r], e = run_ptr[r + 1];
-                const uint32_t ta = a / SW_TILE, tb = (e - 1) / SW_TILE;
-                if (tb == ta) continue;
-                leave_t1[ta] = tb;
-                leave_a[ta] = a;
-                for (uint32_t tl = ta + 1; tl <= tb; ++tl) cont_t0[tl] = ta;
-            }
-            rr.cont_t0 = A.upload(cont_t0);
-            rr.leave_t1 = A.upload(leave_t1);
-            rr.leave_a = A.upload(leave_a);
-            rr.cnt = A.alloc<unsigned>(n_tiles);
-            rr.head = A.alloc<double>((size_t)n_tiles * ncol * K);
-            rr.tail = A.alloc<double>((size_t)n_tiles * ncol * K);
-            rr.run_sum = nullptr;
-            if (!rr.direct) {
-                // combine: run sums (indexed by first row) grouped by level, stable
-                rr.run_sum = A.alloc<double>((size_t)n * ncol * K);
-                std::vector<uint32_t> run_level(R);
-                for (uint64_t r = 0; r < R; ++r) run_level[r] = codes[run_ptr[r]];
-                std::vector<uint32_t> perm(R);
-                stable_argsort_u32(run_level.data(), R, T.n_levels, perm.data());
-                for (auto& x : perm) x = run_ptr[x];   // -> first row of the run
-                std::vector<uint32_t> lp((size_t)T.n_levels + 1, 0);
-                for (uint32_t l : run_level) ++lp[(size_t)l + 1];
-                for (uint32_t l = 0; l < T.n_levels; ++l) lp[l + 1] += lp[l];
-                uint32_t* dlp = A.upload(lp);
-                uint32_t* dperm = A.upload(perm);
-                for (int c = 0; c < ncol; ++c) {
-                    ScatterProb pr{};
-                    pr.seg_ptr = dlp;
-                    pr.order = dperm;
-                    pr.load = nullptr;
-                    pr.out_off = (uint32_t)(T.offset + c * T.n_levels);
-                    pr.ncol = (uint32_t)ncol;
-                    pr.run_sum = rr.run_sum;
-                    pr.col = (uint32_t)c;
-                    rest.push_back(pr);
-                    rest_ptrs.push_back(lp);
-                }
-            }
-            continue;
-        }
-        // remaining: the full-resolution scatter problems of this term
-        size_t first = 0;
-        for (int q = 0; q < t; ++q) first += D.terms[q].cols.size();
-        for (int c = 0; c < ncol; ++c) {
-            rest.push_back(s.scatter_host[first + c]);
-            rest_ptrs.push_back(s.level_ptr_host[t]);
-        }
-    }
-    sk.hist_bytes = (size_t)sp.n_buckets * K * SW_THREADS * sizeof(double);
-    sp.hist_part = A.alloc<double>((size_t)SWEEP_GRID * (sp.n_buckets * K + K));
-    sp.hist_counter = A.alloc<unsigned>(1);
-    sk.atu = A.alloc<double>(s.n_dofs * K);
-    sp.atu = sk.atu;
-    sk.n_rest = (uint32_t)rest.size();
-    if (!rest.empty()) {
-        const int Ttile = K == 1 ? sr_tile<1>() : K == 2 ? sr_tile<2>() : K == 4 ? sr_tile<4>() : sr_tile<8>();
-        HostPlan hp;
-        for (size_t i = 0; i < rest.size(); ++i)
-            hp.add((uint32_t)i, rest_ptrs[i].data(), (uint32_t)rest_ptrs[i].size() - 1, Ttile);
-        sk.rest = make_plan(A, hp, K);
-        sk.rest_probs = A.upload(rest);
-    }
-    sk.ready = true;
-    return sk;
-}
-
-template <int K, bool LSMR>
-void launch_sweep(within_solver& s, within_solver::SweepK& sk, const double* v, double* u, ColState* cur,
-                  Ctl* ctl, cudaStream_t st) {
-    const size_t smem = sk.hist_bytes;
-    static thread_local bool configured[2][9] = {};
-    if (!configured[LSMR][K]) {
-        // the histogram lives in shared memory: ask for the largest carveout
-        CK(cudaFuncSetAttribute(k_sweep<K, LSMR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        configured[LSMR][K] = true;
-    }
-    if (smem > 32 * 1024)   // static + dynamic above the default 48 KB needs the opt-in
-        CK(cudaFuncSetAttribute(k_sweep<K, LSMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_sweep<K, LSMR><<<SWEEP_GRID, SW_THREADS, smem, st>>>(s.op, sk.sp, v, u, cur, ctl, nullptr, nullptr);
-    ++g_launches;
-}
-
-// A^T u (raw sums) into out through the sweep + the remaining segmented reduction
-template <int K>
-void sweep_adjoint_rest(within_solver& s, within_solver::SweepK& sk, const double* u, double* out,
-                        const int* skip, cudaStream_t st) {
-    if (sk.n_rest == 0) return;
-    ScatterF<K, 0> f{sk.rest_probs, u, s.op.sqrt_w, out, nullptr};
-    launch_sr<ScatterF<K, 0>, K>(f, sk.rest, 0, sk.rest.n_tiles, skip, st);
 }
 
 // Classifies the terms for the warp-range row sweep and builds its tables
@@ -777,7 +631,11 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
     rp.n_fix = (uint32_t)fixes.size();
     rp.part = A.alloc<double>((size_t)rw_grid<K>() * (K + (size_t)rp.n_buckets * K));
     rp.counter = A.alloc<unsigned>(1);
-    rk.smem = rp.n_hist > 0 ? (size_t)RW_WARPS * ((size_t)rp.n_buckets * K + 32 * K) * sizeof(double) : 0;
+    // per-lane bins when a block's copy stays within 72 KB (3 blocks per SM)
+    rp.hist_private = (size_t)RW_WARPS * rp.n_buckets * K * 32 * sizeof(double) <= 72 * 1024 ? 1 : 0;
+    if (rp.n_hist == 0) rk.smem = 0;
+    else if (rp.hist_private) rk.smem = (size_t)RW_WARPS * rp.n_buckets * K * 32 * sizeof(double);
+    else rk.smem = (size_t)RW_WARPS * ((size_t)rp.n_buckets * K + 32 * K) * sizeof(double);
     rk.atu = A.alloc<double>(s.n_dofs * K);
     rk.n_rest = (uint32_t)rk.rest_host.size();
     if (rk.n_rest) {
@@ -836,8 +694,10 @@ void rowsweep_rest(within_solver& s, within_solver::RowSweepK& rk, const T* u, T
     }
 }
 
+// WITHIN_SWEEP=0 selects the gather + full segmented-reduction path, any
+// other value the row sweep
 int env_path(int dflt) {
-    if (const char* e = getenv("WITHIN_SWEEP")) return std::max(0, std::min(2, atoi(e)));
+    if (const char* e = getenv("WITHIN_SWEEP")) return atoi(e) == 0 ? 0 : 2;
     return dflt;
 }
 
@@ -863,10 +723,9 @@ within_solver::Work& ensure_work(within_solver& s, int K) {
     if (s.precond && s.precond->kind == 1) schwarz_user_plans(s.schwarz, *s.precond, K);
     ensure_scatter(s, K);
     // Path choice per column count, fixed per process so results stay bitwise
-    // reproducible.  WITHIN_SWEEP=0/1/2 forces a path.
+    // reproducible.  WITHIN_SWEEP=0 forces the gather + scatter path.
     const int path = env_path(2);
     s.path[kidx(K)] = path;
-    if (path == 1) ensure_sweep(s, K);
     if (path == 2) {
         if (K == 1) ensure_rowsweep<1>(s);
         else if (K == 2) ensure_rowsweep<2>(s);
@@ -918,12 +777,6 @@ void iteration(within_solver& s, within_solver::Work& w, int par, cudaStream_t s
         launch_rowsweep<K, 1, double>(s, rk, s.op, rk.atu, w.v, w.u, cur, w.ctl, nullptr, 0, st);
         rowsweep_rest<K, double>(s, rk, w.u, rk.atu, skip, st);
         k_ptilde<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, rk.atu, w.p, cur, w.ctl);
-        ++g_launches;
-    } else if (s.path[kidx(K)] == 1) {
-        auto& sk = s.sweep[kidx(K)];
-        launch_sweep<K, true>(s, sk, w.v, w.u, cur, w.ctl, st);
-        sweep_adjoint_rest<K>(s, sk, w.u, sk.atu, skip, st);
-        k_ptilde<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, sk.atu, w.p, cur, w.ctl);
         ++g_launches;
     } else {
         k_gather_update<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, w.v, w.u, cur, w.ctl, w.partials, w.counter);
@@ -1746,20 +1599,7 @@ int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, 
             if (!stream) CK(cudaStreamSynchronize(st));
             return;
         }
-        if (path == 0) {
-            scatter<1, 0>(*s, u_dev, y_dev, nullptr, nullptr, st);
-            CK(cudaGetLastError());
-            if (!stream) CK(cudaStreamSynchronize(st));
-            return;
-        }
-        auto& sk = ensure_sweep(*s, 1);
-        SweepParams sp = sk.sp;
-        sp.atu = y_dev;   // the sweep's direct/hist sums land in the output
-        within_solver::SweepK tmp = sk;
-        tmp.sp = sp;
-        CK(cudaMemsetAsync(y_dev, 0, s->n_dofs * sizeof(double), st));   // levels no term writes stay 0
-        launch_sweep<1, false>(*s, tmp, nullptr, const_cast<double*>(u_dev), nullptr, nullptr, st);
-        sweep_adjoint_rest<1>(*s, sk, u_dev, y_dev, nullptr, st);
+        scatter<1, 0>(*s, u_dev, y_dev, nullptr, nullptr, st);
         CK(cudaGetLastError());
         if (!stream) CK(cudaStreamSynchronize(st));
     });
