@@ -196,6 +196,25 @@ int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, 
 int within_solver_operator_apply_adjoint_noalloc(within_solver* s, const double* u_dev,
                                                  double* y_dev, void* stream);
 
+/* ---- Many independent designs (no counterpart in the reference API, which
+ * solves one design per Solver; this is the multi-design batch of many small
+ * and large problems, e.g. one design per group or per bootstrap draw).
+ * within_solvers_new builds n Solvers (Solver::new, solver.rs:361-411) with
+ * their set-up spread over `threads` host threads; weights may be NULL or
+ * hold NULL entries.  On failure no solver is left allocated.
+ * within_solvers_solve_batch runs Solver::solve_batch (solver.rs:530-577) of
+ * every solver: Y[i] is n_obs_i x k[i] column-major on the host, X[i] / D[i]
+ * receive x and the demeaned columns (X or D NULL, or entries NULL, to skip),
+ * stats[i] k[i] entries.  `threads` host threads each drive one design at a
+ * time on that design's own stream, so the designs' device work overlaps;
+ * every design keeps its own per-column convergence. ---- */
+int within_solvers_new(uint64_t n, const within_design* const* designs, const double* const* weights,
+                       const within_precond_config* cfg, int32_t device, uint32_t threads,
+                       within_solver** out);
+int within_solvers_solve_batch(uint64_t n, within_solver* const* solvers, const double* const* Y,
+                               const uint64_t* k, const within_lsmr_options* opts, double* const* X,
+                               double* const* D, within_solve_stats* const* stats, uint32_t threads);
+
 /* ---- Preconditioner handle (operator/schwarz.rs:115-183) ---- */
 void within_preconditioner_free(within_preconditioner* p);
 uint64_t within_preconditioner_n(const within_preconditioner* p);

@@ -41,6 +41,8 @@ __all__ = [
     "solve",
     "solve_batch",
     "demean",
+    "SolverSet",
+    "solve_many",
     "config",
 ]
 
@@ -504,6 +506,93 @@ def solve_batch(design, Y, weights=None, options: LsmrOptions | None = None,
     r.time_setup = t1 - t0
     r.time_total = time.perf_counter() - t0
     return r
+
+
+class SolverSet:
+    """Many independent designs solved together (no counterpart in the
+    reference, which has one design per ``Solver``): ``within_solvers_new``
+    builds one solver per design with the set-up spread over host threads, and
+    ``solve_batch`` solves every design's right-hand sides with ``threads``
+    host threads driving the designs' streams concurrently on the GPU.  Each
+    design keeps its own LSMR state and per-column convergence."""
+
+    def __init__(self, designs, weights=None, preconditioner=None, device: int = -1, threads: int = 8,
+                 precision: str = "fp64"):
+        L = _ffi.lib()
+        self._designs = [_Design(d) for d in designs]
+        n = len(self._designs)
+        ws = [None] * n if weights is None else [None if w is None else _as_f64_1d("weights", w)
+                                                  for w in weights]
+        if len(ws) != n:
+            raise ValueError(f"{len(ws)} weight vectors for {n} designs")
+        for i, (d, w) in enumerate(zip(self._designs, ws)):
+            if w is not None and w.shape[0] != d.n_obs:
+                raise ValueError(f"weights {i} has length {w.shape[0]}, expected {d.n_obs}")
+        dh = (C.c_void_p * max(1, n))(*[d.h.value for d in self._designs])
+        wh = (C.c_void_p * max(1, n))(*[None if w is None else w.ctypes.data for w in ws])
+        cfg = _precond_config(preconditioner)
+        out = (C.c_void_p * max(1, n))()
+        self._threads = int(threads)
+        _ffi.check(L.within_solvers_new(n, dh, wh, None if cfg is None else C.byref(cfg), device,
+                                        self._threads, out))
+        self._h = [C.c_void_p(out[i]) for i in range(n)]
+        self._n_obs = [int(L.within_solver_n_obs(h)) for h in self._h]
+        self._n_dofs = [int(L.within_solver_n_dofs(h)) for h in self._h]
+        for h in self._h:
+            _ffi.check(L.within_solver_set_precision(
+                h, {"fp64": _ffi.PRECISION_FP64, "mixed": _ffi.PRECISION_MIXED}[precision]))
+
+    def __len__(self) -> int:
+        return len(self._h)
+
+    def __del__(self):
+        for h in getattr(self, "_h", []):
+            if h:
+                _ffi.lib().within_solver_free(h)
+        self._h = []
+
+    @property
+    def n_obs(self) -> list[int]:
+        return list(self._n_obs)
+
+    @property
+    def n_dofs(self) -> list[int]:
+        return list(self._n_dofs)
+
+    def solve_batch(self, Ys, options: LsmrOptions | None = None, want_x: bool = True):
+        """``Ys[i]``: (n_obs_i, k_i) float64 (or 1-D).  Returns one
+        (x, demeaned, converged, iterations) tuple per design."""
+        n = len(self._h)
+        if len(Ys) != n:
+            raise ValueError(f"{len(Ys)} right-hand-side blocks for {n} designs")
+        Yf = []
+        for i, Y in enumerate(Ys):
+            Y = np.asarray(Y)
+            Y = Y.reshape(-1, 1) if Y.ndim == 1 else Y
+            Y = _as_f64_2d("Y", Y)
+            if Y.shape[0] != self._n_obs[i]:
+                raise ValueError(f"Y[{i}] has {Y.shape[0]} rows, design has {self._n_obs[i]}")
+            Yf.append(Y)
+        ks = np.array([Y.shape[1] for Y in Yf], np.uint64)
+        X = [np.zeros((self._n_dofs[i], Yf[i].shape[1]), order="F") for i in range(n)] if want_x else None
+        D = [np.zeros(Y.shape, order="F") for Y in Yf]
+        st = [(_ffi.SolveStatsC * max(1, int(k)))() for k in ks]
+        yp = (C.c_void_p * max(1, n))(*[Y.ctypes.data for Y in Yf])
+        xp = (C.c_void_p * max(1, n))(*[x.ctypes.data for x in X]) if want_x else None
+        dp = (C.c_void_p * max(1, n))(*[d.ctypes.data for d in D])
+        sp = (C.c_void_p * max(1, n))(*[C.addressof(x) for x in st])
+        hp = (C.c_void_p * max(1, n))(*[h.value for h in self._h])
+        opts = (options or LsmrOptions())._c()
+        _ffi.check(_ffi.lib().within_solvers_solve_batch(n, hp, yp, _ffi.ptr(ks), C.byref(opts), xp, dp, sp,
+                                                         self._threads))
+        return [((X[i] if want_x else None), D[i], [bool(st[i][j].converged) for j in range(int(ks[i]))],
+                 [int(st[i][j].iterations) for j in range(int(ks[i]))]) for i in range(n)]
+
+
+def solve_many(designs, Ys, weights=None, options: LsmrOptions | None = None, preconditioner=None,
+               threads: int = 8, precision: str = "fp64"):
+    """One-shot ``SolverSet(designs, weights, preconditioner).solve_batch(Ys)``."""
+    return SolverSet(designs, weights, preconditioner, threads=threads, precision=precision).solve_batch(Ys, options)
 
 
 from .autograd import demean  # noqa: E402  (differentiable demeaning; imports torch lazily)

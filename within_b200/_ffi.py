@@ -90,6 +90,8 @@ _SIGNATURES = [
     ("within_solver_operator_apply", C.c_int, [P, P, P, P]),
     ("within_solver_operator_apply_adjoint", C.c_int, [P, P, P, P]),
     ("within_solver_operator_apply_adjoint_noalloc", C.c_int, [P, P, P, P]),
+    ("within_solvers_new", C.c_int, [U64, P, P, P, C.c_int32, C.c_uint32, P]),
+    ("within_solvers_solve_batch", C.c_int, [U64, P, P, P, P, P, P, P, C.c_uint32]),
     ("within_preconditioner_free", None, [P]),
     ("within_preconditioner_n", U64, [P]),
     ("within_preconditioner_variant_name", C.c_char_p, [P]),

@@ -788,10 +788,21 @@ k_alpha_step(uint32_t n, const double* __restrict__ v, const double* __restrict_
 }
 
 // v <- v / alpha; h_bar, x, h update (recurrence.rs:143-191)
+// Ring of the last `cap` (v, p/alpha) pairs for the windowed M-orthogonal
+// reorthogonalisation (bidiag.rs:113-217, 489-512); cap = 0 disables it.
+// Layout [slot][dof][K]; the e-th pair pushed (e = 0 at initialisation, the
+// iteration count after each step) lives in slot e mod cap.
+struct Ring {
+    double* V;
+    double* P;
+    int cap;
+};
+
 template <int K>
 __global__ void k_solution_update(uint32_t n, double* __restrict__ v, double* __restrict__ h,
                                   double* __restrict__ hb, double* __restrict__ x,
-                                  const ColState* nxt, const Ctl* ctl) {
+                                  const ColState* nxt, const Ctl* ctl, Ring ring = Ring{nullptr, nullptr, 0},
+                                  const double* __restrict__ p = nullptr) {
     if (ctl->k5_skip) return;
     double vs[K], tx[K], thb[K], th[K];
     bool up[K];
@@ -802,6 +813,13 @@ __global__ void k_solution_update(uint32_t n, double* __restrict__ v, double* __
         tx[k] = nxt[k].t_x;
         thb[k] = nxt[k].t_hbar;
         th[k] = nxt[k].t_h;
+    }
+    size_t slot[K];
+    double ps[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        slot[k] = ring.cap ? (size_t)(nxt[k].itn % ring.cap) : 0;
+        ps[k] = nxt[k].alpha > 0.0 ? 1.0 / nxt[k].alpha : 0.0;
     }
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
 #pragma unroll
@@ -815,8 +833,69 @@ __global__ void k_solution_update(uint32_t n, double* __restrict__ v, double* __
             hb[o] = hbv;
             x[o] += tx[k] * hbv;
             h[o] = vn - th[k] * ho;
+            if (ring.cap) {
+                const size_t r = (slot[k] * n + j) * K + k;
+                ring.V[r] = vn;
+                ring.P[r] = p[o] * ps[k];
+            }
         }
     }
+}
+
+// One step of the windowed M-orthogonalisation of v against the j-th oldest
+// stored pair (bidiag.rs:489-512, modified Gram-Schmidt order): c = <v, P_e>.
+// Pairs pushed so far: itn + 1; stored: the last min(itn + 1, cap).
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS)
+k_reorth_dot(uint32_t n, int j, Ring ring, const double* __restrict__ v, const ColState* cur, const Ctl* ctl,
+             double* coef, double* partials, unsigned* counter) {
+    if (ctl->all_done) return;
+    size_t slot[K];
+    bool ok[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const long long pushed = cur[k].itn + 1;
+        const long long cnt = pushed < ring.cap ? pushed : ring.cap;
+        ok[k] = !cur[k].done && j < cnt;
+        slot[k] = ok[k] ? (size_t)((pushed - cnt + j) % ring.cap) : 0;
+    }
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (ok[k]) acc[k] += v[(size_t)i * K + k] * ring.P[(slot[k] * n + i) * K + k];
+    double tot[K];
+    if (grid_reduce<K>(acc, partials, counter, tot) && threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) coef[k] = ok[k] ? tot[k] : 0.0;
+}
+
+// v -= c V_e, p -= c P_e with the coefficient of k_reorth_dot
+template <int K>
+__global__ void k_reorth_axpy(uint32_t n, int j, Ring ring, double* __restrict__ v, double* __restrict__ p,
+                              const ColState* cur, const Ctl* ctl, const double* coef) {
+    if (ctl->all_done) return;
+    size_t slot[K];
+    double c[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const long long pushed = cur[k].itn + 1;
+        const long long cnt = pushed < ring.cap ? pushed : ring.cap;
+        const bool ok = !cur[k].done && j < cnt;
+        slot[k] = ok ? (size_t)((pushed - cnt + j) % ring.cap) : 0;
+        c[k] = ok ? coef[k] : 0.0;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (c[k] == 0.0) continue;
+            const size_t o = (size_t)i * K + k;
+            const size_t r = (slot[k] * n + i) * K + k;
+            v[o] -= c[k] * ring.V[r];
+            p[o] -= c[k] * ring.P[r];
+        }
 }
 
 // ---------------------------------------------------------------------------
@@ -1001,10 +1080,14 @@ k_alpha_init(uint32_t n, const double* __restrict__ v, const double* __restrict_
 // v <- v / alpha_1, h = v, x = 0, h_bar = 0  (SolutionState::init)
 template <int K>
 __global__ void k_init_vectors(uint32_t n, double* __restrict__ v, double* __restrict__ h,
-                               double* __restrict__ hb, double* __restrict__ x, const ColState* st) {
-    double vs[K];
+                               double* __restrict__ hb, double* __restrict__ x, const ColState* st,
+                               Ring ring = Ring{nullptr, nullptr, 0}, const double* __restrict__ p = nullptr) {
+    double vs[K], ps[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) vs[k] = (st[k].done || st[k].alpha == 0.0) ? 1.0 : st[k].vscale;
+    for (int k = 0; k < K; ++k) {
+        vs[k] = (st[k].done || st[k].alpha == 0.0) ? 1.0 : st[k].vscale;
+        ps[k] = st[k].alpha > 0.0 ? 1.0 / st[k].alpha : 0.0;
+    }
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -1014,6 +1097,11 @@ __global__ void k_init_vectors(uint32_t n, double* __restrict__ v, double* __res
             h[o] = vn;
             hb[o] = 0.0;
             x[o] = 0.0;
+            if (ring.cap) {   // the first pair, slot 0
+                const size_t r = (size_t)j * K + k;
+                ring.V[r] = vn;
+                ring.P[r] = p[o] * ps[k];
+            }
         }
 }
 

@@ -25,6 +25,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/within_gpu.h"
@@ -458,6 +459,10 @@ struct within_solver {
         uint64_t graph_iters = 0;
         cudaGraphExec_t loop_graph = nullptr;  // the whole loop: a device-side while node
         bool loop_failed = false;
+        // windowed reorthogonalisation (local_size): the ring the graphs were built for
+        Ring ring{nullptr, nullptr, 0};
+        double* coef = nullptr;
+        uint64_t ring_alloc = 0;   // slots allocated
     } work[4];
     // mixed-precision workspaces per K (refine.cuh)
     struct MixedWork {
@@ -784,9 +789,16 @@ void iteration(within_solver& s, within_solver::Work& w, int par, cudaStream_t s
         scatter<K, 1>(s, w.u, w.p, cur, skip, st);
     }
     precond_apply<K>(s, w.ctl, w.p, w.v, skip, st);
+    for (int j = 0; j < w.ring.cap; ++j) {   // M-MGS against the stored window (bidiag.rs:489-512)
+        k_reorth_dot<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, j, w.ring, w.v, cur, w.ctl, w.coef, w.partials,
+                                                          w.counter);
+        k_reorth_axpy<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, j, w.ring, w.v, w.p, cur, w.ctl, w.coef);
+        g_launches += 2;
+    }
     k_alpha_step<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, cur, nxt, w.ctl, w.partials, w.counter);
     ++g_launches;
-    k_solution_update<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, nxt, w.ctl);
+    k_solution_update<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, nxt, w.ctl, w.ring,
+                                                                      w.p);
     ++g_launches;
     (void)n;
 }
@@ -866,7 +878,7 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
     precond_apply<K>(s, w.ctl, w.p, w.v, nullptr, st);
     k_alpha_init<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, w.st, w.st + 8, w.ctl, w.partials,
                                                       w.counter);
-    k_init_vectors<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, w.st);
+    k_init_vectors<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, w.st, w.ring, w.p);
     g_launches += 6;
     Ctl ctl{};
     if (build_loop_graph<K>(s, w)) {
@@ -1134,13 +1146,38 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
         }
 }
 
+// The reorthogonalisation window of a workspace: cap = min(local_size, m, n)
+// pairs (bidiag.rs:113-217).  The graphs bake the window in, so a change of
+// local_size rebuilds them.
+void set_ring(within_solver& s, within_solver::Work& w, int K, uint64_t local_size) {
+    const uint64_t cap = std::min<uint64_t>(local_size, std::min<uint64_t>(s.n_obs, s.n_dofs));
+    if ((int)cap == w.ring.cap) return;
+    if (cap > 4096) throw WError(ERR_UNSUPPORTED, "local_size above 4096 is not supported");
+    if (w.graph) cudaGraphExecDestroy(w.graph);
+    if (w.loop_graph) cudaGraphExecDestroy(w.loop_graph);
+    w.graph = nullptr;
+    w.loop_graph = nullptr;
+    if (cap > w.ring_alloc) {
+        w.ring.V = s.arena.alloc<double>(cap * s.n_dofs * K);
+        w.ring.P = s.arena.alloc<double>(cap * s.n_dofs * K);
+        w.ring_alloc = cap;
+    }
+    if (!w.coef) w.coef = s.arena.alloc<double>(8);
+    w.ring.cap = (int)cap;
+}
+
 void dispatch_solve(within_solver& s, const double* Y_dev, uint64_t k, double tol, uint64_t maxiter,
-                    double* X_dev, double* D_dev, within_solve_stats* stats, cudaStream_t st) {
+                    double* X_dev, double* D_dev, within_solve_stats* stats, cudaStream_t st,
+                    uint64_t local_size = 0) {
     const double t0 = now_s();
+    if (local_size && s.precision == WITHIN_PRECISION_MIXED)
+        throw WError(ERR_UNSUPPORTED, "local_size (windowed reorthogonalisation) applies to the FP64 LSMR solve; "
+                                      "the mixed-precision solve refines instead");
     for (uint64_t c0 = 0; c0 < k; c0 += 8) {
         const uint32_t kk = (uint32_t)std::min<uint64_t>(8, k - c0);
         const int K = k_bucket(kk);
         auto& w = ensure_work(s, K);
+        if (s.precision != WITHIN_PRECISION_MIXED) set_ring(s, w, K, local_size);
         const double* Y = Y_dev + c0 * s.n_obs;
         double* X = X_dev ? X_dev + c0 * s.n_dofs : nullptr;
         double* D = D_dev ? D_dev + c0 * s.n_obs : nullptr;
@@ -1174,8 +1211,7 @@ void validate_opts(const within_lsmr_options* o, double& tol, uint64_t& maxiter,
     }
     if (!std::isfinite(tol) || tol < 0.0)
         throw WError(ERR_INVALID, "tolerance must be finite and nonnegative, got " + std::to_string(tol));
-    if (local_size != 0)
-        throw WError(ERR_UNSUPPORTED, "local_size (windowed reorthogonalisation) is not supported by this build");
+
 }
 
 template <class F>
@@ -1359,7 +1395,7 @@ void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr
         }
     } fr{s.stream, dY, dX, dD};
     CK(cudaMemcpyAsync(dY, pY, k * n * sizeof(double), cudaMemcpyHostToDevice, s.stream));
-    dispatch_solve(s, dY, k, tol, maxiter, dX, dD, stats, s.stream);
+    dispatch_solve(s, dY, k, tol, maxiter, dX, dD, stats, s.stream, ls);
     CK(cudaMemcpyAsync(pD, dD, k * n * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     CK(cudaMemcpyAsync(pX, dX, k * nd * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     CK(cudaStreamSynchronize(s.stream));
@@ -1369,6 +1405,46 @@ void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr
         if (s.reparam.active())
             for (uint64_t j = 0; j < k; ++j) s.reparam.back_transform(X + j * nd);
     }
+}
+
+// Runs fn(i) for i in [0, n) on `threads` host threads (device `dev` current
+// in each); the first failure (code, message) is rethrown on the caller.
+template <class F>
+void parallel_for(uint64_t n, uint32_t threads, int dev, F fn) {
+    std::atomic<uint64_t> next{0};
+    std::mutex emu;
+    int ecode = 0;
+    std::string emsg;
+    auto work = [&] {
+        try {
+            set_device(dev);
+            for (uint64_t i; (i = next.fetch_add(1)) < n;) {
+                {
+                    std::lock_guard<std::mutex> g(emu);
+                    if (ecode) return;
+                }
+                fn(i);
+            }
+        } catch (const WError& e) {
+            std::lock_guard<std::mutex> g(emu);
+            if (!ecode) {
+                ecode = e.code;
+                emsg = e.what();
+            }
+        } catch (const std::exception& e) {
+            std::lock_guard<std::mutex> g(emu);
+            if (!ecode) {
+                ecode = ERR_CUDA;
+                emsg = e.what();
+            }
+        }
+    };
+    const uint32_t t = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(threads ? threads : 1, n));
+    std::vector<std::thread> pool;
+    for (uint32_t j = 1; j < t; ++j) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    if (ecode) throw WError(ecode, emsg);
 }
 
 }  // namespace
@@ -1460,6 +1536,40 @@ int within_solver_new(const within_design* design, const double* weights, const 
     return guarded([&] { *out = make_solver(design, weights, cfg, prebuilt, device); });
 }
 
+int within_solvers_new(uint64_t n, const within_design* const* designs, const double* const* weights,
+                       const within_precond_config* cfg, int32_t device, uint32_t threads, within_solver** out) {
+    return guarded([&] {
+        for (uint64_t i = 0; i < n; ++i) out[i] = nullptr;
+        int dev = device;
+        if (dev < 0) CK(cudaGetDevice(&dev));
+        try {
+            parallel_for(n, threads, dev, [&](uint64_t i) {
+                if (!designs[i]) throw WError(ERR_INVALID, "design " + std::to_string(i) + " is null");
+                out[i] = make_solver(designs[i], weights ? weights[i] : nullptr, cfg, nullptr, dev);
+            });
+        } catch (...) {
+            for (uint64_t i = 0; i < n; ++i) {
+                delete out[i];
+                out[i] = nullptr;
+            }
+            throw;
+        }
+    });
+}
+
+int within_solvers_solve_batch(uint64_t n, within_solver* const* solvers, const double* const* Y, const uint64_t* k,
+                               const within_lsmr_options* opts, double* const* X, double* const* D,
+                               within_solve_stats* const* stats, uint32_t threads) {
+    return guarded([&] {
+        if (n == 0) return;
+        parallel_for(n, threads, solvers[0]->device, [&](uint64_t i) {
+            if (k[i] == 0) return;
+            host_solve(*solvers[i], Y[i], k[i], opts, X ? X[i] : nullptr, D ? D[i] : nullptr,
+                       stats ? stats[i] : nullptr);
+        });
+    });
+}
+
 void within_solver_free(within_solver* s) {
     if (!s) return;
     cudaSetDevice(s->device);
@@ -1534,7 +1644,7 @@ int within_solver_solve_batch_device(within_solver* s, const double* Y_dev, uint
         std::lock_guard<std::mutex> g(s->mu);
         set_device(s->device);
         cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
-        dispatch_solve(*s, Y_dev, k, tol, maxiter, X_dev, D_dev, stats, st);
+        dispatch_solve(*s, Y_dev, k, tol, maxiter, X_dev, D_dev, stats, st, ls);
         if (X_dev && s->reparam.active()) {
             std::vector<double> hx(k * s->n_dofs);
             CK(cudaMemcpyAsync(hx.data(), X_dev, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
