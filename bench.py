@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision batched section")
+    ap.add_argument("--no-many", action="store_true", help="skip the many-designs section")
+    ap.add_argument("--many", type=int, default=256, help="designs in the many-designs section")
+    ap.add_argument("--no-autograd", action="store_true", help="skip the differentiable-demeaning section")
     ap.add_argument("--cpu-sample-iters", type=int, default=3)
     return ap.parse_args()
 
@@ -236,6 +239,89 @@ def mixed_section(W, codes, dev, stream, args):
     return out
 
 
+def many_section(W, args):
+    """Many independent designs: `args.many` designs with n log-uniform in
+    [1e4, 2e6], 2-3 uniform factors with level counts log-uniform in
+    [20, n/10], k = 8 right-hand sides each, through SolverSet.solve_batch
+    (host buffers in and out); solves/s = designs x 8 / wall time of the
+    batch (host-driven concurrent streams, so the host clock is the measure)."""
+    from within_b200 import workloads as WL
+    cases = WL.many_designs(count=args.many, k=8)
+    rows = int(sum(c.shape[0] for c, _ in cases))
+    t0 = time.perf_counter()
+    ss = W.SolverSet([c for c, _ in cases], threads=16)
+    t_setup = time.perf_counter() - t0
+    Ys = [Y for _, Y in cases]
+    opts = W.LsmrOptions(tol=args.tol)
+    ss.solve_batch(Ys, opts, want_x=False)
+    reps = 2
+    t1 = time.perf_counter()
+    for _ in range(reps):
+        out = ss.solve_batch(Ys, opts, want_x=False)
+    t = (time.perf_counter() - t1) / reps
+    its = [it for o in out for it in o[3]]
+    res = {"designs": len(cases), "k": 8, "rows_total": rows, "value": len(cases) * 8 / t, "unit": UNIT,
+           "s_per_batch": t, "setup_s": t_setup, "iterations_max": int(max(its)),
+           "iterations_median": float(np.median(its)), "converged": all(all(o[2]) for o in out),
+           "fp64": True, "timing": "host wall clock of SolverSet.solve_batch, host buffers in and out"}
+    del ss
+    return res
+
+
+def autograd_section(W, dev):
+    """Differentiable demeaning on the varying-slopes panel (n = 2e6, firm 50k
+    Pareto(1.5) with intercept + slope, year 30, weights lognormal(0, 0.5)):
+    forward and backward time, and the gradients against central differences
+    (step 1e-6) of the GPU solver on 8 weight and 8 response coordinates."""
+    import torch
+    from within_b200 import workloads as WL
+    firm, year, x, z, w, v = WL.slopes_panel()
+    eff = [W.Effect(firm, True, [x]), W.Effect(year, True)]
+    opts = W.LsmrOptions(tol=1e-13, maxiter=20000)
+    zt = torch.tensor(z, device=dev, requires_grad=True)
+    wt = torch.tensor(w, device=dev, requires_grad=True)
+    vt = torch.tensor(v, device=dev)
+    solver = W.Solver(eff, weights=w, device=dev.index)
+    out = W.demean(zt, eff, weights=wt, options=opts, solver=solver)
+    (vt * out).sum().backward()
+    torch.cuda.synchronize(dev)
+    zt.grad = None
+    wt.grad = None
+    a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    a.record()
+    out = W.demean(zt, eff, weights=wt, options=opts, solver=solver)
+    loss = (vt * out).sum()
+    b.record()
+    loss.backward()
+    c.record()
+    torch.cuda.synchronize(dev)
+    gw = wt.grad.cpu().numpy()
+    gz = zt.grad.cpu().numpy()
+    rng = np.random.default_rng(5)
+    idx = rng.choice(z.size, 8, replace=False)
+    h = 1e-6
+
+    def r_of(wv, zv):
+        return W.Solver(eff, weights=wv, device=dev.index).solve(zv, opts).demeaned
+
+    fd_w, fd_z = [], []
+    base = solver.solve(z, opts).demeaned
+    for i in idx:
+        wp, wm = w.copy(), w.copy()
+        wp[i] += h
+        wm[i] -= h
+        fd_w.append(float(v @ (r_of(wp, z) - r_of(wm, z))) / (2 * h))
+        zp = z.copy()
+        zp[i] += h
+        fd_z.append(float(v @ (solver.solve(zp, opts).demeaned - base)) / h)
+    fd_w, fd_z = np.array(fd_w), np.array(fd_z)
+    return {"n": int(z.size), "forward_ms": a.elapsed_time(b), "backward_ms": b.elapsed_time(c),
+            "grad_w_rel_err_vs_fd": float(np.max(np.abs(gw[idx] - fd_w)) / np.max(np.abs(fd_w))),
+            "grad_z_rel_err_vs_fd": float(np.max(np.abs(gz[idx] - fd_z)) / np.max(np.abs(fd_z))),
+            "fd": "central differences, step 1e-6, 8 random weight coordinates (new Solver per "
+                  "perturbation); forward differences for the linear z coordinates; tol 1e-13"}
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
@@ -313,6 +399,8 @@ def run_ours(args):
                "iterations_max": max(s_[1] for s_ in stb), "demeaned_err_vs_fp64_tol1e-12": err_b,
                "speedup_vs_single": (kb / t_b) / value * world}
     mixed = None if args.no_mixed else mixed_section(W, codes, dev, stream, args)
+    many = None if (args.no_many or world > 1) else many_section(W, args)
+    autograd = None if (args.no_autograd or world > 1) else autograd_section(W, dev)
     # e2e through the host API (numpy in, numpy out)
     for _ in range(1):
         solver.solve(y, opts)
@@ -363,6 +451,7 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(n, nd),
         "iterations": it, "lsmr_iters_per_s": world * sum(iters) / t_max, "setup_s": t_setup,
         "demeaned_err_vs_fp64_tol1e-12": err, "batched_fp64": batched, "mixed_batched": mixed,
+        "many_designs": many, "autograd": autograd,
         "roofline": roof,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * (n + nd)},
