@@ -52,7 +52,7 @@ __host__ __device__ constexpr int rw_rows() { return K >= 4 ? 2 : K == 2 ? 4 : 8
 template <int K>
 __host__ __device__ constexpr int rw_chunk() { return 32 * rw_rows<K>(); }
 template <int K>
-__host__ __device__ constexpr int rw_min_blocks() { return K >= 8 || K == 1 ? 2 : 3; }
+__host__ __device__ constexpr int rw_min_blocks() { return 2; }
 // fixed grid: 148 SMs x resident blocks per SM
 template <int K>
 __host__ __device__ constexpr int rw_grid() { return 148 * rw_min_blocks<K>(); }
@@ -131,6 +131,73 @@ __device__ __forceinline__ void rw_load_codes(const uint32_t* __restrict__ c, ui
     }
 }
 
+// N consecutive values (16-byte aligned when full) as doubles
+template <int N, class T>
+__device__ __forceinline__ void rw_load_vals(const T* __restrict__ src, int n_valid, double (&out)[N]) {
+    if (n_valid == N) {
+        if constexpr (sizeof(T) == 8) {
+#pragma unroll
+            for (int i = 0; i < N / 2; ++i) {
+                const double2 q = *reinterpret_cast<const double2*>(src + 2 * i);
+                out[2 * i] = q.x;
+                out[2 * i + 1] = q.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < N / 4; ++i) {
+                const float4 q = *reinterpret_cast<const float4*>(src + 4 * i);
+                out[4 * i] = q.x;
+                out[4 * i + 1] = q.y;
+                out[4 * i + 2] = q.z;
+                out[4 * i + 3] = q.w;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) out[i] = i < n_valid ? (double)src[i] : 0.0;
+    }
+}
+
+template <int N, class T>
+__device__ __forceinline__ void rw_store_vals(T* __restrict__ dst, int n_valid, const T (&in)[N]) {
+    if (n_valid == N) {
+        if constexpr (sizeof(T) == 8) {
+#pragma unroll
+            for (int i = 0; i < N / 2; ++i)
+                *reinterpret_cast<double2*>(dst + 2 * i) = make_double2(in[2 * i], in[2 * i + 1]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < N / 4; ++i)
+                *reinterpret_cast<float4*>(dst + 4 * i) = make_float4(in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3]);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            if (i < n_valid) dst[i] = in[i];
+    }
+}
+
+constexpr int RW_QR = 3;   // terms whose codes stay in registers for a whole chunk
+
+// codes of term t for the lane's rows: from the registers of the first RW_QR
+// terms, else loaded
+template <int R, class T>
+__device__ __forceinline__ void rw_pick_codes(const OpParamsT<T>& p, int t, uint32_t row0, int nr,
+                                              const uint32_t (&cdq)[RW_QR][R], uint32_t (&cd)[R]) {
+    if (t < RW_QR) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            uint32_t c = cdq[0][r];
+#pragma unroll
+            for (int q = 1; q < RW_QR; ++q)
+                if (t == q) c = cdq[q][r];
+            cd[r] = c;
+        }
+    } else {
+        rw_load_codes<R>(p.codes[t], row0, nr, cd);
+    }
+}
+
 template <class T>
 __device__ __forceinline__ double rw_load(const OpParamsT<T>& p, int t, int c, uint32_t row) {
     const int li = p.load[t][c];
@@ -201,22 +268,52 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     for (uint32_t c0 = r0; c0 < r1; c0 += CH) {
         const uint32_t row0 = c0 + (uint32_t)lane * R;
         const int nr = row0 < r1 ? (int)min((uint32_t)R, r1 - row0) : 0;
+        // ---- every load that depends on nothing else, issued at once: the codes
+        // of the first RW_QR terms (kept for the whole chunk), u and sqrt(w)
+        uint32_t cdq[RW_QR][R];
+#pragma unroll
+        for (int t = 0; t < RW_QR; ++t) {
+            if (t < p.Q) {
+                rw_load_codes<R>(p.codes[t], row0, nr, cdq[t]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) cdq[t][r] = 0u;
+            }
+        }
+        double uin[R * K];
+        if (MODE != 2) rw_load_vals<R * K, T>(u + (size_t)row0 * K, nr * K, uin);
+        double wv[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) wv[r] = (r < nr && p.sqrt_w) ? (double)__ldg(p.sqrt_w + row0 + r) : 1.0;
         // ---- row values b = W^{1/2} u (mode 0), of the updated u (mode 1), or w D p (mode 2)
         double b[R][K];
         if (MODE == 0) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const double w = (r < nr && p.sqrt_w) ? (double)__ldg(p.sqrt_w + row0 + r) : 1.0;
+            for (int r = 0; r < R; ++r)
 #pragma unroll
-                for (int k = 0; k < K; ++k) b[r][k] = r < nr ? w * (double)u[(size_t)(row0 + r) * K + k] : 0.0;
-            }
+                for (int k = 0; k < K; ++k) b[r][k] = r < nr ? wv[r] * uin[r * K + k] : 0.0;
         } else {
             double s[R][K];
 #pragma unroll
             for (int r = 0; r < R; ++r)
 #pragma unroll
                 for (int k = 0; k < K; ++k) s[r][k] = 0.0;
-            for (int t = 0; t < p.Q; ++t) {
+#pragma unroll
+            for (int t = 0; t < RW_QR; ++t) {
+                if (t >= p.Q) break;
+                for (int c = 0; c < p.ncol[t]; ++c) {
+                    const size_t col = (size_t)p.off[t] + (size_t)c * p.L[t];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        if (r >= nr) continue;
+                        const double ld = rw_load(p, t, c, row0 + r);
+                        const T* xr = v + (col + cdq[t][r]) * K;
+#pragma unroll
+                        for (int k = 0; k < K; ++k) s[r][k] += (double)__ldg(xr + k) * ld;
+                    }
+                }
+            }
+            for (int t = RW_QR; t < p.Q; ++t) {
                 uint32_t cd[R];
                 rw_load_codes<R>(p.codes[t], row0, nr, cd);
                 for (int c = 0; c < p.ncol[t]; ++c) {
@@ -231,30 +328,33 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                     }
                 }
             }
+            T outv[R * K];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const double w = (r < nr && p.sqrt_w) ? (double)__ldg(p.sqrt_w + row0 + r) : 1.0;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                     double val = 0.0;
                     if (r < nr) {
-                        const double av = p.sqrt_w ? w * s[r][k] : s[r][k];
+                        const double av = p.sqrt_w ? wv[r] * s[r][k] : s[r][k];
                         if (MODE == 1) {
-                            T* up = u + (size_t)(row0 + r) * K + k;
-                            const double nu = act[k] ? av + scale[k] * (double)(*up) : (double)(*up);
+                            const double nu = act[k] ? av + scale[k] * uin[r * K + k] : uin[r * K + k];
                             const T nut = (T)nu;
-                            if (act[k]) *up = nut;
                             accn[k] += (double)nut * (double)nut;
                             val = (double)nut;
+                            outv[r * K + k] = nut;
                         } else {
                             const T tt = (T)av;
-                            if (store) u[(size_t)(row0 + r) * K + k] = tt;
                             val = (double)tt;
+                            outv[r * K + k] = tt;
                         }
+                    } else {
+                        outv[r * K + k] = (T)0;
                     }
-                    b[r][k] = p.sqrt_w ? w * val : val;
+                    b[r][k] = p.sqrt_w ? wv[r] * val : val;
                 }
             }
+            // finished columns store their unchanged u back (same bytes)
+            if (MODE == 1 || store) rw_store_vals<R * K, T>(u + (size_t)row0 * K, nr * K, outv);
         }
 
         // ---- hist terms: per-lane bins, or per-warp bins grouped by level per 32-row step
@@ -262,7 +362,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             const int t = rw.hist[hh].term;
             const int ncol = p.ncol[t];
             uint32_t hc[R];
-            rw_load_codes<R>(p.codes[t], row0, nr, hc);
+            rw_pick_codes<R>(p, t, row0, nr, cdq, hc);
             if (rw.hist_private) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
@@ -315,7 +415,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             const int ncol = p.ncol[t];
             const uint32_t* cdp = p.codes[t];
             uint32_t cd[R];
-            rw_load_codes<R>(cdp, row0, nr, cd);
+            rw_pick_codes<R>(p, t, row0, nr, cdq, cd);
             // head flags: a row whose code differs from the previous row's
             const uint32_t upc = __shfl_up_sync(FULL, cd[R - 1], 1);
             const uint32_t pc0 = lane == 0 ? prevc[j] : upc;

@@ -10,8 +10,9 @@
 // tile, so work is balanced no matter how the segment lengths are distributed
 // (a Pareto firm of 10^6 rows costs the same per row as a worker of 10).  A CTA
 // loads its tile (coalesced where the value functor reads contiguously), runs
-// a block-wide segmented inclusive scan (CUB BlockScan) and emits every segment
-// that starts and ends inside the tile.  A segment that crosses tiles leaves a
+// a block-wide segmented inclusive scan over all K columns at once (thread
+// sums, a warp shuffle scan, one shared-memory exchange of the warp
+// aggregates) and emits every segment that starts and ends inside the tile.  A segment that crosses tiles leaves a
 // tail partial (its owner tile) and head partials (the tiles it continues into);
 // the last of those CTAs to finish -- decided by one atomic counter per split
 // segment, not a wait -- adds them in tile order and emits.  Every sum is
@@ -22,39 +23,18 @@
 // segment pointer arrays, which never change after set-up.
 #pragma once
 #include <cstdint>
-#include <cub/block/block_scan.cuh>
 
 #include "segplan.hpp"
 
 namespace wgpu {
 
 template <int K>
-struct SegItem {
-    double v[K];
-    int sid;  // id of the segment that starts here (scan: the segment this position belongs to), -1 = none
-};
-
-template <int K>
-struct SegSumOp {
-    __device__ __forceinline__ SegItem<K> operator()(const SegItem<K>& a, const SegItem<K>& b) const {
-        if (b.sid >= 0) return b;
-        SegItem<K> c;
-#pragma unroll
-        for (int k = 0; k < K; ++k) c.v[k] = a.v[k] + b.v[k];
-        c.sid = a.sid;
-        return c;
-    }
-};
-
-template <int K>
-constexpr int sr_items() { return K >= 4 ? 2 : 4; }
+constexpr int sr_items() { return K >= 8 ? 2 : 4; }
 template <int K>
 constexpr int sr_tile() { return SR_THREADS * sr_items<K>(); }
 // resident CTAs per SM the register budget is sized for (no spills at K = 8)
 template <int K>
 constexpr int sr_min_blocks() { return K >= 8 ? 2 : (K >= 4 ? 3 : (K >= 2 ? 4 : 6)); }
-// the scan runs one column at a time over the positions' K-wide values
-using SegItem1 = SegItem<1>;
 
 // F provides:
 //   using Prob = ...;                 (trivially copyable, <= 256 bytes)
@@ -63,9 +43,11 @@ using SegItem1 = SegItem<1>;
 //   __device__ void value(const Prob&, uint32_t pos, double (&v)[K]) const;
 //   __device__ void emit(const Prob&, uint32_t seg, const double (&s)[K]) const;
 //
-// The block scan carries, for every position, the id of the segment it belongs
-// to, so the thread holding a segment's last position emits it straight from
-// registers; only the 2048-entry head table lives in shared memory.
+// The scan carries, for every position, the id of the segment it belongs to
+// (-1: the segment continuing from the previous tile), so the thread holding
+// a segment's last position emits it straight from registers; the scan's
+// combine is "a segment start resets the sum", and the id >= 0 of the last
+// start doubles as the reset flag.
 template <class F, int K>
 __global__ void __launch_bounds__(SR_THREADS, sr_min_blocks<K>())
 segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
@@ -75,8 +57,9 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     constexpr int ITEMS = sr_items<K>();
     constexpr int T = SR_THREADS * ITEMS;
     using Prob = typename F::Prob;
-    using Scan = cub::BlockScan<SegItem1, SR_THREADS>;
-    __shared__ typename Scan::TempStorage scan_tmp;
+    constexpr int NW = SR_THREADS / 32;
+    __shared__ double wagg[NW][K];
+    __shared__ int wsid[NW];
     __shared__ int headseg[T + 1];
     __shared__ double wsum[(SR_THREADS / 32) * K];
     __shared__ SRTile tile;
@@ -122,23 +105,85 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
             sid[i] = -2;   // past the tile end: never emitted
         }
     }
-    // one segmented inclusive scan per column; the carried segment id is the
-    // same for every column
+    // segmented inclusive scan of all K columns: (1) the thread's own items,
+    const unsigned FULL = 0xffffffffu;
+    const int lane = tid & 31, wid = tid >> 5;
+    int ts = -1;   // id of the thread's last segment start, -1 = none
+    double tv[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        SegItem1 it[ITEMS];
+    for (int k = 0; k < K; ++k) tv[k] = 0.0;
 #pragma unroll
-        for (int i = 0; i < ITEMS; ++i) {
-            it[i].v[0] = val[i][k];
-            it[i].sid = sid[i];
+    for (int i = 0; i < ITEMS; ++i) {
+        if (sid[i] >= 0) {
+            ts = sid[i];
+#pragma unroll
+            for (int k = 0; k < K; ++k) tv[k] = val[i][k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) tv[k] += val[i][k];
         }
-        if (k > 0) __syncthreads();   // scan_tmp reuse
-        Scan(scan_tmp).InclusiveScan(it, it, SegSumOp<1>());
+    }
+    // (2) the warp (shuffle tree),
 #pragma unroll
-        for (int i = 0; i < ITEMS; ++i) {
-            val[i][k] = it[i].v[0];
-            if (k == K - 1) sid[i] = it[i].sid;
+    for (int d = 1; d < 32; d <<= 1) {
+        double up[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) up[k] = __shfl_up_sync(FULL, tv[k], d);
+        const int us = __shfl_up_sync(FULL, ts, d);
+        if (lane >= d && ts < 0) {
+            ts = us;
+#pragma unroll
+            for (int k = 0; k < K; ++k) tv[k] += up[k];
         }
+    }
+    double ex[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) ex[k] = __shfl_up_sync(FULL, tv[k], 1);
+    int exs = __shfl_up_sync(FULL, ts, 1);
+    if (lane == 0) {
+        exs = -1;
+#pragma unroll
+        for (int k = 0; k < K; ++k) ex[k] = 0.0;
+    }
+    if (lane == 31) {
+        wsid[wid] = ts;
+#pragma unroll
+        for (int k = 0; k < K; ++k) wagg[wid][k] = tv[k];
+    }
+    __syncthreads();
+    // (3) the warps before this one, in warp order
+    int cs = -1;
+    double cv[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) cv[k] = 0.0;
+    for (int q = 0; q < wid; ++q) {
+        if (wsid[q] >= 0) {
+            cs = wsid[q];
+#pragma unroll
+            for (int k = 0; k < K; ++k) cv[k] = wagg[q][k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) cv[k] += wagg[q][k];
+        }
+    }
+    // carry into this thread, then its items again
+    int rs = exs >= 0 ? exs : cs;
+    double run[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) run[k] = exs >= 0 ? ex[k] : cv[k] + ex[k];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        if (sid[i] >= 0) {
+            rs = sid[i];
+#pragma unroll
+            for (int k = 0; k < K; ++k) run[k] = val[i][k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) run[k] += val[i][k];
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) val[i][k] = run[k];
+        if (sid[i] != -2) sid[i] = rs;
     }
 
     // emit at the last position of each segment piece held by this thread
