@@ -45,6 +45,8 @@ struct CgCol {
     int err;
 };
 
+static_assert(sizeof(CgCol) % sizeof(double) == 0, "CgCol is addressed in doubles by the residual sweep");
+
 // r = b - A x (FP64) and ||r||^2 per column
 template <int K>
 __global__ void __launch_bounds__(RED_THREADS)

@@ -32,7 +32,8 @@
 // Modes: 0 -- A^T u of a given u (Operator::apply_adjoint);  1 -- LSMR step
 // (u updated and stored, beta);  2 -- normal operator A^T A p for the CG of
 // the mixed-precision solve (t = A p formed in registers; stored only when
-// rest terms need it).
+// rest terms need it);  3 -- the refinement step's FP64 residual r = b - A x,
+// ||r||^2 and g = A^T r in one pass (r stored only when rest terms need it).
 #pragma once
 #include <type_traits>
 
@@ -207,8 +208,9 @@ __device__ __forceinline__ double rw_load(const OpParamsT<T>& p, int t, int c, u
 template <int K, int MODE, class T>
 __global__ void __launch_bounds__(RW_THREADS, rw_min_blocks<K>())
 k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__ u, ColState* cur, Ctl* ctl,
-           const int* skip, int store) {
+           const int* skip, int store, const T* __restrict__ rhs, double* sq_out, int sq_stride) {
     using TO = std::conditional_t<MODE == 2, T, double>;
+    constexpr bool NORM = MODE == 1 || MODE == 3;   // the row values' squared norm per column
     constexpr int R = rw_rows<K>();
     constexpr int CH = 32 * R;
     constexpr int MAXCR = rw_max_cols<K>();
@@ -281,7 +283,8 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             }
         }
         double uin[R * K];
-        if (MODE != 2) rw_load_vals<R * K, T>(u + (size_t)row0 * K, nr * K, uin);
+        if (MODE == 0 || MODE == 1) rw_load_vals<R * K, T>(u + (size_t)row0 * K, nr * K, uin);
+        if (MODE == 3) rw_load_vals<R * K, T>(rhs + (size_t)row0 * K, nr * K, uin);
         double wv[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) wv[r] = (r < nr && p.sqrt_w) ? (double)__ldg(p.sqrt_w + row0 + r) : 1.0;
@@ -342,6 +345,11 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                             accn[k] += (double)nut * (double)nut;
                             val = (double)nut;
                             outv[r * K + k] = nut;
+                        } else if (MODE == 3) {
+                            const double rr = uin[r * K + k] - av;
+                            accn[k] += rr * rr;
+                            val = rr;
+                            outv[r * K + k] = (T)rr;
                         } else {
                             const T tt = (T)av;
                             val = (double)tt;
@@ -578,7 +586,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             bins[i * 32] = s;
         }
     }
-    if (MODE == 1) {
+    if (NORM) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const double s = warp_sum(accn[k]);
@@ -587,7 +595,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     }
     __syncthreads();
     double* mypart = rw.part + (size_t)blockIdx.x * stride;
-    if (MODE == 1 && threadIdx.x < K) {
+    if (NORM && threadIdx.x < K) {
         double s = 0.0;
         for (int w = 0; w < RW_WARPS; ++w) s += red[w][threadIdx.x];
         mypart[threadIdx.x] = s;
@@ -608,11 +616,12 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     __threadfence();
     // ---- last block: grand totals in block order, bins -> A^T u, crossing runs
     for (int i = wid; i < stride; i += RW_WARPS) {
-        if (i < K && MODE != 1) continue;
+        if (i < K && !NORM) continue;
         const double a = warp_col_sum(rw.part, gridDim.x, stride, i);
         if (lane != 0) continue;
         if (i < K) {
-            if (act[i]) cur[i].beta = sqrt(a);
+            if (MODE == 1 && act[i]) cur[i].beta = sqrt(a);
+            if (MODE == 3) sq_out[(size_t)i * sq_stride] = a;
             continue;
         }
         const int bk = (i - K) / K, k = (i - K) % K;

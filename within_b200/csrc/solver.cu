@@ -656,6 +656,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
         CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
         CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
         CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
     }
     rk.ready = true;
     return rk;
@@ -678,10 +679,12 @@ void ensure_rowsweep_f(within_solver& s) {
 
 template <int K, int MODE, class T>
 void launch_rowsweep(within_solver& s, within_solver::RowSweepK& rk, const OpParamsT<T>& op, void* atu, const T* v,
-                     T* u, ColState* cur, Ctl* ctl, const int* skip, int store, cudaStream_t st) {
+                     T* u, ColState* cur, Ctl* ctl, const int* skip, int store, cudaStream_t st,
+                     const T* rhs = nullptr, double* sq_out = nullptr, int sq_stride = 0) {
     RwParams rp = rk.rp;
     rp.atu = atu;
-    k_rowsweep<K, MODE, T><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip, store);
+    k_rowsweep<K, MODE, T><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip, store, rhs,
+                                                                       sq_out, sq_stride);
     ++g_launches;
 }
 
@@ -1096,8 +1099,17 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
     CgCol fin[8];
     Ctl ctl{};
     for (int outer = 0;; ++outer) {
-        k_resid64<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, m.x64, w.b, m.r64, m.st, w.partials, w.counter);
-        scatter<K, 0>(s, m.r64, m.g64, nullptr, nullptr, st);
+        if (s.path[kidx(K)] == 2) {   // r = b - A x, ||r||^2 and g = A^T r in one row sweep
+            auto& rk = s.rsw[kidx(K)];
+            launch_rowsweep<K, 3, double>(s, rk, s.op, m.g64, m.x64, m.r64, nullptr, nullptr, nullptr,
+                                          rk.rest_needs_rows ? 1 : 0, st, w.b, &m.st[0].rnorm2,
+                                          (int)(sizeof(CgCol) / sizeof(double)));
+            rowsweep_rest<K, double>(s, rk, m.r64, m.g64, nullptr, st);
+            g_launches -= 1;   // counted below with the fixed kernels of the step
+        } else {
+            k_resid64<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, m.x64, w.b, m.r64, m.st, w.partials, w.counter);
+            scatter<K, 0>(s, m.r64, m.g64, nullptr, nullptr, st);
+        }
         k_cg_start<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.g64, m.res, m.d);
         precond_apply<K, float>(s, m.ctl, m.res, m.z, nullptr, st);
         k_cg_init<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.p, m.st, m.ctl, outer == 0 ? 1 : 0,
@@ -1107,7 +1119,19 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
         CK(cudaStreamSynchronize(st));
         if (ctl.all_done || ctl.err) break;
         const int runs0 = ctl.bodies_run;
-        CK(cudaGraphLaunch(m.loop_graph, st));
+        if (const char* e = getenv("WITHIN_GRAPH_LOOP"); e && atoi(e) == 0) {
+            // plain launches, one host check per iteration (for profilers that
+            // do not follow conditional graph bodies)
+            for (uint64_t it = 0; it <= maxiter; ++it) {
+                cg_iteration<K>(s, w, m, st);
+                CK(cudaMemcpyAsync(&ctl, m.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (ctl.all_done || ctl.err) break;
+            }
+            ctl.bodies_run = runs0;
+        } else {
+            CK(cudaGraphLaunch(m.loop_graph, st));
+        }
         k_add_delta<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.d, m.x64);
         ++g_launches;
         CK(cudaMemcpyAsync(&ctl, m.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
