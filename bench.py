@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-many", action="store_true", help="skip the many-designs section")
     ap.add_argument("--many", type=int, default=256, help="designs in the many-designs section")
     ap.add_argument("--no-autograd", action="store_true", help="skip the differentiable-demeaning section")
+    ap.add_argument("--kernel-timeline", choices=["fp64", "mixed"], default=None,
+                    help="instead of the bench line: per-kernel device times of one solve (torch.profiler "
+                         "/ CUPTI timestamps); 'mixed' = weighted panel, k = 4, mixed precision")
     ap.add_argument("--cpu-sample-iters", type=int, default=3)
     return ap.parse_args()
 
@@ -477,8 +480,50 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def kernel_timeline(args):
+    """Per-kernel device durations of one solve of the bench workload, from
+    CUPTI timestamps (torch.profiler).  The conditional-graph loop reports one
+    body (two LSMR iterations / one CG iteration); the table gives each
+    kernel's mean duration and count within the recorded window."""
+    import collections
+    import re
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    import within_b200 as W
+    codes, y = workload(args.rows)
+    dev = torch.device("cuda", 0)
+    if args.kernel_timeline == "mixed":
+        rng = np.random.default_rng(4)
+        w = rng.lognormal(0.0, 1.0, codes.shape[0])
+        s = W.Solver(codes, weights=w, precision="mixed")
+        Y = torch.tensor(np.asfortranarray(rng.standard_normal((codes.shape[0], 4))), device=dev)
+        Y = Y.t().contiguous().t()
+    else:
+        s = W.Solver(codes)
+        Y = torch.tensor(y, device=dev)
+    opts = W.LsmrOptions(tol=args.tol)
+    for _ in range(2):
+        s.solve_device(Y, opts)
+    torch.cuda.synchronize(dev)
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        s.solve_device(Y, opts)
+        torch.cuda.synchronize(dev)
+    dur = collections.defaultdict(list)
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA and e.name.startswith("void wgpu::") or \
+                e.name.startswith("wgpu::"):
+            dur[re.sub(r"\(.*", "", e.name).replace("void ", "")].append(e.device_time_total if hasattr(
+                e, "device_time_total") else e.cuda_time_total)
+    out = {k: {"launches": len(v), "mean_us": float(np.mean(v)), "total_us": float(np.sum(v))}
+           for k, v in sorted(dur.items(), key=lambda kv: -sum(kv[1]))}
+    print(json.dumps({"kernel_timeline": args.kernel_timeline, "rows": args.rows, "kernels": out}, indent=1))
+
+
 def main():
     args = parse()
+    if args.kernel_timeline:
+        kernel_timeline(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -29,6 +29,8 @@
 //               order.
 //   rest terms  left to the segmented reduction over the level-sorted
 //               observation permutation (segreduce.cuh).
+// SIMPLE: every term is intercept-only (one column, no loading), chosen per
+// design at set-up.
 // Modes: 0 -- A^T u of a given u (Operator::apply_adjoint);  1 -- LSMR step
 // (u updated and stored, beta);  2 -- normal operator A^T A p for the CG of
 // the mixed-precision solve (t = A p formed in registers; stored only when
@@ -205,7 +207,7 @@ __device__ __forceinline__ double rw_load(const OpParamsT<T>& p, int t, int c, u
     return li < 0 ? 1.0 : (double)__ldg(p.loads[li] + row);
 }
 
-template <int K, int MODE, class T>
+template <int K, int MODE, class T, bool SIMPLE>
 __global__ void __launch_bounds__(RW_THREADS, rw_min_blocks<K>())
 k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__ u, ColState* cur, Ctl* ctl,
            const int* skip, int store, const T* __restrict__ rhs, double* sq_out, int sq_stride) {
@@ -304,12 +306,12 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
 #pragma unroll
             for (int t = 0; t < RW_QR; ++t) {
                 if (t >= p.Q) break;
-                for (int c = 0; c < p.ncol[t]; ++c) {
+                for (int c = 0; c < (SIMPLE ? 1 : p.ncol[t]); ++c) {
                     const size_t col = (size_t)p.off[t] + (size_t)c * p.L[t];
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         if (r >= nr) continue;
-                        const double ld = rw_load(p, t, c, row0 + r);
+                        const double ld = (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r));
                         const T* xr = v + (col + cdq[t][r]) * K;
 #pragma unroll
                         for (int k = 0; k < K; ++k) s[r][k] += (double)__ldg(xr + k) * ld;
@@ -319,12 +321,12 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             for (int t = RW_QR; t < p.Q; ++t) {
                 uint32_t cd[R];
                 rw_load_codes<R>(p.codes[t], row0, nr, cd);
-                for (int c = 0; c < p.ncol[t]; ++c) {
+                for (int c = 0; c < (SIMPLE ? 1 : p.ncol[t]); ++c) {
                     const size_t col = (size_t)p.off[t] + (size_t)c * p.L[t];
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         if (r >= nr) continue;
-                        const double ld = rw_load(p, t, c, row0 + r);
+                        const double ld = (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r));
                         const T* xr = v + (col + cd[r]) * K;
 #pragma unroll
                         for (int k = 0; k < K; ++k) s[r][k] += (double)__ldg(xr + k) * ld;
@@ -368,7 +370,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
         // ---- hist terms: per-lane bins, or per-warp bins grouped by level per 32-row step
         for (int hh = 0; hh < rw.n_hist; ++hh) {
             const int t = rw.hist[hh].term;
-            const int ncol = p.ncol[t];
+            const int ncol = (SIMPLE ? 1 : p.ncol[t]);
             uint32_t hc[R];
             rw_pick_codes<R>(p, t, row0, nr, cdq, hc);
             if (rw.hist_private) {
@@ -376,7 +378,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                 for (int r = 0; r < R; ++r) {
                     if (r >= nr) break;
                     for (int c = 0; c < ncol; ++c) {
-                        const double ld = rw_load(p, t, c, row0 + r);
+                        const double ld = (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r));
                         const int bk = rw.hist[hh].bucket0 + (int)hc[r] * ncol + c;
 #pragma unroll
                         for (int k = 0; k < K; ++k) bins[(bk * K + k) * 32 + lane] += ld * b[r][k];
@@ -390,7 +392,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                 const unsigned grp = __match_any_sync(FULL, key);
                 const int leader = __ffs(grp) - 1;
                 for (int c = 0; c < ncol; ++c) {
-                    const double ld = r < nr ? rw_load(p, t, c, row0 + r) : 0.0;
+                    const double ld = r < nr ? (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r)) : 0.0;
 #pragma unroll
                     for (int k = 0; k < K; ++k) stage[lane * K + k] = ld * b[r][k];
                     __syncwarp();
@@ -420,7 +422,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
             if (j >= rw.n_run) break;
             const RwRun& RR = rw.run[j];
             const int t = RR.term;
-            const int ncol = p.ncol[t];
+            const int ncol = (SIMPLE ? 1 : p.ncol[t]);
             const uint32_t* cdp = p.codes[t];
             uint32_t cd[R];
             rw_pick_codes<R>(p, t, row0, nr, cdq, cd);
@@ -465,7 +467,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                 double val[R][K];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const double ld = r < nr ? rw_load(p, t, c, row0 + r) : 0.0;
+                    const double ld = r < nr ? (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r)) : 0.0;
 #pragma unroll
                     for (int k = 0; k < K; ++k) val[r][k] = ld * b[r][k];
                 }
@@ -562,7 +564,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
         for (int j = 0; j < RW_MAX_RUN; ++j) {
             if (j >= rw.n_run) break;
             const RwRun& RR = rw.run[j];
-            const int ncol = p.ncol[RR.term];
+            const int ncol = (SIMPLE ? 1 : p.ncol[RR.term]);
             const uint32_t* cdp = p.codes[RR.term];
             const bool cont = r1 < p.n && __ldg(cdp + r1) == __ldg(cdp + r1 - 1);
             if (foreign[j] && !cont) continue;
@@ -627,7 +629,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
         const int bk = (i - K) / K, k = (i - K) % K;
         for (int hh = 0; hh < rw.n_hist; ++hh) {
             const int t = rw.hist[hh].term;
-            const int ncol = p.ncol[t];
+            const int ncol = (SIMPLE ? 1 : p.ncol[t]);
             const int b0 = rw.hist[hh].bucket0;
             if (bk >= b0 && bk < b0 + (int)p.L[t] * ncol) {
                 const int lv = (bk - b0) / ncol, c = (bk - b0) % ncol;
@@ -640,7 +642,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
         const RwFix fx = rw.fix[f];
         const RwRun& RR = rw.run[fx.run];
         const int t = RR.term;
-        const int ncol = p.ncol[t];
+        const int ncol = (SIMPLE ? 1 : p.ncol[t]);
         for (int c = 0; c < ncol; ++c)
 #pragma unroll
             for (int k = 0; k < K; ++k) {

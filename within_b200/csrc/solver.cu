@@ -490,6 +490,7 @@ struct within_solver {
         ScatterProb* rest_probs_f = nullptr;
         uint32_t n_rest = 0;
         bool rest_needs_rows = false;        // a full-resolution rest term reads the row vector
+        bool simple = false;                 // every term intercept-only: the specialised sweep
         double* atu = nullptr;               // n_dofs * K raw A^T u (LSMR)
     } rsw[4];
     // per column bucket, the LSMR step's operator path:
@@ -634,6 +635,9 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
     }
     rp.fix = A.upload(fixes);
     rp.n_fix = (uint32_t)fixes.size();
+    rk.simple = true;
+    for (const Term& T : D.terms)
+        if (T.cols.size() != 1 || T.cols[0] >= 0) rk.simple = false;
     rp.part = A.alloc<double>((size_t)rw_grid<K>() * (K + (size_t)rp.n_buckets * K));
     rp.counter = A.alloc<unsigned>(1);
     // per-lane bins when a block's copy stays within 72 KB (3 blocks per SM)
@@ -653,10 +657,16 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
     }
     // dynamic shared memory above the default needs the opt-in (set outside any capture)
     if (rk.smem > 40 * 1024) {
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.smem));
+        const int sm = (int)rk.smem;
+        const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double, false>, attr, sm));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double, false>, attr, sm));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float, false>, attr, sm));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double, false>, attr, sm));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double, true>, attr, sm));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double, true>, attr, sm));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float, true>, attr, sm));
+        CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double, true>, attr, sm));
     }
     rk.ready = true;
     return rk;
@@ -683,8 +693,12 @@ void launch_rowsweep(within_solver& s, within_solver::RowSweepK& rk, const OpPar
                      const T* rhs = nullptr, double* sq_out = nullptr, int sq_stride = 0) {
     RwParams rp = rk.rp;
     rp.atu = atu;
-    k_rowsweep<K, MODE, T><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip, store, rhs,
-                                                                       sq_out, sq_stride);
+    if (rk.simple)
+        k_rowsweep<K, MODE, T, true><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
+                                                                                rhs, sq_out, sq_stride);
+    else
+        k_rowsweep<K, MODE, T, false><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip,
+                                                                                 store, rhs, sq_out, sq_stride);
     ++g_launches;
 }
 
