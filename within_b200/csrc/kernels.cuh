@@ -53,7 +53,8 @@ struct Ctl {
     int err;          // first error code raised on the device
     int bodies_left;  // device-side graph loop: bodies (2 iterations each) still allowed
     int bodies_run;   // device-side graph loop: bodies executed
-    int pad[3];
+    int outer;        // mixed precision: refinement steps taken
+    int pad[2];
 };
 
 // End of one body (two LSMR iterations) of the device-side graph loop: run

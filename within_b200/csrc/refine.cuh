@@ -91,10 +91,12 @@ __global__ void k_cg_start(uint32_t n, const double* __restrict__ g, T* __restri
 }
 
 // p = z, rho0 = <res, z>, and the outer stopping tests at the FP64 residual
+// first < 0: the first refinement step is the one with ctl->outer == 0.  With
+// use_h, the inner loop's conditional node runs only if a column is active.
 template <int K, class T>
 __global__ void __launch_bounds__(RED_THREADS)
 k_cg_init(uint32_t n, const T* __restrict__ res, const T* __restrict__ z, T* __restrict__ p, CgCol* st, Ctl* ctl,
-          int first, double* partials, unsigned* counter) {
+          int first, double* partials, unsigned* counter, int use_h, cudaGraphConditionalHandle h_in) {
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
@@ -108,6 +110,7 @@ k_cg_init(uint32_t n, const T* __restrict__ res, const T* __restrict__ z, T* __r
         }
     double tot[K];
     if (!grid_reduce<K>(acc, partials, counter, tot) || threadIdx.x != 0) return;
+    if (first < 0) first = ctl->outer == 0 ? 1 : 0;
     bool any = false;
     for (int k = 0; k < K; ++k) {
         CgCol c = st[k];
@@ -147,6 +150,17 @@ k_cg_init(uint32_t n, const T* __restrict__ res, const T* __restrict__ z, T* __r
     }
     ctl->all_done = any ? 0 : 1;
     ctl->k5_skip = 0;
+    if (use_h) cudaGraphSetConditional(h_in, any ? 1u : 0u);
+}
+
+// End of one refinement step of the device-driven mixed solve: take another
+// step while a column has not converged (at most 64 steps).
+__global__ void k_outer_cond(const CgCol* st, Ctl* ctl, cudaGraphConditionalHandle h_out) {
+    bool any = false;
+    for (int k = 0; k < 8; ++k) any = any || !st[k].done;
+    const int o = ctl->outer + 1;
+    ctl->outer = o;
+    cudaGraphSetConditional(h_out, (any && !ctl->err && o < 64) ? 1u : 0u);
 }
 
 // alpha = rho / <p, A^T A p>

@@ -473,6 +473,9 @@ struct within_solver {
         Ctl* ctl;
         cudaGraphExec_t loop_graph = nullptr;
         uint64_t body_launches = 0;
+        cudaGraphExec_t solve_graph = nullptr;   // refinement steps and inner loops, all on the device
+        bool solve_graph_failed = false;
+        uint64_t pre_launches = 0, post_launches = 0;
     } mixed[4];
     // pinned staging for the host entry points
     double* pin = nullptr;
@@ -502,8 +505,10 @@ struct within_solver {
             if (w.graph) cudaGraphExecDestroy(w.graph);
             if (w.loop_graph) cudaGraphExecDestroy(w.loop_graph);
         }
-        for (auto& m : mixed)
+        for (auto& m : mixed) {
             if (m.loop_graph) cudaGraphExecDestroy(m.loop_graph);
+            if (m.solve_graph) cudaGraphExecDestroy(m.solve_graph);
+        }
         if (pin) cudaFreeHost(pin);
         if (stream) cudaStreamDestroy(stream);
         if (precond && --precond->refs == 0) delete precond;
@@ -1088,6 +1093,101 @@ void build_cg_loop(within_solver& s, within_solver::Work& w, within_solver::Mixe
     CK(cudaGraphDestroy(g));
 }
 
+// One refinement step's set-up: r = b - A x, ||r||, g = A^T r in FP64, the
+// FP32 copy of g, z = M^-1 g, rho0 and the outer stopping tests (k_cg_init).
+template <int K>
+void mixed_pre(within_solver& s, within_solver::Work& w, within_solver::MixedWork& m, cudaStream_t st, int first,
+               int use_h, cudaGraphConditionalHandle h_in) {
+    const uint32_t nd = (uint32_t)s.n_dofs;
+    if (s.path[kidx(K)] == 2) {   // r = b - A x, ||r||^2 and g = A^T r in one row sweep
+        auto& rk = s.rsw[kidx(K)];
+        launch_rowsweep<K, 3, double>(s, rk, s.op, m.g64, m.x64, m.r64, nullptr, nullptr, nullptr,
+                                      rk.rest_needs_rows ? 1 : 0, st, w.b, &m.st[0].rnorm2,
+                                      (int)(sizeof(CgCol) / sizeof(double)));
+        rowsweep_rest<K, double>(s, rk, m.r64, m.g64, nullptr, st);
+    } else {
+        k_resid64<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, m.x64, w.b, m.r64, m.st, w.partials, w.counter);
+        ++g_launches;
+        scatter<K, 0>(s, m.r64, m.g64, nullptr, nullptr, st);
+    }
+    k_cg_start<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.g64, m.res, m.d);
+    precond_apply<K, float>(s, m.ctl, m.res, m.z, nullptr, st);
+    k_cg_init<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.p, m.st, m.ctl, first, w.partials,
+                                                           w.counter, use_h, h_in);
+    g_launches += 2;
+}
+
+// The whole mixed solve as one graph: a WHILE node over refinement steps
+// whose body is [mixed_pre, a WHILE node over CG iterations, x += d,
+// k_outer_cond].  One launch and one host wait per solve; returns false if
+// the runtime refuses nested conditional nodes (the host then drives the
+// refinement steps).
+template <int K>
+bool build_mixed_graph(within_solver& s, within_solver::Work& w, within_solver::MixedWork& m) {
+    if (m.solve_graph) return true;
+    if (m.solve_graph_failed) return false;
+    const uint32_t nd = (uint32_t)s.n_dofs;
+    auto cond_params = [](cudaGraphConditionalHandle h, unsigned char* raw) -> cudaGraphNodeParams& {
+        cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        return np;
+    };
+    cudaGraph_t g = nullptr;
+    cudaStream_t cs = nullptr;
+    bool ok = false;
+    do {
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
+        cudaGraphConditionalHandle h_out, h_in;
+        if (cudaGraphConditionalHandleCreate(&h_out, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+        alignas(cudaGraphNodeParams) unsigned char raw_out[sizeof(cudaGraphNodeParams)] = {};
+        cudaGraphNodeParams& np_out = cond_params(h_out, raw_out);
+        cudaGraphNode_t n_out;
+        if (cudaGraphAddNode(&n_out, g, nullptr, 0, &np_out) != cudaSuccess) break;
+        cudaGraph_t body = np_out.conditional.phGraph_out[0];
+        if (cudaGraphConditionalHandleCreate(&h_in, body, 0, 0) != cudaSuccess) break;
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) break;
+        const uint64_t l0 = g_launches;
+        CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        mixed_pre<K>(s, w, m, cs, -1, 1, h_in);
+        cudaStreamCaptureStatus cst;
+        cudaGraph_t capg;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capg, &deps, &ndeps));
+        alignas(cudaGraphNodeParams) unsigned char raw_in[sizeof(cudaGraphNodeParams)] = {};
+        cudaGraphNodeParams& np_in = cond_params(h_in, raw_in);
+        cudaGraphNode_t n_in;
+        CK(cudaGraphAddNode(&n_in, capg, deps, ndeps, &np_in));
+        cudaGraph_t inner = np_in.conditional.phGraph_out[0];
+        CK(cudaStreamUpdateCaptureDependencies(cs, &n_in, 1, cudaStreamSetCaptureDependencies));
+        m.pre_launches = g_launches - l0;
+        const uint64_t l1 = g_launches;
+        k_add_delta<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, cs>>>(nd, m.d, m.x64);
+        k_outer_cond<<<1, 1, 0, cs>>>(m.st, m.ctl, h_out);
+        m.post_launches = g_launches - l1 + 2;
+        CK(cudaStreamEndCapture(cs, &body));
+        const uint64_t l2 = g_launches;
+        CK(cudaStreamBeginCaptureToGraph(cs, inner, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        cg_iteration<K>(s, w, m, cs);
+        k_loop_cond<<<1, 1, 0, cs>>>(m.ctl, h_in);
+        m.body_launches = g_launches - l2 + 1;
+        CK(cudaStreamEndCapture(cs, &inner));
+        g_launches = l0;
+        CK(cudaGraphInstantiate(&m.solve_graph, g, 0));
+        ok = true;
+    } while (false);
+    if (cs) cudaStreamDestroy(cs);
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+        cudaGetLastError();
+        m.solve_graph_failed = true;
+    }
+    return ok;
+}
+
 // Mixed-precision solve of K columns: FP64 refinement steps around FP32-storage
 // CG on the normal equations (refine.cuh); same outputs as run_lsmr.
 template <int K>
@@ -1112,23 +1212,17 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
     ++g_launches;
     CgCol fin[8];
     Ctl ctl{};
-    for (int outer = 0;; ++outer) {
-        if (s.path[kidx(K)] == 2) {   // r = b - A x, ||r||^2 and g = A^T r in one row sweep
-            auto& rk = s.rsw[kidx(K)];
-            launch_rowsweep<K, 3, double>(s, rk, s.op, m.g64, m.x64, m.r64, nullptr, nullptr, nullptr,
-                                          rk.rest_needs_rows ? 1 : 0, st, w.b, &m.st[0].rnorm2,
-                                          (int)(sizeof(CgCol) / sizeof(double)));
-            rowsweep_rest<K, double>(s, rk, m.r64, m.g64, nullptr, st);
-            g_launches -= 1;   // counted below with the fixed kernels of the step
-        } else {
-            k_resid64<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, m.x64, w.b, m.r64, m.st, w.partials, w.counter);
-            scatter<K, 0>(s, m.r64, m.g64, nullptr, nullptr, st);
-        }
-        k_cg_start<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.g64, m.res, m.d);
-        precond_apply<K, float>(s, m.ctl, m.res, m.z, nullptr, st);
-        k_cg_init<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.p, m.st, m.ctl, outer == 0 ? 1 : 0,
-                                                               w.partials, w.counter);
-        g_launches += 3;
+    const char* gl = getenv("WITHIN_GRAPH_LOOP");
+    const bool device_driven = !(gl && atoi(gl) == 0) && build_mixed_graph<K>(s, w, m);
+    if (device_driven) {
+        CK(cudaGraphLaunch(m.solve_graph, st));
+        CK(cudaMemcpyAsync(&ctl, m.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        g_launches += (uint64_t)ctl.outer * (m.pre_launches + m.post_launches) +
+                      (uint64_t)ctl.bodies_run * m.body_launches;
+    }
+    for (int outer = 0; !device_driven; ++outer) {
+        mixed_pre<K>(s, w, m, st, outer == 0 ? 1 : 0, 0, cudaGraphConditionalHandle{});
         CK(cudaMemcpyAsync(&ctl, m.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (ctl.all_done || ctl.err) break;
