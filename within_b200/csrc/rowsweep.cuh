@@ -51,7 +51,7 @@ constexpr int RW_MAX_BUCKETS = 64;   // levels x columns over all hist terms
 constexpr int RW_RUN_VALS = 8;       // columns x K of a run term (register carry)
 
 template <int K>
-__host__ __device__ constexpr int rw_rows() { return K >= 4 ? 2 : K == 2 ? 4 : 8; }
+__host__ __device__ constexpr int rw_rows() { return K >= 8 ? 2 : K >= 2 ? 4 : 8; }
 template <int K>
 __host__ __device__ constexpr int rw_chunk() { return 32 * rw_rows<K>(); }
 template <int K>
@@ -86,7 +86,7 @@ struct RwHist {
 struct RwParams {
     uint32_t rows_per_range;     // multiple of the chunk
     int n_run, n_hist, n_buckets;
-    int hist_private;            // bins per lane (bins x K x 32 doubles per warp), else match-grouped
+    int hist_private;            // bins per lane (buckets x K x 32 per warp), else match-grouped
     RwRun run[RW_MAX_RUN];
     RwHist hist[RW_MAX_HIST];
     const RwFix* fix;
@@ -95,6 +95,32 @@ struct RwParams {
     unsigned* counter;
     void* atu;                   // raw A^T u of the run(direct)/hist terms: double, or T in mode 2
 };
+
+// Shared memory of the histogram terms: per-lane bins (bytes of all warps'
+// bins, 16-byte aligned) followed by one FP64 sum per bucket and warp; or
+// per-warp FP64 bins plus a 32 x K staging row per warp.
+template <int BIN_BYTES>
+__host__ __device__ constexpr size_t rw_private_bytes(int nb) {
+    return ((size_t)RW_WARPS * nb * 32 * BIN_BYTES + 15) / 16 * 16;
+}
+constexpr size_t RW_PRIVATE_LIMIT = 100 * 1024;   // 2 blocks per SM
+// dynamic shared memory any launch can ask for: the per-lane limit, or the
+// per-warp bins of RW_MAX_BUCKETS x 8 columns plus staging
+constexpr size_t RW_SMEM_CAP = 104 * 1024;
+static_assert(RW_SMEM_CAP >= RW_PRIVATE_LIMIT && RW_SMEM_CAP >= (size_t)RW_WARPS * (RW_MAX_BUCKETS * 8 + 32 * 8) * 8,
+              "shared-memory ceiling below a reachable request");
+template <int K, int BIN_BYTES>
+inline size_t rw_smem_bytes(int n_buckets, int n_hist, bool& priv) {
+    const int nb = n_buckets * K;
+    priv = false;
+    if (n_hist == 0) return 0;
+    const size_t pb = rw_private_bytes<BIN_BYTES>(nb) + (size_t)RW_WARPS * nb * sizeof(double);
+    if (pb <= RW_PRIVATE_LIMIT) {
+        priv = true;
+        return pb;
+    }
+    return (size_t)RW_WARPS * ((size_t)nb + 32 * K) * sizeof(double);
+}
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -227,10 +253,19 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nb = rw.n_buckets * K;
-    const int bw = rw.hist_private ? nb * 32 : nb;   // bin doubles per warp
-    double* bins = rw_sm + (size_t)wid * bw;
-    double* stage = rw_sm + (size_t)RW_WARPS * bw + (size_t)wid * 32 * K;
-    for (int i = lane; i < bw; i += 32) bins[i] = 0.0;
+    // per-lane bins hold each lane's few rows per bucket in the storage type of
+    // the mode (FP32 in the FP32 normal operator); every later sum is FP64
+    using BinT = std::conditional_t<MODE == 2, T, double>;
+    BinT* pbins = reinterpret_cast<BinT*>(rw_sm) + (size_t)wid * nb * 32;
+    double* wsums = reinterpret_cast<double*>(reinterpret_cast<char*>(rw_sm) +
+                                              rw_private_bytes<sizeof(BinT)>(nb)) + (size_t)wid * nb;
+    double* bins = rw_sm + (size_t)wid * nb;
+    double* stage = rw_sm + (size_t)RW_WARPS * nb + (size_t)wid * 32 * K;
+    if (rw.hist_private) {
+        for (int i = lane; i < nb * 32; i += 32) pbins[i] = (BinT)0;
+    } else {
+        for (int i = lane; i < nb; i += 32) bins[i] = 0.0;
+    }
     __syncwarp();
     TO* atu = reinterpret_cast<TO*>(rw.atu);
 
@@ -381,7 +416,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                         const double ld = (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r));
                         const int bk = rw.hist[hh].bucket0 + (int)hc[r] * ncol + c;
 #pragma unroll
-                        for (int k = 0; k < K; ++k) bins[(bk * K + k) * 32 + lane] += ld * b[r][k];
+                        for (int k = 0; k < K; ++k) pbins[(bk * K + k) * 32 + lane] += (BinT)(ld * b[r][k]);
                     }
                 }
                 continue;
@@ -580,12 +615,12 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
 
     // ---- block partials: ||u||^2 (mode 1) and the bins, in warp order
     const int stride = K + nb;
-    if (rw.hist_private) {   // lanes of each warp in order, into the lane-0 slot
+    if (rw.hist_private) {   // lanes of each warp in order
         __syncwarp();
         for (int i = lane; i < nb; i += 32) {
             double s = 0.0;
-            for (int l = 0; l < 32; ++l) s += bins[i * 32 + l];
-            bins[i * 32] = s;
+            for (int l = 0; l < 32; ++l) s += (double)pbins[i * 32 + l];
+            wsums[i] = s;
         }
     }
     if (NORM) {
@@ -602,11 +637,15 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
         for (int w = 0; w < RW_WARPS; ++w) s += red[w][threadIdx.x];
         mypart[threadIdx.x] = s;
     }
-    for (int i = threadIdx.x; i < nb; i += RW_THREADS) {
-        const size_t slot = rw.hist_private ? (size_t)i * 32 : (size_t)i;
-        double s = 0.0;
-        for (int w = 0; w < RW_WARPS; ++w) s += rw_sm[(size_t)w * bw + slot];
-        mypart[K + i] = s;
+    {
+        const double* base = rw.hist_private
+            ? reinterpret_cast<const double*>(reinterpret_cast<const char*>(rw_sm) + rw_private_bytes<sizeof(BinT)>(nb))
+            : rw_sm;
+        for (int i = threadIdx.x; i < nb; i += RW_THREADS) {
+            double s = 0.0;
+            for (int w = 0; w < RW_WARPS; ++w) s += base[(size_t)w * nb + i];
+            mypart[K + i] = s;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {

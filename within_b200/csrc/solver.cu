@@ -495,6 +495,7 @@ struct within_solver {
         bool rest_needs_rows = false;        // a full-resolution rest term reads the row vector
         bool simple = false;                 // every term intercept-only: the specialised sweep
         double* atu = nullptr;               // n_dofs * K raw A^T u (LSMR)
+        size_t smem_f = 0;                   // shared memory of the FP32 normal-operator mode
     } rsw[4];
     // per column bucket, the LSMR step's operator path:
     // 0 gather + full segmented-reduction scatter, 2 warp-range row sweep (rowsweep.cuh)
@@ -645,11 +646,10 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
         if (T.cols.size() != 1 || T.cols[0] >= 0) rk.simple = false;
     rp.part = A.alloc<double>((size_t)rw_grid<K>() * (K + (size_t)rp.n_buckets * K));
     rp.counter = A.alloc<unsigned>(1);
-    // per-lane bins when a block's copy stays within 72 KB (3 blocks per SM)
-    rp.hist_private = (size_t)RW_WARPS * rp.n_buckets * K * 32 * sizeof(double) <= 72 * 1024 ? 1 : 0;
-    if (rp.n_hist == 0) rk.smem = 0;
-    else if (rp.hist_private) rk.smem = (size_t)RW_WARPS * rp.n_buckets * K * 32 * sizeof(double);
-    else rk.smem = (size_t)RW_WARPS * ((size_t)rp.n_buckets * K + 32 * K) * sizeof(double);
+    // histogram shared memory per bin type (FP64 modes / the FP32 normal operator)
+    bool pv;
+    rk.smem = rw_smem_bytes<K, 8>(rp.n_buckets, rp.n_hist, pv);
+    rk.smem_f = rw_smem_bytes<K, 4>(rp.n_buckets, rp.n_hist, pv);
     rk.atu = A.alloc<double>(s.n_dofs * K);
     rk.n_rest = (uint32_t)rk.rest_host.size();
     if (rk.n_rest) {
@@ -661,17 +661,28 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
         rk.rest_probs = A.upload(rk.rest_host);
     }
     // dynamic shared memory above the default needs the opt-in (set outside any capture)
-    if (rk.smem > 40 * 1024) {
-        const int sm = (int)rk.smem;
-        const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double, false>, attr, sm));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double, false>, attr, sm));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float, false>, attr, sm));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double, false>, attr, sm));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double, true>, attr, sm));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double, true>, attr, sm));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float, true>, attr, sm));
-        CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double, true>, attr, sm));
+    // The dynamic shared-memory ceiling is a property of the kernel function
+    // (shared by every solver in the process), so it is raised once per device
+    // to a bound that covers every design, never to one design's size.
+    {
+        static std::mutex mu;
+        static std::vector<std::pair<int, int>> done;
+        std::lock_guard<std::mutex> g(mu);
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        if (std::find(done.begin(), done.end(), std::make_pair(dev, K)) == done.end()) {
+            const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+            const int cap = (int)RW_SMEM_CAP;
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double, false>, attr, cap));
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double, false>, attr, cap));
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float, false>, attr, cap));
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double, false>, attr, cap));
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 0, double, true>, attr, cap));
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double, true>, attr, cap));
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float, true>, attr, cap));
+            CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double, true>, attr, cap));
+            done.emplace_back(dev, K);
+        }
     }
     rk.ready = true;
     return rk;
@@ -698,12 +709,16 @@ void launch_rowsweep(within_solver& s, within_solver::RowSweepK& rk, const OpPar
                      const T* rhs = nullptr, double* sq_out = nullptr, int sq_stride = 0) {
     RwParams rp = rk.rp;
     rp.atu = atu;
+    constexpr int BIN_BYTES = MODE == 2 ? (int)sizeof(T) : 8;
+    bool priv;
+    const size_t smem = rw_smem_bytes<K, BIN_BYTES>(rp.n_buckets, rp.n_hist, priv);
+    rp.hist_private = priv ? 1 : 0;
     if (rk.simple)
-        k_rowsweep<K, MODE, T, true><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
-                                                                                rhs, sq_out, sq_stride);
+        k_rowsweep<K, MODE, T, true><<<rw_grid<K>(), RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
+                                                                             rhs, sq_out, sq_stride);
     else
-        k_rowsweep<K, MODE, T, false><<<rw_grid<K>(), RW_THREADS, rk.smem, st>>>(op, rp, v, u, cur, ctl, skip,
-                                                                                 store, rhs, sq_out, sq_stride);
+        k_rowsweep<K, MODE, T, false><<<rw_grid<K>(), RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
+                                                                              rhs, sq_out, sq_stride);
     ++g_launches;
 }
 
