@@ -79,6 +79,74 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// K consecutive values of an interleaved vector row as doubles, and back:
+// one 16-byte access per 16 bytes of the row (rows are 16-byte aligned
+// whenever they are 16 bytes or longer).
+template <int K, class T>
+__device__ __forceinline__ void ldk(const T* p, double (&v)[K]) {
+    if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < K / 2; ++i) {
+            const double2 q = reinterpret_cast<const double2*>(p)[i];
+            v[2 * i] = q.x;
+            v[2 * i + 1] = q.y;
+        }
+    } else if constexpr (sizeof(T) == 4 && K % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < K / 4; ++i) {
+            const float4 q = reinterpret_cast<const float4*>(p)[i];
+            v[4 * i] = q.x;
+            v[4 * i + 1] = q.y;
+            v[4 * i + 2] = q.z;
+            v[4 * i + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = (double)p[k];
+    }
+}
+
+// ldk through the read-only path (data no thread of the kernel writes)
+template <int K, class T>
+__device__ __forceinline__ void ldgk(const T* __restrict__ p, double (&v)[K]) {
+    if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < K / 2; ++i) {
+            const double2 q = __ldg(reinterpret_cast<const double2*>(p) + i);
+            v[2 * i] = q.x;
+            v[2 * i + 1] = q.y;
+        }
+    } else if constexpr (sizeof(T) == 4 && K % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < K / 4; ++i) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(p) + i);
+            v[4 * i] = q.x;
+            v[4 * i + 1] = q.y;
+            v[4 * i + 2] = q.z;
+            v[4 * i + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = (double)__ldg(p + k);
+    }
+}
+
+template <int K, class T>
+__device__ __forceinline__ void stk(T* p, const double (&v)[K]) {
+    if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < K / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(v[2 * i], v[2 * i + 1]);
+    } else if constexpr (sizeof(T) == 4 && K % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < K / 4; ++i)
+            reinterpret_cast<float4*>(p)[i] =
+                make_float4((float)v[4 * i], (float)v[4 * i + 1], (float)v[4 * i + 2], (float)v[4 * i + 3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) p[k] = (T)v[k];
+    }
+}
+
 // Column i of a [nblk][stride] table of block partials, summed in one fixed
 // order by a whole warp: lane l adds rows l, l+32, ..., then a fixed shuffle
 // tree; every lane returns the total.
@@ -299,7 +367,10 @@ struct ScatterF {
         }
         if (sqrt_w) f *= (double)__ldg(sqrt_w + i);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = f * (double)u[(size_t)i * K + k];
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        ldk<K, T>(u + (size_t)i * K, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] *= f;
     }
     __device__ void emit(const Prob& pr, uint32_t seg, const double (&s)[K]) const {
         T* o = out + ((size_t)pr.out_off + seg) * K;
@@ -405,11 +476,10 @@ struct RestrictF {
     __device__ void value(const Prob&, uint32_t j, double (&v)[K]) const {
         const uint32_t g = __ldg(S.glob + j);
         const double sc = __ldg(S.scale + j);
+        ldk<K, T>(r + (size_t)g * K, v);
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            v[k] = sc * r[(size_t)g * K + k];
-            S.rl[(size_t)j * K + k] = v[k];
-        }
+        for (int k = 0; k < K; ++k) v[k] *= sc;
+        stk<K, T>(S.rl + (size_t)j * K, v);
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t sub = p.seg_base + seg;
@@ -432,7 +502,10 @@ struct CtF {
         const uint32_t e = __ldg(S.ct_col + a);
         const double f = __ldg(S.ct_val + a);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = f * S.rl[(size_t)e * K + k];
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        ldk<K, T>(S.rl + (size_t)e * K, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] *= f;
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t row = p.seg_base + seg;
@@ -463,7 +536,8 @@ struct KeptSumF {
     __device__ void value(const Prob&, uint32_t q, double (&v)[K]) const {
         const uint32_t u = __ldg(S.ct_row_red + q);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = S.rb[(size_t)u * K + k];
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        ldk<K, T>(S.rb + (size_t)u * K, v);
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t sub = p.seg_base + seg;
@@ -520,7 +594,10 @@ struct FwdF {
         const uint32_t c = __ldg(S.fwd_col + a);
         const double l = __ldg(S.fwd_val + a);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = l * S.yv[(size_t)c * K + k];
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        ldk<K, T>(S.yv + (size_t)c * K, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] *= l;
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t u = S.fwd_row[p.seg_base + seg];
@@ -548,7 +625,10 @@ struct CoreF {
         const uint32_t c = __ldg(S.core_col + a);
         const double g = __ldg(S.core_val + a);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = g * S.yv[(size_t)c * K + k];
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        ldk<K, T>(S.yv + (size_t)c * K, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] *= g;
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t u = S.core_row_slot[p.seg_base + seg];
@@ -568,7 +648,10 @@ struct BwdF {
         const uint32_t c = __ldg(S.bwd_col + a);
         const double l = __ldg(S.bwd_val + a);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = l * S.xv[(size_t)c * K + k];
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        ldk<K, T>(S.xv + (size_t)c * K, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] *= l;
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t v = S.bwd_row[p.seg_base + seg];
@@ -594,7 +677,8 @@ struct CF {
             kept_solution<K, T>(S, cc & 0x7fffffffu, x);
         } else {
 #pragma unroll
-            for (int k = 0; k < K; ++k) x[k] = S.xv[(size_t)cc * K + k];
+            for (int k = 0; k < K; ++k) x[k] = 0.0;
+            ldk<K, T>(S.xv + (size_t)cc * K, x);
         }
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = c * x[k];
@@ -622,7 +706,8 @@ struct MeanF {
         const uint32_t ne = S.n_elim[s];
         if (kk < ne) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) v[k] = S.sl[(size_t)j * K + k];
+            for (int k = 0; k < K; ++k) v[k] = 0.0;
+            ldk<K, T>(S.sl + (size_t)j * K, v);
         } else {
             kept_solution<K, T>(S, S.red_off[s] + (kk - ne), v);
 #pragma unroll

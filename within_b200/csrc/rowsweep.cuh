@@ -347,9 +347,10 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                     for (int r = 0; r < R; ++r) {
                         if (r >= nr) continue;
                         const double ld = (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r));
-                        const T* xr = v + (col + cdq[t][r]) * K;
+                        double xg[K];
+                        ldgk<K, T>(v + (col + cdq[t][r]) * K, xg);
 #pragma unroll
-                        for (int k = 0; k < K; ++k) s[r][k] += (double)__ldg(xr + k) * ld;
+                        for (int k = 0; k < K; ++k) s[r][k] += xg[k] * ld;
                     }
                 }
             }
@@ -362,9 +363,10 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
                     for (int r = 0; r < R; ++r) {
                         if (r >= nr) continue;
                         const double ld = (SIMPLE ? 1.0 : rw_load(p, t, c, row0 + r));
-                        const T* xr = v + (col + cd[r]) * K;
+                        double xg[K];
+                        ldgk<K, T>(v + (col + cd[r]) * K, xg);
 #pragma unroll
-                        for (int k = 0; k < K; ++k) s[r][k] += (double)__ldg(xr + k) * ld;
+                        for (int k = 0; k < K; ++k) s[r][k] += xg[k] * ld;
                     }
                 }
             }
