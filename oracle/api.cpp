@@ -88,7 +88,7 @@ double now() {
 extern "C" {
 
 const char* or_last_error(void) { return g_err.c_str(); }
-void or_set_threads(int) {}
+void or_set_threads(int t) { orc::g_threads = t < 1 ? 1 : t; }
 
 void or_stable_argsort(const uint32_t* key, size_t n_obs, size_t n_levels, uint32_t* perm) {
     stable_argsort(key, n_obs, n_levels, perm);

@@ -108,16 +108,18 @@ void gather_apply(const Design& d, const double* src, double* dst, const double*
     for (size_t q = 0; q < d.terms.size(); ++q) {
         const auto& t = d.terms[q];
         const uint32_t* lv = d.codes[q].data();
-        for (size_t i = 0; i < n; ++i) {
-            size_t lev = lv[i];
-            double acc = -0.0;
-            for (size_t c = 0; c < t.columns.size(); ++c) {
-                double coef = src[t.offset + c * t.n_levels + lev];
-                int k = t.columns[c];
-                acc += (k < 0) ? coef * 1.0 : coef * d.loads[k][i];
+        par_ranges(n, 65536, [&](size_t a, size_t b, int) {
+            for (size_t i = a; i < b; ++i) {
+                size_t lev = lv[i];
+                double acc = -0.0;
+                for (size_t c = 0; c < t.columns.size(); ++c) {
+                    double coef = src[t.offset + c * t.n_levels + lev];
+                    int k = t.columns[c];
+                    acc += (k < 0) ? coef * 1.0 : coef * d.loads[k][i];
+                }
+                dst[i] += acc;
             }
-            dst[i] += acc;
-        }
+        });
     }
     if (scale)
         for (size_t i = 0; i < n; ++i) dst[i] *= scale[i];
@@ -130,6 +132,32 @@ void gather_apply(const Design& d, const double* src, double* dst, const double*
 void scatter_apply(const Design& d, const double* u, const double* sqrt_w, double* dst) {
     const size_t n = d.n_obs;
     for (size_t j = 0; j < d.n_dofs; ++j) dst[j] = 0.0;
+    if (g_threads > 1 && n >= 65536) {   // timing mode: per-thread accumulators summed in thread order
+        const int T = g_threads;
+        std::vector<double> part((size_t)T * d.n_dofs, 0.0);
+        par_ranges(n, 0, [&](size_t a, size_t b, int tid) {
+            double* my = part.data() + (size_t)tid * d.n_dofs;
+            for (size_t i = a; i < b; ++i) {
+                double bv = sqrt_w ? sqrt_w[i] * u[i] : u[i];
+                for (size_t q = 0; q < d.terms.size(); ++q) {
+                    const auto& t = d.terms[q];
+                    const uint32_t lv = d.codes[q][i];
+                    for (size_t c = 0; c < t.columns.size(); ++c) {
+                        int k = t.columns[c];
+                        my[t.offset + c * t.n_levels + lv] += (k < 0) ? bv : d.loads[k][i] * bv;
+                    }
+                }
+            }
+        });
+        par_ranges(d.n_dofs, 0, [&](size_t a, size_t b, int) {
+            for (size_t j = a; j < b; ++j) {
+                double s = 0.0;
+                for (int r = 0; r < T; ++r) s += part[(size_t)r * d.n_dofs + j];
+                dst[j] = s;
+            }
+        });
+        return;
+    }
     for (size_t q = 0; q < d.terms.size(); ++q) {
         const auto& t = d.terms[q];
         const uint32_t* lv = d.codes[q].data();

@@ -42,12 +42,22 @@ double compensated_sum(const double* v, size_t n) {
     return sum + comp;
 }
 
+int g_threads = 1;
+constexpr size_t PAR_MIN = 65536;
+
 static double dot(const double* a, const double* b, size_t n) {
+    if (g_threads > 1) return par_sum(n, PAR_MIN, [&](size_t i) { return a[i] * b[i]; });
     double s = 0;
     for (size_t i = 0; i < n; ++i) s += a[i] * b[i];
     return s;
 }
 static double axpy_with_sq_norm(double* y, const double* x, double scale, size_t n) {
+    if (g_threads > 1)
+        return par_sum(n, PAR_MIN, [&](size_t i) {
+            double v = x[i] + scale * y[i];
+            y[i] = v;
+            return v * v;
+        });
     double s = 0;
     for (size_t i = 0; i < n; ++i) {
         double v = x[i] + scale * y[i];
@@ -57,10 +67,14 @@ static double axpy_with_sq_norm(double* y, const double* x, double scale, size_t
     return s;
 }
 static void axpby(double* y, const double* x, double alpha, double beta, size_t n) {
-    for (size_t i = 0; i < n; ++i) y[i] = alpha * x[i] + beta * y[i];
+    par_ranges(n, PAR_MIN, [&](size_t a, size_t b, int) {
+        for (size_t i = a; i < b; ++i) y[i] = alpha * x[i] + beta * y[i];
+    });
 }
 static void scale_in_place(double* y, double s, size_t n) {
-    for (size_t i = 0; i < n; ++i) y[i] *= s;
+    par_ranges(n, PAR_MIN, [&](size_t a, size_t b, int) {
+        for (size_t i = a; i < b; ++i) y[i] *= s;
+    });
 }
 
 // bidiag.rs:98-111

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstddef>
 #include <string>
+#include <thread>
 #include <vector>
 #include <stdexcept>
 
@@ -82,6 +83,46 @@ struct LsmrResult {
 };
 double vec_norm(const double* v, size_t n);
 double compensated_sum(const double* v, size_t n);
+
+// Host threads of the timing mode (or_set_threads).  1 -- the default, and
+// what every parity test uses -- keeps the reference's single-thread
+// summation order; more threads split the row loops, reductions and SpMVs
+// into contiguous ranges on std::threads (as the reference's Rayon path
+// parallelises them), changing only the order of floating-point sums.
+extern int g_threads;
+
+// f(begin, end, thread) over [0, n) in g_threads contiguous ranges.
+template <class F>
+void par_ranges(size_t n, size_t min_n, F f) {
+    const int T = g_threads;
+    if (T <= 1 || n < min_n) {
+        f((size_t)0, n, 0);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t per = (n + T - 1) / T;
+    for (int t = 1; t < T; ++t) {
+        const size_t a = (size_t)t * per, b = std::min(n, a + per);
+        if (a >= b) break;
+        pool.emplace_back([=, &f] { f(a, b, t); });
+    }
+    f(0, std::min(n, per), 0);
+    for (auto& th : pool) th.join();
+}
+
+// sum over [0, n) of g(i): per-range partials added in range order
+template <class G>
+double par_sum(size_t n, size_t min_n, G g) {
+    std::vector<double> part((size_t)std::max(1, g_threads), 0.0);
+    par_ranges(n, min_n, [&](size_t a, size_t b, int t) {
+        double s = 0.0;
+        for (size_t i = a; i < b; ++i) s += g(i);
+        part[t] = s;
+    });
+    double s = 0.0;
+    for (double v : part) s += v;
+    return s;
+}
 LsmrResult lsmr(const LinOp& a, const double* b, double tol, size_t maxiter, size_t local_size);
 LsmrResult mlsmr(const LinOp& a, const double* b, const LinOp& m, double tol, size_t maxiter,
                  size_t local_size);

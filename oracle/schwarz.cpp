@@ -44,11 +44,13 @@ static Csr transpose(const Csr& a) {  // csr_block.rs:58-90
 
 // y = base + A x (csr_block.rs:174-190, sequential order)
 static void spmv_assign_add(const Csr& a, const double* x, const double* base, double* y) {
-    for (size_t i = 0; i < a.nrows; ++i) {
-        double acc = base[i];
-        for (uint32_t k = a.indptr[i]; k < a.indptr[i + 1]; ++k) acc += a.data[k] * x[a.indices[k]];
-        y[i] = acc;
-    }
+    par_ranges(a.nrows, 8192, [&](size_t lo, size_t hi, int) {
+        for (size_t i = lo; i < hi; ++i) {
+            double acc = base[i];
+            for (uint32_t k = a.indptr[i]; k < a.indptr[i + 1]; ++k) acc += a.data[k] * x[a.indices[k]];
+            y[i] = acc;
+        }
+    });
 }
 
 struct CrossTab {  // cross_tab.rs:100-107
@@ -884,6 +886,27 @@ struct SchwarzPrecond : Preconditioner {
     size_t n_subdomains() const override { return subs.size(); }
     void apply(const double* r, double* z) const override {
         for (size_t i = 0; i < n; ++i) z[i] = 0.0;
+        if (g_threads > 1 && subs.size() > 1) {
+            // timing mode: subdomains concurrently (executor.rs:55-166), each
+            // into its own buffer, added in subdomain order
+            std::vector<std::vector<double>> zs(subs.size());
+            std::vector<std::thread> pool;
+            for (size_t q = 0; q < subs.size(); ++q)
+                pool.emplace_back([&, q] {
+                    const auto& s = subs[q];
+                    const size_t nl = s.globals.size();
+                    std::vector<double> rl(nl, 0.0), sl;
+                    for (size_t i = 0; i < nl; ++i)
+                        rl[i] = s.pw.empty() ? r[s.globals[i]] : r[s.globals[i]] * s.pw[i];
+                    s.solver.solve_local(rl, sl);
+                    zs[q].resize(nl);
+                    for (size_t i = 0; i < nl; ++i) zs[q][i] = s.pw.empty() ? sl[i] : sl[i] * s.pw[i];
+                });
+            for (auto& th : pool) th.join();
+            for (size_t q = 0; q < subs.size(); ++q)
+                for (size_t i = 0; i < subs[q].globals.size(); ++i) z[subs[q].globals[i]] += zs[q][i];
+            return;
+        }
         std::vector<double> rl, sl;
         for (const auto& s : subs) {
             size_t nl = s.globals.size();

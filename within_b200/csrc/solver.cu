@@ -1507,6 +1507,30 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
     return s.release();
 }
 
+// Large host copies (the staging of the host entry points) split over host
+// threads: one thread moves ~5-10 GB/s, and first touches of freshly
+// allocated caller buffers fault page by page, so a single-threaded copy of a
+// 10M-row column costs more than the device solve.
+void par_memcpy(void* dst, const void* src, size_t bytes) {
+    const size_t chunk = (size_t)8 << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned t = (unsigned)std::min<size_t>(std::min<unsigned>(hw, 16u), (bytes + chunk - 1) / chunk);
+    if (t <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t per = (bytes + t - 1) / t;
+    std::vector<std::thread> pool;
+    for (unsigned j = 1; j < t; ++j) {
+        const size_t a = j * per;
+        if (a >= bytes) break;
+        const size_t len = std::min(per, bytes - a);
+        pool.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, len); });
+    }
+    std::memcpy(dst, src, std::min(per, bytes));
+    for (auto& th : pool) th.join();
+}
+
 void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr_options* opts, double* X,
                 double* Dm, within_solve_stats* stats) {
     double tol;
@@ -1525,7 +1549,7 @@ void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr
     double* pY = s.pin;
     double* pD = s.pin + k * n;
     double* pX = s.pin + 2 * k * n;
-    std::memcpy(pY, Y, k * n * sizeof(double));
+    par_memcpy(pY, Y, k * n * sizeof(double));
     double* dY = nullptr;
     double* dX = nullptr;
     double* dD = nullptr;
@@ -1546,9 +1570,9 @@ void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr
     CK(cudaMemcpyAsync(pD, dD, k * n * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     CK(cudaMemcpyAsync(pX, dX, k * nd * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     CK(cudaStreamSynchronize(s.stream));
-    if (Dm) std::memcpy(Dm, pD, k * n * sizeof(double));
+    if (Dm) par_memcpy(Dm, pD, k * n * sizeof(double));
     if (X) {
-        std::memcpy(X, pX, k * nd * sizeof(double));
+        par_memcpy(X, pX, k * nd * sizeof(double));
         if (s.reparam.active())
             for (uint64_t j = 0; j < k; ++j) s.reparam.back_transform(X + j * nd);
     }
