@@ -229,6 +229,9 @@ def mixed_section(W, codes, dev, stream, args):
     # machine does not land on one arm only
     sm = W.Solver(codes, weights=w, device=dev.index, precision="mixed")
     reps = max(2, args.steps // 2)
+    for _ in range(4):   # both arms warm before the rounds
+        s.solve_device(y1, opts)
+        sm.solve_device(Y, opts)
     rounds_p, rounds_m = [], []
     for _ in range(5):
         tp, (_, Dp, stp) = timed(lambda: s.solve_device(y1, opts), reps)
@@ -456,9 +459,13 @@ def run_ours(args):
     bytes_scatter = 4 * Q * n + 8 * n + 8 * nd         # codes/permutation, u, out
     achieved = (bytes_gather + bytes_scatter) / (t_gather + t_scatter) / 1e9
     peak, peak_kind = peaks()
-    roof = {"bound": "hbm", "kernel": "design operator pair (gather D v + segmented-reduction D^T u)",
+    # DRAM bytes per launch of the pair, ncu on the 10M-row panel (dram__bytes_read.sum +
+    # dram__bytes_write.sum of k_apply and of the adjoint row sweep; the small run-combine
+    # launch is not included): profiles/operator_traffic_akm10m.md
+    traffic = (128803072 + 45006848 + 201513472 + 15891200) if n == 10_000_000 else None
+    roof = {"bound": "hbm", "kernel": "design operator pair (gather k_apply D v + row-sweep D^T u and its run combine)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_kind": peak_kind, "traffic": None,
+            "peak_kind": peak_kind, "traffic": traffic,
             "gather_gbs": bytes_gather / t_gather / 1e9, "scatter_gbs": bytes_scatter / t_scatter / 1e9,
             "algorithmic_bytes_per_launch": {"gather": bytes_gather, "scatter": bytes_scatter}}
     line = {

@@ -911,7 +911,14 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
     k_norm_b<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
                                                   w.ctl, w.partials, w.counter);
     k_scale_u<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, w.b, w.u, w.st);
-    scatter<K, 0>(s, w.u, w.p, w.st, nullptr, st);
+    if (s.path[kidx(K)] == 2) {   // p~ = A^T u through the row sweep (adjoint mode) and its rest
+        auto& rk = s.rsw[kidx(K)];
+        CK(cudaMemsetAsync(w.p, 0, (size_t)nd * K * sizeof(double), st));   // levels no row reaches stay 0
+        launch_rowsweep<K, 0, double>(s, rk, s.op, w.p, nullptr, w.u, nullptr, nullptr, nullptr, 0, st);
+        rowsweep_rest<K, double>(s, rk, w.u, w.p, nullptr, st);
+    } else {
+        scatter<K, 0>(s, w.u, w.p, w.st, nullptr, st);
+    }
     precond_apply<K>(s, w.ctl, w.p, w.v, nullptr, st);
     k_alpha_init<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, w.st, w.st + 8, w.ctl, w.partials,
                                                       w.counter);
