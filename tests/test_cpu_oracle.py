@@ -147,3 +147,26 @@ def test_input_validation(oracle):
         s.solve(np.array([1.0, np.nan, 0, 0, 0]))
     with pytest.raises(oracle.OracleError):
         oracle.OracleSolver(np.array([[np.iinfo(np.uint32).max]], np.uint32))
+
+
+def test_threaded_timing_mode_matches_reference_order(oracle):
+    """The restatement's timing mode (all host threads, used only by the
+    bench's CPU baseline and reference arm) solves the same system: demeaned
+    vectors agree with the single-thread reference order to rounding, and the
+    one-thread mode stays bitwise identical run to run."""
+    from within_b200 import workloads as W
+    n = 200_000
+    codes = W.akm_panel(n=n, n_workers=n // 10, n_firms=n // 100, seed=8)
+    y = W.akm_response(n, seed=9)
+    s = oracle.OracleSolver(codes)
+    try:
+        oracle.lib().or_set_threads(1)
+        a = s.solve(y, tol=1e-10, maxiter=2000)
+        b = s.solve(y, tol=1e-10, maxiter=2000)
+        oracle.lib().or_set_threads(4)
+        c = s.solve(y, tol=1e-10, maxiter=2000)
+    finally:
+        oracle.lib().or_set_threads(1)
+    assert np.array_equal(a.demeaned, b.demeaned)
+    assert c.converged
+    assert np.max(np.abs(a.demeaned - c.demeaned)) / np.max(np.abs(y)) < 1e-8
