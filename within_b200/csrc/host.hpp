@@ -81,7 +81,7 @@ struct PrecondCfg {
     bool scaling_error = false;
     // round-parallel factor: when to stop the rounds (host_schwarz.cpp ac_rounds)
     uint32_t core_dense_max = 2048;
-    double core_min_frac = 0.1;
+    double core_min_frac = 0.3;
     uint32_t max_rounds = 64;
 };
 

@@ -51,11 +51,11 @@ constexpr int RW_MAX_BUCKETS = 64;   // levels x columns over all hist terms
 constexpr int RW_RUN_VALS = 8;       // columns x K of a run term (register carry)
 
 template <int K>
-__host__ __device__ constexpr int rw_rows() { return K >= 8 ? 2 : K >= 2 ? 4 : 8; }
+__host__ __device__ constexpr int rw_rows() { return K >= 8 ? 2 : 4; }
 template <int K>
 __host__ __device__ constexpr int rw_chunk() { return 32 * rw_rows<K>(); }
 template <int K>
-__host__ __device__ constexpr int rw_min_blocks() { return 2; }
+__host__ __device__ constexpr int rw_min_blocks() { return K == 1 ? 3 : 2; }
 // fixed grid: 148 SMs x resident blocks per SM
 template <int K>
 __host__ __device__ constexpr int rw_grid() { return 148 * rw_min_blocks<K>(); }
