@@ -451,17 +451,18 @@ template <int K, class T = double>
 __device__ __forceinline__ void kept_solution(const SchwarzDevT<T>& S, uint32_t u, double (&o)[K]) {
     const uint32_t s = S.red_sub[u];
     const int m = S.mode[s];
-    if (m == 0) {
+    ldk<K, T>(S.xv + (size_t)u * K, o);
+    if (m != 0) {
+        double q[K];
+        if (m == 1) {
+            ldk<K, T>(S.xv + (size_t)(S.red_off[s] + S.n_kept[s]) * K, q);
 #pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = S.xv[(size_t)u * K + k];
-    } else if (m == 1) {
-        const size_t g = (size_t)(S.red_off[s] + S.n_kept[s]) * K;
+            for (int k = 0; k < K; ++k) o[k] = o[k] - q[k];
+        } else {
+            ldk<K, T>(S.xv + (size_t)(u + S.n_kept[s]) * K, q);
 #pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = S.xv[(size_t)u * K + k] - S.xv[g + k];
-    } else {
-        const size_t w = (size_t)(u + S.n_kept[s]) * K;
-#pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = 0.5 * (S.xv[(size_t)u * K + k] - S.xv[w + k]);
+            for (int k = 0; k < K; ++k) o[k] = 0.5 * (o[k] - q[k]);
+        }
     }
 }
 
@@ -485,8 +486,10 @@ struct RestrictF {
         const uint32_t sub = p.seg_base + seg;
         const bool fl = S.mode[sub] == 0;
         const double inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
+        double o[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) S.m1[(size_t)sub * K + k] = fl ? s[k] * inv : 0.0;
+        for (int k = 0; k < K; ++k) o[k] = fl ? s[k] * inv : 0.0;
+        stk<K, T>(S.m1 + (size_t)sub * K, o);
     }
 };
 
@@ -515,13 +518,16 @@ struct CtF {
         const bool cover = S.mode[sub] == 2;
         const uint32_t nk = S.n_kept[sub];
         const double rsum = S.ct_rowsum[row];
+        double m[K], rlv[K], val[K], neg[K];
+        ldk<K, T>(S.m1 + (size_t)sub * K, m);
+        ldk<K, T>(S.rl + (size_t)slot * K, rlv);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const double m = S.m1[(size_t)sub * K + k];
-            const double val = (S.rl[(size_t)slot * K + k] - m) + (s[k] - m * rsum);
-            S.rb[(size_t)rbi * K + k] = val;
-            if (cover) S.rb[(size_t)(rbi + nk) * K + k] = -val;
+            val[k] = (rlv[k] - m[k]) + (s[k] - m[k] * rsum);
+            neg[k] = -val[k];
         }
+        stk<K, T>(S.rb + (size_t)rbi * K, val);
+        if (cover) stk<K, T>(S.rb + (size_t)(rbi + nk) * K, neg);
     }
 };
 
@@ -542,23 +548,33 @@ struct KeptSumF {
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t sub = p.seg_base + seg;
         const int m = S.mode[sub];
+        double o[K];
+        if (m == 0) {
+            const double rn = (double)S.red_n[sub];
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            if (m == 0) {
-                S.m2[(size_t)sub * K + k] = s[k] / (double)S.red_n[sub];
-            } else {
-                S.m2[(size_t)sub * K + k] = 0.0;
-                if (m == 1) S.rb[(size_t)(S.red_off[sub] + S.n_kept[sub]) * K + k] = -s[k];
+            for (int k = 0; k < K; ++k) o[k] = s[k] / rn;
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) o[k] = 0.0;
+            if (m == 1) {
+                double neg[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) neg[k] = -s[k];
+                stk<K, T>(S.rb + (size_t)(S.red_off[sub] + S.n_kept[sub]) * K, neg);
             }
         }
+        stk<K, T>(S.m2 + (size_t)sub * K, o);
     }
 };
 
 template <int K, class T = double>
 __device__ __forceinline__ void reduced_rhs(const SchwarzDevT<T>& S, uint32_t u, double (&b)[K]) {
     const uint32_t s = S.red_sub[u];
+    double m[K];
+    ldk<K, T>(S.rb + (size_t)u * K, b);
+    ldk<K, T>(S.m2 + (size_t)s * K, m);
 #pragma unroll
-    for (int k = 0; k < K; ++k) b[k] = S.rb[(size_t)u * K + k] - S.m2[(size_t)s * K + k];
+    for (int k = 0; k < K; ++k) b[k] -= m[k];
 }
 
 // S5 (small systems): x = G b with the dense generalised inverse G
@@ -577,8 +593,7 @@ struct DenseF {
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t u = S.dense_row_slot[p.seg_base + seg];
-#pragma unroll
-        for (int k = 0; k < K; ++k) S.xv[(size_t)u * K + k] = s[k];
+        stk<K, T>(S.xv + (size_t)u * K, s);
     }
 };
 
@@ -604,12 +619,14 @@ struct FwdF {
         double b[K];
         reduced_rhs<K, T>(S, u, b);
         const double di = S.dinv[u];
+        double y[K], x[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const double y = b[k] - s[k];
-            S.yv[(size_t)u * K + k] = y;
-            S.xv[(size_t)u * K + k] = y * di;
+            y[k] = b[k] - s[k];
+            x[k] = y[k] * di;
         }
+        stk<K, T>(S.yv + (size_t)u * K, y);
+        stk<K, T>(S.xv + (size_t)u * K, x);
     }
 };
 
@@ -632,8 +649,7 @@ struct CoreF {
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t u = S.core_row_slot[p.seg_base + seg];
-#pragma unroll
-        for (int k = 0; k < K; ++k) S.xv[(size_t)u * K + k] = s[k];
+        stk<K, T>(S.xv + (size_t)u * K, s);
     }
 };
 
@@ -655,8 +671,11 @@ struct BwdF {
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t v = S.bwd_row[p.seg_base + seg];
+        double x[K];
+        ldk<K, T>(S.xv + (size_t)v * K, x);
 #pragma unroll
-        for (int k = 0; k < K; ++k) S.xv[(size_t)v * K + k] -= s[k];
+        for (int k = 0; k < K; ++k) x[k] -= s[k];
+        stk<K, T>(S.xv + (size_t)v * K, x);
     }
 };
 
@@ -687,9 +706,12 @@ struct CF {
         const uint32_t e = S.elim_slot[p.seg_base + seg];
         const uint32_t sub = S.slot_sub[e];
         const double ie = S.inv_e[e];
+        double rlv[K], m[K], o[K];
+        ldk<K, T>(S.rl + (size_t)e * K, rlv);
+        ldk<K, T>(S.m1 + (size_t)sub * K, m);
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-            S.sl[(size_t)e * K + k] = (S.rl[(size_t)e * K + k] - S.m1[(size_t)sub * K + k]) * ie + s[k];
+        for (int k = 0; k < K; ++k) o[k] = (rlv[k] - m[k]) * ie + s[k];
+        stk<K, T>(S.sl + (size_t)e * K, o);
     }
 };
 
@@ -710,16 +732,17 @@ struct MeanF {
             ldk<K, T>(S.sl + (size_t)j * K, v);
         } else {
             kept_solution<K, T>(S, S.red_off[s] + (kk - ne), v);
-#pragma unroll
-            for (int k = 0; k < K; ++k) S.sl[(size_t)j * K + k] = v[k];
+            stk<K, T>(S.sl + (size_t)j * K, v);
         }
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
         const uint32_t sub = p.seg_base + seg;
         const bool fl = S.mode[sub] == 0;
         const double inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
+        double o[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) S.m3[(size_t)sub * K + k] = fl ? s[k] * inv : 0.0;
+        for (int k = 0; k < K; ++k) o[k] = fl ? s[k] * inv : 0.0;
+        stk<K, T>(S.m3 + (size_t)sub * K, o);
     }
 };
 
@@ -736,13 +759,14 @@ struct ProlongF {
         const uint32_t j = __ldg(S.dof_slot + a);
         const uint32_t s = __ldg(S.slot_sub + j);
         const double sc = __ldg(S.scale + j);
+        double m[K];
+        ldk<K, T>(S.sl + (size_t)j * K, v);
+        ldk<K, T>(S.m3 + (size_t)s * K, m);
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = sc * (S.sl[(size_t)j * K + k] - S.m3[(size_t)s * K + k]);
+        for (int k = 0; k < K; ++k) v[k] = sc * (v[k] - m[k]);
     }
     __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
-        T* o = z + (size_t)(p.seg_base + seg) * K;
-#pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = (T)s[k];
+        stk<K, T>(z + (size_t)(p.seg_base + seg) * K, s);
     }
 };
 

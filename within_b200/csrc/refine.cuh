@@ -30,7 +30,7 @@
 
 namespace wgpu {
 
-constexpr double CG_FLOOR = 1e-5;   // inner solve: stop at this reduction of sqrt(<g, M^-1 g>)
+constexpr double CG_FLOOR = 1e-5;   // default inner floor: stop at this reduction of sqrt(<g, M^-1 g>)
 
 struct CgCol {
     double rho, rho0, alpha, beta, alpha_prev, beta_prev;
@@ -38,6 +38,7 @@ struct CgCol {
     double rnorm2;    // ||r||^2 of the outer residual, tracked through the inner solve
     double bnorm;     // ||b||
     double tol;
+    double floor;     // inner solve stops at this reduction of sqrt(<g, M^-1 g>)
     long long itn, inner, maxiter;
     int active;       // inner CG iterating
     int done;         // converged (or out of iterations)
@@ -241,7 +242,7 @@ k_cg_beta(uint32_t n, const T* __restrict__ res, const T* __restrict__ z, CgCol*
             c.inner += 1;
             const double rn = sqrt(c.rnorm2);
             const double gn = sqrt(rho_new);
-            if (gn <= CG_FLOOR * sqrt(c.rho0) || gn <= c.tol * sqrt(c.anorm2) * rn || rn <= c.tol * c.bnorm ||
+            if (gn <= c.floor * sqrt(c.rho0) || gn <= c.tol * sqrt(c.anorm2) * rn || rn <= c.tol * c.bnorm ||
                 c.itn >= c.maxiter || rho_new == 0.0)
                 c.active = 0;
         } else {
@@ -281,11 +282,12 @@ __global__ void k_add_delta(uint32_t n, const T* __restrict__ d, double* __restr
         for (int k = 0; k < K; ++k) x[(size_t)j * K + k] += (double)d[(size_t)j * K + k];
 }
 
-__global__ void k_cg_setup(CgCol* st, int k_used, double tol, long long maxiter, Ctl* ctl) {
+__global__ void k_cg_setup(CgCol* st, int k_used, double tol, long long maxiter, Ctl* ctl, double floor) {
     for (int k = 0; k < 8; ++k) {
         CgCol c;
         memset(&c, 0, sizeof(c));
         c.tol = tol;
+        c.floor = floor;
         c.maxiter = maxiter;
         c.stop = STOP_NONE;
         if (k >= k_used) {

@@ -1229,8 +1229,10 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
     const double t_solve0 = now_s();
     build_cg_loop<K>(s, w, m);
     CK(cudaMemsetAsync(m.x64, 0, (size_t)nd * K * sizeof(double), st));
+    double floor = CG_FLOOR;
+    if (const char* e = getenv("WITHIN_CG_FLOOR")) floor = atof(e);
     k_cg_setup<<<1, 1, 0, st>>>(m.st, (int)k_used, tol, (long long)std::min<uint64_t>(maxiter, (uint64_t)1 << 40),
-                                m.ctl);
+                                m.ctl, floor);
     ++g_launches;
     CgCol fin[8];
     Ctl ctl{};
