@@ -79,11 +79,12 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// K consecutive values of an interleaved vector row as doubles, and back:
+// K consecutive values of an interleaved vector row into registers of type A
+// (double, or float in the mixed-precision inner solve), and back:
 // one 16-byte access per 16 bytes of the row (rows are 16-byte aligned
 // whenever they are 16 bytes or longer).
-template <int K, class T>
-__device__ __forceinline__ void ldk(const T* p, double (&v)[K]) {
+template <int K, class T, class A>
+__device__ __forceinline__ void ldk(const T* p, A (&v)[K]) {
     if constexpr (sizeof(T) == 8 && K % 2 == 0) {
 #pragma unroll
         for (int i = 0; i < K / 2; ++i) {
@@ -102,13 +103,13 @@ __device__ __forceinline__ void ldk(const T* p, double (&v)[K]) {
         }
     } else {
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = (double)p[k];
+        for (int k = 0; k < K; ++k) v[k] = (A)p[k];
     }
 }
 
 // ldk through the read-only path (data no thread of the kernel writes)
-template <int K, class T>
-__device__ __forceinline__ void ldgk(const T* __restrict__ p, double (&v)[K]) {
+template <int K, class T, class A>
+__device__ __forceinline__ void ldgk(const T* __restrict__ p, A (&v)[K]) {
     if constexpr (sizeof(T) == 8 && K % 2 == 0) {
 #pragma unroll
         for (int i = 0; i < K / 2; ++i) {
@@ -127,12 +128,12 @@ __device__ __forceinline__ void ldgk(const T* __restrict__ p, double (&v)[K]) {
         }
     } else {
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = (double)__ldg(p + k);
+        for (int k = 0; k < K; ++k) v[k] = (A)__ldg(p + k);
     }
 }
 
-template <int K, class T>
-__device__ __forceinline__ void stk(T* p, const double (&v)[K]) {
+template <int K, class T, class A>
+__device__ __forceinline__ void stk(T* p, const A (&v)[K]) {
     if constexpr (sizeof(T) == 8 && K % 2 == 0) {
 #pragma unroll
         for (int i = 0; i < K / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(v[2 * i], v[2 * i + 1]);
@@ -345,6 +346,7 @@ struct ScatterProb {
 template <int K, int EPI, class T = double>
 struct ScatterF {
     using Prob = ScatterProb;
+    using Acc = double;
     const ScatterProb* probs;
     const T* u;
     const T* sqrt_w;
@@ -448,12 +450,12 @@ struct SegProb {          // generic: one pointer array + a segment base
 
 // solution of kept index k (reduced slot u) after the gauge / cover read-back
 template <int K, class T = double>
-__device__ __forceinline__ void kept_solution(const SchwarzDevT<T>& S, uint32_t u, double (&o)[K]) {
+__device__ __forceinline__ void kept_solution(const SchwarzDevT<T>& S, uint32_t u, T (&o)[K]) {
     const uint32_t s = S.red_sub[u];
     const int m = S.mode[s];
     ldk<K, T>(S.xv + (size_t)u * K, o);
     if (m != 0) {
-        double q[K];
+        T q[K];
         if (m == 1) {
             ldk<K, T>(S.xv + (size_t)(S.red_off[s] + S.n_kept[s]) * K, q);
 #pragma unroll
@@ -461,7 +463,7 @@ __device__ __forceinline__ void kept_solution(const SchwarzDevT<T>& S, uint32_t 
         } else {
             ldk<K, T>(S.xv + (size_t)(u + S.n_kept[s]) * K, q);
 #pragma unroll
-            for (int k = 0; k < K; ++k) o[k] = 0.5 * (o[k] - q[k]);
+            for (int k = 0; k < K; ++k) o[k] = (T)0.5 * (o[k] - q[k]);
         }
     }
 }
@@ -470,25 +472,26 @@ __device__ __forceinline__ void kept_solution(const SchwarzDevT<T>& S, uint32_t 
 template <int K, class T = double>
 struct RestrictF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     const T* r;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t j, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t j, T (&v)[K]) const {
         const uint32_t g = __ldg(S.glob + j);
-        const double sc = __ldg(S.scale + j);
+        const T sc = __ldg(S.scale + j);
         ldk<K, T>(r + (size_t)g * K, v);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] *= sc;
         stk<K, T>(S.rl + (size_t)j * K, v);
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t sub = p.seg_base + seg;
         const bool fl = S.mode[sub] == 0;
-        const double inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
-        double o[K];
+        const T inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
+        T o[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = fl ? s[k] * inv : 0.0;
+        for (int k = 0; k < K; ++k) o[k] = fl ? s[k] * inv : (T)0;
         stk<K, T>(S.m1 + (size_t)sub * K, o);
     }
 };
@@ -498,27 +501,28 @@ struct RestrictF {
 template <int K, class T = double>
 struct CtF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t a, T (&v)[K]) const {
         const uint32_t e = __ldg(S.ct_col + a);
-        const double f = __ldg(S.ct_val + a);
+        const T f = __ldg(S.ct_val + a);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = 0.0;
         ldk<K, T>(S.rl + (size_t)e * K, v);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] *= f;
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t row = p.seg_base + seg;
         const uint32_t slot = S.ct_row_slot[row];
         const uint32_t sub = S.slot_sub[slot];
         const uint32_t rbi = S.ct_row_red[row];
         const bool cover = S.mode[sub] == 2;
         const uint32_t nk = S.n_kept[sub];
-        const double rsum = S.ct_rowsum[row];
-        double m[K], rlv[K], val[K], neg[K];
+        const T rsum = S.ct_rowsum[row];
+        T m[K], rlv[K], val[K], neg[K];
         ldk<K, T>(S.m1 + (size_t)sub * K, m);
         ldk<K, T>(S.rl + (size_t)slot * K, rlv);
 #pragma unroll
@@ -536,28 +540,29 @@ struct CtF {
 template <int K, class T = double>
 struct KeptSumF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t q, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t q, T (&v)[K]) const {
         const uint32_t u = __ldg(S.ct_row_red + q);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = 0.0;
         ldk<K, T>(S.rb + (size_t)u * K, v);
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t sub = p.seg_base + seg;
         const int m = S.mode[sub];
-        double o[K];
+        T o[K];
         if (m == 0) {
-            const double rn = (double)S.red_n[sub];
+            const T rn = (double)S.red_n[sub];
 #pragma unroll
             for (int k = 0; k < K; ++k) o[k] = s[k] / rn;
         } else {
 #pragma unroll
             for (int k = 0; k < K; ++k) o[k] = 0.0;
             if (m == 1) {
-                double neg[K];
+                T neg[K];
 #pragma unroll
                 for (int k = 0; k < K; ++k) neg[k] = -s[k];
                 stk<K, T>(S.rb + (size_t)(S.red_off[sub] + S.n_kept[sub]) * K, neg);
@@ -568,9 +573,9 @@ struct KeptSumF {
 };
 
 template <int K, class T = double>
-__device__ __forceinline__ void reduced_rhs(const SchwarzDevT<T>& S, uint32_t u, double (&b)[K]) {
+__device__ __forceinline__ void reduced_rhs(const SchwarzDevT<T>& S, uint32_t u, T (&b)[K]) {
     const uint32_t s = S.red_sub[u];
-    double m[K];
+    T m[K];
     ldk<K, T>(S.rb + (size_t)u * K, b);
     ldk<K, T>(S.m2 + (size_t)s * K, m);
 #pragma unroll
@@ -581,17 +586,18 @@ __device__ __forceinline__ void reduced_rhs(const SchwarzDevT<T>& S, uint32_t u,
 template <int K, class T = double>
 struct DenseF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
-        double b[K];
+    __device__ void value(const Prob&, uint32_t a, T (&v)[K]) const {
+        T b[K];
         reduced_rhs<K, T>(S, __ldg(S.dense_col + a), b);
-        const double g = __ldg(S.dense_val + a);
+        const T g = __ldg(S.dense_val + a);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = g * b[k];
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t u = S.dense_row_slot[p.seg_base + seg];
         stk<K, T>(S.xv + (size_t)u * K, s);
     }
@@ -602,24 +608,25 @@ struct DenseF {
 template <int K, class T = double>
 struct FwdF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t a, T (&v)[K]) const {
         const uint32_t c = __ldg(S.fwd_col + a);
-        const double l = __ldg(S.fwd_val + a);
+        const T l = __ldg(S.fwd_val + a);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = 0.0;
         ldk<K, T>(S.yv + (size_t)c * K, v);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] *= l;
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t u = S.fwd_row[p.seg_base + seg];
-        double b[K];
+        T b[K];
         reduced_rhs<K, T>(S, u, b);
-        const double di = S.dinv[u];
-        double y[K], x[K];
+        const T di = S.dinv[u];
+        T y[K], x[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             y[k] = b[k] - s[k];
@@ -635,19 +642,20 @@ struct FwdF {
 template <int K, class T = double>
 struct CoreF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t a, T (&v)[K]) const {
         const uint32_t c = __ldg(S.core_col + a);
-        const double g = __ldg(S.core_val + a);
+        const T g = __ldg(S.core_val + a);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = 0.0;
         ldk<K, T>(S.yv + (size_t)c * K, v);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] *= g;
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t u = S.core_row_slot[p.seg_base + seg];
         stk<K, T>(S.xv + (size_t)u * K, s);
     }
@@ -657,21 +665,22 @@ struct CoreF {
 template <int K, class T = double>
 struct BwdF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t a, T (&v)[K]) const {
         const uint32_t c = __ldg(S.bwd_col + a);
-        const double l = __ldg(S.bwd_val + a);
+        const T l = __ldg(S.bwd_val + a);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = 0.0;
         ldk<K, T>(S.xv + (size_t)c * K, v);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] *= l;
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t v = S.bwd_row[p.seg_base + seg];
-        double x[K];
+        T x[K];
         ldk<K, T>(S.xv + (size_t)v * K, x);
 #pragma unroll
         for (int k = 0; k < K; ++k) x[k] -= s[k];
@@ -685,13 +694,14 @@ struct BwdF {
 template <int K, class T = double>
 struct CF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t a, T (&v)[K]) const {
         const uint32_t cc = __ldg(S.c_col + a);
-        const double c = __ldg(S.c_val + a);
-        double x[K];
+        const T c = __ldg(S.c_val + a);
+        T x[K];
         if (cc & 0x80000000u) {
             kept_solution<K, T>(S, cc & 0x7fffffffu, x);
         } else {
@@ -702,11 +712,11 @@ struct CF {
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = c * x[k];
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t e = S.elim_slot[p.seg_base + seg];
         const uint32_t sub = S.slot_sub[e];
-        const double ie = S.inv_e[e];
-        double rlv[K], m[K], o[K];
+        const T ie = S.inv_e[e];
+        T rlv[K], m[K], o[K];
         ldk<K, T>(S.rl + (size_t)e * K, rlv);
         ldk<K, T>(S.m1 + (size_t)sub * K, m);
 #pragma unroll
@@ -719,10 +729,11 @@ struct CF {
 template <int K, class T = double>
 struct MeanF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t j, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t j, T (&v)[K]) const {
         const uint32_t s = __ldg(S.slot_sub + j);
         const uint32_t kk = j - S.loc_ptr[s];
         const uint32_t ne = S.n_elim[s];
@@ -735,13 +746,13 @@ struct MeanF {
             stk<K, T>(S.sl + (size_t)j * K, v);
         }
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         const uint32_t sub = p.seg_base + seg;
         const bool fl = S.mode[sub] == 0;
-        const double inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
-        double o[K];
+        const T inv = 1.0 / (double)(S.loc_ptr[sub + 1] - S.loc_ptr[sub]);
+        T o[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) o[k] = fl ? s[k] * inv : 0.0;
+        for (int k = 0; k < K; ++k) o[k] = fl ? s[k] * inv : (T)0;
         stk<K, T>(S.m3 + (size_t)sub * K, o);
     }
 };
@@ -751,21 +762,22 @@ struct MeanF {
 template <int K, class T = double>
 struct ProlongF {
     using Prob = SegProb;
+    using Acc = T;   // sums in the storage type (FP32 in the mixed-precision inner solve)
     const SegProb* probs;
     SchwarzDevT<T> S;
     T* z;
     __device__ const uint32_t* seg_ptr(const Prob& p) const { return p.seg_ptr; }
-    __device__ void value(const Prob&, uint32_t a, double (&v)[K]) const {
+    __device__ void value(const Prob&, uint32_t a, T (&v)[K]) const {
         const uint32_t j = __ldg(S.dof_slot + a);
         const uint32_t s = __ldg(S.slot_sub + j);
-        const double sc = __ldg(S.scale + j);
-        double m[K];
+        const T sc = __ldg(S.scale + j);
+        T m[K];
         ldk<K, T>(S.sl + (size_t)j * K, v);
         ldk<K, T>(S.m3 + (size_t)s * K, m);
 #pragma unroll
         for (int k = 0; k < K; ++k) v[k] = sc * (v[k] - m[k]);
     }
-    __device__ void emit(const Prob& p, uint32_t seg, const double (&s)[K]) const {
+    __device__ void emit(const Prob& p, uint32_t seg, const T (&s)[K]) const {
         stk<K, T>(z + (size_t)(p.seg_base + seg) * K, s);
     }
 };

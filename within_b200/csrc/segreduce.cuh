@@ -33,15 +33,21 @@ constexpr int sr_items() { return K >= 8 ? 2 : 4; }
 template <int K>
 constexpr int sr_tile() { return SR_THREADS * sr_items<K>(); }
 // resident CTAs per SM the register budget is sized for (no spills at K = 8)
-template <int K>
-constexpr int sr_min_blocks() { return K >= 8 ? 2 : (K >= 4 ? 3 : (K >= 2 ? 4 : 6)); }
+// (the register footprint scales with K x the accumulator width)
+template <int K, class A = double>
+constexpr int sr_min_blocks() {
+    constexpr int w = K * (int)sizeof(A) / 8;
+    return w >= 8 ? 2 : (w >= 4 ? 3 : (w >= 2 ? 4 : 6));
+}
 
 // F provides:
 //   using Prob = ...;                 (trivially copyable, <= 256 bytes)
 //   const Prob* probs;                (device array)
 //   __device__ const uint32_t* seg_ptr(const Prob&) const;
-//   __device__ void value(const Prob&, uint32_t pos, double (&v)[K]) const;
-//   __device__ void emit(const Prob&, uint32_t seg, const double (&s)[K]) const;
+//   using Acc = double | float;       (register type of the values and the scan)
+//   __device__ void value(const Prob&, uint32_t pos, Acc (&v)[K]) const;
+//   __device__ void emit(const Prob&, uint32_t seg, const Acc (&s)[K]) const;
+// Split-segment partials cross tiles in double whatever Acc is.
 //
 // The scan carries, for every position, the id of the segment it belongs to
 // (-1: the segment continuing from the previous tile), so the thread holding
@@ -49,7 +55,7 @@ constexpr int sr_min_blocks() { return K >= 8 ? 2 : (K >= 4 ? 3 : (K >= 2 ? 4 : 
 // combine is "a segment start resets the sum", and the id >= 0 of the last
 // start doubles as the reset flag.
 template <class F, int K>
-__global__ void __launch_bounds__(SR_THREADS, sr_min_blocks<K>())
+__global__ void __launch_bounds__(SR_THREADS, sr_min_blocks<K, typename F::Acc>())
 segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
                  const SRSplit* __restrict__ splits, double* __restrict__ head_buf,
                  double* __restrict__ tail_buf, unsigned* __restrict__ counters,
@@ -57,8 +63,9 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     constexpr int ITEMS = sr_items<K>();
     constexpr int T = SR_THREADS * ITEMS;
     using Prob = typename F::Prob;
+    using A = typename F::Acc;
     constexpr int NW = SR_THREADS / 32;
-    __shared__ double wagg[NW][K];
+    __shared__ A wagg[NW][K];
     __shared__ int wsid[NW];
     __shared__ int headseg[T + 1];
     __shared__ double wsum[(SR_THREADS / 32) * K];
@@ -82,16 +89,16 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
         if (b > a) {
             headseg[a - p0] = (int)s;
         } else {
-            double z[K];
+            A z[K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) z[k] = 0.0;
+            for (int k = 0; k < K; ++k) z[k] = (A)0;
             f.emit(prob, s, z);   // empty segment
         }
     }
     __syncthreads();
 
     // values of this thread's positions, all K columns (index loads shared)
-    double val[ITEMS][K];
+    A val[ITEMS][K];
     int sid[ITEMS];
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
@@ -101,7 +108,7 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
             sid[i] = headseg[p];
         } else {
 #pragma unroll
-            for (int k = 0; k < K; ++k) val[i][k] = 0.0;
+            for (int k = 0; k < K; ++k) val[i][k] = (A)0;
             sid[i] = -2;   // past the tile end: never emitted
         }
     }
@@ -109,9 +116,9 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     const unsigned FULL = 0xffffffffu;
     const int lane = tid & 31, wid = tid >> 5;
     int ts = -1;   // id of the thread's last segment start, -1 = none
-    double tv[K];
+    A tv[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) tv[k] = 0.0;
+    for (int k = 0; k < K; ++k) tv[k] = (A)0;
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         if (sid[i] >= 0) {
@@ -126,7 +133,7 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     // (2) the warp (shuffle tree),
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        double up[K];
+        A up[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) up[k] = __shfl_up_sync(FULL, tv[k], d);
         const int us = __shfl_up_sync(FULL, ts, d);
@@ -136,14 +143,14 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
             for (int k = 0; k < K; ++k) tv[k] += up[k];
         }
     }
-    double ex[K];
+    A ex[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) ex[k] = __shfl_up_sync(FULL, tv[k], 1);
     int exs = __shfl_up_sync(FULL, ts, 1);
     if (lane == 0) {
         exs = -1;
 #pragma unroll
-        for (int k = 0; k < K; ++k) ex[k] = 0.0;
+        for (int k = 0; k < K; ++k) ex[k] = (A)0;
     }
     if (lane == 31) {
         wsid[wid] = ts;
@@ -153,9 +160,9 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     __syncthreads();
     // (3) the warps before this one, in warp order
     int cs = -1;
-    double cv[K];
+    A cv[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) cv[k] = 0.0;
+    for (int k = 0; k < K; ++k) cv[k] = (A)0;
     for (int q = 0; q < wid; ++q) {
         if (wsid[q] >= 0) {
             cs = wsid[q];
@@ -168,7 +175,7 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     }
     // carry into this thread, then its items again
     int rs = exs >= 0 ? exs : cs;
-    double run[K];
+    A run[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) run[k] = exs >= 0 ? ex[k] : cv[k] + ex[k];
 #pragma unroll
@@ -195,7 +202,7 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
         const bool last = (P + 1 == p1) || headseg[p + 1] >= 0;
         if (!last) continue;
         const int sg = sid[i];
-        double o[K];
+        A o[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) o[k] = val[i][k];
         if (sg >= 0) {
@@ -203,12 +210,12 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
                 f.emit(prob, (uint32_t)sg, o);
             } else {   // the owned segment that runs past the tile: tail partial
 #pragma unroll
-                for (int k = 0; k < K; ++k) tail_buf[(size_t)tile.tail_split * K + k] = o[k];
+                for (int k = 0; k < K; ++k) tail_buf[(size_t)tile.tail_split * K + k] = (double)o[k];
                 __threadfence();
             }
         } else {       // the segment continuing into this tile: head partial
 #pragma unroll
-            for (int k = 0; k < K; ++k) head_buf[(size_t)gtile * K + k] = o[k];
+            for (int k = 0; k < K; ++k) head_buf[(size_t)gtile * K + k] = (double)o[k];
             __threadfence();
         }
     }
@@ -249,12 +256,12 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
         }
         __syncthreads();
         if (tid == 0) {
-            double tot[K];
+            A tot[K];
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 double v = __ldcg(&tail_buf[(size_t)id * K + k]);
                 for (int w = 0; w < SR_THREADS / 32; ++w) v += wsum[w * K + k];
-                tot[k] = v;
+                tot[k] = (A)v;
             }
             Prob pr = (sp.problem == tile.problem) ? prob : f.probs[sp.problem];
             f.emit(pr, sp.seg, tot);
