@@ -251,6 +251,48 @@ def test_adjoint_sweep_classes_match_oracle(wb, oracle, seed, path, monkeypatch)
         assert rel_inf(b.demeaned[:, k], refk.demeaned, Y[:, k]) < DEMEAN_TOL
 
 
+@pytest.mark.parametrize("weighted", [False, True])
+def test_intercept_sweep_multi_chunk_ranges(wb, oracle, weighted, monkeypatch):
+    """The intercept-only row sweep on a panel long enough for several chunks
+    per warp range (n > 3552 x 128): a worker-sorted term with some workers
+    longer than a range, firm runs along the worker order (run ordinals, runs
+    crossing chunks and ranges: the crossing-run fix-up launch), a 20-level
+    histogram term, an observation count that is not a multiple of 4.  The
+    adjoint against the restatement; solves against the gather + segmented
+    reduction path (WITHIN_SWEEP=0)."""
+    import torch
+    rng = np.random.default_rng(5 + int(weighted))
+    n_w = 60000
+    counts = rng.integers(1, 40, n_w)
+    counts[rng.choice(n_w, 20, replace=False)] = rng.integers(3000, 9000, 20)
+    worker = np.repeat(np.arange(n_w), counts).astype(np.uint32)
+    n = worker.size
+    if n % 4 == 0:
+        worker = worker[:-1]
+        n -= 1
+    change = np.ones(n, bool)
+    change[1:] = (worker[1:] != worker[:-1]) | (rng.random(n - 1) < 0.03)
+    firm = rng.integers(0, 8000, int(change.sum())).astype(np.uint32)[np.cumsum(change) - 1]
+    year = rng.integers(0, 20, n).astype(np.uint32)
+    cats = [worker, firm, year]
+    w = rng.lognormal(0.0, 1.0, n) if weighted else None
+    monkeypatch.delenv("WITHIN_SWEEP", raising=False)
+    s = wb.Solver([wb.Effect(c, True) for c in cats], weights=w)
+    o = oracle.OracleSolver([oracle.Effect(c, True) for c in cats], weights=w, cfg=oracle.precond_cfg("diagonal"))
+    u = rng.standard_normal(n)
+    atu = torch.empty(s.n_dofs, dtype=torch.float64, device="cuda")
+    s.operator_apply_adjoint_device(torch.tensor(u, device="cuda"), atu)
+    np.testing.assert_allclose(atu.cpu().numpy(), o.apply_adjoint(u), rtol=1e-11, atol=1e-9)
+    y = rng.standard_normal(n)
+    opts = wb.LsmrOptions(tol=1e-9, maxiter=5000)
+    r = s.solve(y, opts)
+    monkeypatch.setenv("WITHIN_SWEEP", "0")
+    r0 = wb.Solver([wb.Effect(c, True) for c in cats], weights=w).solve(y, opts)
+    assert r.converged and r0.converged
+    assert abs(r.iterations - r0.iterations) <= 2, (r.iterations, r0.iterations)
+    assert rel_inf(r.demeaned, r0.demeaned, y) < DEMEAN_TOL
+
+
 @pytest.fixture(scope="module")
 def multi_k_case(oracle):
     """A worker-sorted panel with a firm slope and a year term, weights, and 5

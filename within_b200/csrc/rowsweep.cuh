@@ -233,6 +233,122 @@ __device__ __forceinline__ double rw_load(const OpParamsT<T>& p, int t, int c, u
     return li < 0 ? 1.0 : (double)__ldg(p.loads[li] + row);
 }
 
+// Block partials of ||u||^2 (modes 1, 3) and of the histogram bins in warp
+// order, then in the last block to finish: grand totals in block order and
+// the bins into A^T u (the runs that cross range boundaries: k_rw_fix).
+template <int K, int MODE, class T, bool SIMPLE>
+__device__ __forceinline__ void rw_finish(const OpParamsT<T>& p, const RwParams& rw, const double (&accn)[K],
+                                          const bool (&act)[K], ColState* cur, double* sq_out, int sq_stride) {
+    using TO = std::conditional_t<MODE == 2, T, double>;
+    using BinT = std::conditional_t<MODE == 2, T, double>;
+    constexpr bool NORM = MODE == 1 || MODE == 3;
+    extern __shared__ double rw_sm[];
+    __shared__ double red[RW_WARPS][K];
+    __shared__ int is_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nb = rw.n_buckets * K;
+    const BinT* pbins = reinterpret_cast<const BinT*>(rw_sm) + (size_t)wid * nb * 32;
+    double* wsums = reinterpret_cast<double*>(reinterpret_cast<char*>(rw_sm) +
+                                              rw_private_bytes<sizeof(BinT)>(nb)) + (size_t)wid * nb;
+    TO* atu = reinterpret_cast<TO*>(rw.atu);
+    const int stride = K + nb;
+    if (rw.hist_private) {   // lanes of each warp in order
+        __syncwarp();
+        for (int i = lane; i < nb; i += 32) {
+            double s = 0.0;
+            for (int l = 0; l < 32; ++l) s += (double)pbins[i * 32 + l];
+            wsums[i] = s;
+        }
+    }
+    if (NORM) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double s = warp_sum(accn[k]);
+            if (lane == 0) red[wid][k] = s;
+        }
+    }
+    __syncthreads();
+    double* mypart = rw.part + (size_t)blockIdx.x * stride;
+    if (NORM && threadIdx.x < K) {
+        double s = 0.0;
+        for (int w = 0; w < RW_WARPS; ++w) s += red[w][threadIdx.x];
+        mypart[threadIdx.x] = s;
+    }
+    {
+        const double* base = rw.hist_private
+            ? reinterpret_cast<const double*>(reinterpret_cast<const char*>(rw_sm) + rw_private_bytes<sizeof(BinT)>(nb))
+            : rw_sm;
+        for (int i = threadIdx.x; i < nb; i += RW_THREADS) {
+            double s = 0.0;
+            for (int w = 0; w < RW_WARPS; ++w) s += base[(size_t)w * nb + i];
+            mypart[K + i] = s;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        is_last = atomicAdd(rw.counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    // ---- last block: grand totals in block order, bins -> A^T u, crossing runs
+    for (int i = wid; i < stride; i += RW_WARPS) {
+        if (i < K && !NORM) continue;
+        const double a = warp_col_sum(rw.part, gridDim.x, stride, i);
+        if (lane != 0) continue;
+        if (i < K) {
+            if (MODE == 1 && act[i]) cur[i].beta = sqrt(a);
+            if (MODE == 3) sq_out[(size_t)i * sq_stride] = a;
+            continue;
+        }
+        const int bk = (i - K) / K, k = (i - K) % K;
+        for (int hh = 0; hh < rw.n_hist; ++hh) {
+            const int t = rw.hist[hh].term;
+            const int ncol = (SIMPLE ? 1 : p.ncol[t]);
+            const int b0 = rw.hist[hh].bucket0;
+            if (bk >= b0 && bk < b0 + (int)p.L[t] * ncol) {
+                const int lv = (bk - b0) / ncol, c = (bk - b0) % ncol;
+                const size_t dof = (size_t)p.off[t] + (size_t)c * p.L[t] + lv;
+                atu[dof * K + k] = (TO)a;
+            }
+        }
+    }
+    if (threadIdx.x == 0) *rw.counter = 0;
+}
+
+// The runs that cross range boundaries (tail of range g0 + heads of g0+1..g1,
+// in range order), one thread per run, launched after the sweep: thousands
+// of short dependent load chains that would otherwise run one block's worth
+// at a time at the end of the sweep.
+template <int K, int MODE, class T, bool SIMPLE>
+__global__ void __launch_bounds__(256)
+k_rw_fix(OpParamsT<T> p, RwParams rw, const Ctl* ctl, const int* skip) {
+    using TO = std::conditional_t<MODE == 2, T, double>;
+    if (MODE == 1 && ctl->all_done) return;
+    if (MODE != 1 && skip && *skip) return;
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= rw.n_fix) return;
+    TO* atu = reinterpret_cast<TO*>(rw.atu);
+    const RwFix fx = rw.fix[f];
+    const RwRun& RR = rw.run[fx.run];
+    const int t = RR.term;
+    const int ncol = (SIMPLE ? 1 : p.ncol[t]);
+    for (int c = 0; c < ncol; ++c)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double a = __ldcg(&RR.tail[((size_t)fx.g0 * ncol + c) * K + k]);
+            for (uint32_t h = fx.g0 + 1; h <= fx.g1; ++h) a += __ldcg(&RR.head[((size_t)h * ncol + c) * K + k]);
+            if (RR.direct) {
+                const size_t dof = (size_t)p.off[t] + (size_t)c * p.L[t] + fx.id;
+                atu[dof * K + k] = (TO)a;
+            } else {
+                RR.run_sum[((size_t)fx.id * ncol + c) * K + k] = a;
+            }
+        }
+}
+
+
 template <int K, int MODE, class T, bool SIMPLE>
 __global__ void __launch_bounds__(RW_THREADS, rw_min_blocks<K>())
 k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__ u, ColState* cur, Ctl* ctl,
@@ -243,8 +359,6 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     constexpr int CH = 32 * R;
     constexpr int MAXCR = rw_max_cols<K>();
     extern __shared__ double rw_sm[];
-    __shared__ double red[RW_WARPS][K];
-    __shared__ int is_last;
     if (MODE == 1 && ctl->all_done) {
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->k5_skip = 1;
         return;
@@ -615,89 +729,7 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
         }
     }
 
-    // ---- block partials: ||u||^2 (mode 1) and the bins, in warp order
-    const int stride = K + nb;
-    if (rw.hist_private) {   // lanes of each warp in order
-        __syncwarp();
-        for (int i = lane; i < nb; i += 32) {
-            double s = 0.0;
-            for (int l = 0; l < 32; ++l) s += (double)pbins[i * 32 + l];
-            wsums[i] = s;
-        }
-    }
-    if (NORM) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const double s = warp_sum(accn[k]);
-            if (lane == 0) red[wid][k] = s;
-        }
-    }
-    __syncthreads();
-    double* mypart = rw.part + (size_t)blockIdx.x * stride;
-    if (NORM && threadIdx.x < K) {
-        double s = 0.0;
-        for (int w = 0; w < RW_WARPS; ++w) s += red[w][threadIdx.x];
-        mypart[threadIdx.x] = s;
-    }
-    {
-        const double* base = rw.hist_private
-            ? reinterpret_cast<const double*>(reinterpret_cast<const char*>(rw_sm) + rw_private_bytes<sizeof(BinT)>(nb))
-            : rw_sm;
-        for (int i = threadIdx.x; i < nb; i += RW_THREADS) {
-            double s = 0.0;
-            for (int w = 0; w < RW_WARPS; ++w) s += base[(size_t)w * nb + i];
-            mypart[K + i] = s;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        is_last = atomicAdd(rw.counter, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!is_last) return;
-    __threadfence();
-    // ---- last block: grand totals in block order, bins -> A^T u, crossing runs
-    for (int i = wid; i < stride; i += RW_WARPS) {
-        if (i < K && !NORM) continue;
-        const double a = warp_col_sum(rw.part, gridDim.x, stride, i);
-        if (lane != 0) continue;
-        if (i < K) {
-            if (MODE == 1 && act[i]) cur[i].beta = sqrt(a);
-            if (MODE == 3) sq_out[(size_t)i * sq_stride] = a;
-            continue;
-        }
-        const int bk = (i - K) / K, k = (i - K) % K;
-        for (int hh = 0; hh < rw.n_hist; ++hh) {
-            const int t = rw.hist[hh].term;
-            const int ncol = (SIMPLE ? 1 : p.ncol[t]);
-            const int b0 = rw.hist[hh].bucket0;
-            if (bk >= b0 && bk < b0 + (int)p.L[t] * ncol) {
-                const int lv = (bk - b0) / ncol, c = (bk - b0) % ncol;
-                const size_t dof = (size_t)p.off[t] + (size_t)c * p.L[t] + lv;
-                atu[dof * K + k] = (TO)a;
-            }
-        }
-    }
-    for (uint32_t f = threadIdx.x; f < rw.n_fix; f += RW_THREADS) {
-        const RwFix fx = rw.fix[f];
-        const RwRun& RR = rw.run[fx.run];
-        const int t = RR.term;
-        const int ncol = (SIMPLE ? 1 : p.ncol[t]);
-        for (int c = 0; c < ncol; ++c)
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                double a = __ldcg(&RR.tail[((size_t)fx.g0 * ncol + c) * K + k]);
-                for (uint32_t h = fx.g0 + 1; h <= fx.g1; ++h) a += __ldcg(&RR.head[((size_t)h * ncol + c) * K + k]);
-                if (RR.direct) {
-                    const size_t dof = (size_t)p.off[t] + (size_t)c * p.L[t] + fx.id;
-                    atu[dof * K + k] = (TO)a;
-                } else {
-                    RR.run_sum[((size_t)fx.id * ncol + c) * K + k] = a;
-                }
-            }
-    }
-    if (threadIdx.x == 0) *rw.counter = 0;
+    rw_finish<K, MODE, T, SIMPLE>(p, rw, accn, act, cur, sq_out, sq_stride);
 }
 
 // p~ <- A^T u / beta - (beta / alpha) p~ over all DOFs (bidiag.rs:474-485),

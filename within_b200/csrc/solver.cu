@@ -720,6 +720,12 @@ void launch_rowsweep(within_solver& s, within_solver::RowSweepK& rk, const OpPar
         k_rowsweep<K, MODE, T, false><<<rw_grid<K>(), RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
                                                                               rhs, sq_out, sq_stride);
     ++g_launches;
+    if (rp.n_fix) {   // the runs crossing range boundaries, after every range has written its partials
+        const unsigned fb = (rp.n_fix + 255) / 256;
+        if (rk.simple) k_rw_fix<K, MODE, T, true><<<fb, 256, 0, st>>>(op, rp, ctl, skip);
+        else k_rw_fix<K, MODE, T, false><<<fb, 256, 0, st>>>(op, rp, ctl, skip);
+        ++g_launches;
+    }
 }
 
 // the run combines and full-resolution rest terms of A^T u, raw sums into out
