@@ -271,6 +271,43 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     }
 }
 
+// One thread per segment, for a single problem whose segments are all short
+// (at most SEGT_MAX_LEN positions, as the rows of C and the DOFs' slot lists
+// are): each thread sums its segment's positions in order and emits, with no
+// tile barrier, scan or split bookkeeping.  The order is fixed, so results
+// are bitwise reproducible.
+constexpr uint32_t SEGT_MAX_LEN = 32;
+constexpr int SEGT_THREADS = 256;
+
+template <class F, int K>
+__global__ void __launch_bounds__(SEGT_THREADS)
+segthread_kernel(F f, uint32_t n_seg, const int* __restrict__ skip) {
+    using A = typename F::Acc;
+    if (skip && *skip) return;
+    const uint32_t sg = blockIdx.x * SEGT_THREADS + threadIdx.x;
+    if (sg >= n_seg) return;
+    const typename F::Prob pr = f.probs[0];
+    const uint32_t* ptr = f.seg_ptr(pr);
+    const uint32_t a = __ldg(ptr + sg), b = __ldg(ptr + sg + 1);
+    A acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = (A)0;
+    for (uint32_t q = a; q < b; ++q) {
+        A v[K];
+        f.value(pr, q, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += v[k];
+    }
+    f.emit(pr, sg, acc);
+}
+
+// the longest segment of a pointer array (host)
+inline uint32_t seg_max_len(const uint32_t* ptr, size_t n_seg) {
+    uint32_t m = 0;
+    for (size_t i = 0; i < n_seg; ++i) m = ptr[i + 1] - ptr[i] > m ? ptr[i + 1] - ptr[i] : m;
+    return m;
+}
+
 // Host-side plan of one launch (device arrays).
 struct SRPlan {
     int n_tiles = 0;

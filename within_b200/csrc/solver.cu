@@ -105,6 +105,13 @@ DevPlan make_plan(Arena& A, const HostPlan& hp, int K) {
 }
 
 template <class F, int K>
+void launch_segthread(const F& f, uint32_t n_seg, const int* skip, cudaStream_t st) {
+    if (!n_seg) return;
+    segthread_kernel<F, K><<<(n_seg + SEGT_THREADS - 1) / SEGT_THREADS, SEGT_THREADS, 0, st>>>(f, n_seg, skip);
+    ++g_launches;
+}
+
+template <class F, int K>
 void launch_sr(const F& f, const DevPlan& p, uint32_t lo, uint32_t hi, const int* skip, cudaStream_t st) {
     if (hi <= lo) return;
     segreduce_kernel<F, K><<<hi - lo, SR_THREADS, 0, st>>>(f, p.tiles, lo, p.splits, p.head, p.tail,
@@ -291,6 +298,8 @@ void ensure_precond_f(within_preconditioner& P) {
 // plans' partial/counter buffers and the work vectors, per column bucket K.
 struct KPlans {
     DevPlan restrict_, ct, kept, dense, fwd, bwd, c, prolong, core;
+    // C and the prolongation on one thread per segment when every segment is short
+    uint32_t c_thread = 0, prolong_thread = 0;   // segment counts (0: segmented reduction)
     SchwarzWork w;
     SchwarzWorkT<float> wf;   // mixed-precision inner solve, allocated on first use
     bool ready = false;
@@ -327,6 +336,12 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     kp.dense = one(H.dense_rows_ptr);
     kp.c = one(H.c_ptr);
     kp.prolong = one(H.dof_ptr);
+    const char* segt = getenv("WITHIN_SEGTHREAD");
+    const bool segt_on = !(segt && atoi(segt) == 0);
+    if (segt_on && H.c_ptr.size() > 1 && seg_max_len(H.c_ptr.data(), H.c_ptr.size() - 1) <= SEGT_MAX_LEN)
+        kp.c_thread = (uint32_t)(H.c_ptr.size() - 1);
+    if (segt_on && H.dof_ptr.size() > 1 && seg_max_len(H.dof_ptr.data(), H.dof_ptr.size() - 1) <= SEGT_MAX_LEN)
+        kp.prolong_thread = (uint32_t)(H.dof_ptr.size() - 1);
     kp.core = one(H.core_rows_ptr);
     auto rounds = [&](const std::vector<uint32_t>& rptr, const std::vector<uint32_t>& ptr) {
         HostPlan hp;
@@ -414,9 +429,11 @@ void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const T* r, T* z, c
     if (P.has_core) launch_sr<CoF, K>(CoF{P.p_core, S}, kp.core, 0, kp.core.n_tiles, skip, st);
     for (uint32_t r = P.n_rounds; r-- > 0;)
         launch_sr<BF, K>(BF{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
-    launch_sr<CFT, K>(CFT{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
+    if (kp.c_thread) launch_segthread<CFT, K>(CFT{P.p_c, S}, kp.c_thread, skip, st);
+    else launch_sr<CFT, K>(CFT{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
     launch_sr<MF, K>(MF{P.p_restrict, S}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
-    launch_sr<PF, K>(PF{P.p_prolong, S, z}, kp.prolong, 0, kp.prolong.n_tiles, skip, st);
+    if (kp.prolong_thread) launch_segthread<PF, K>(PF{P.p_prolong, S, z}, kp.prolong_thread, skip, st);
+    else launch_sr<PF, K>(PF{P.p_prolong, S, z}, kp.prolong, 0, kp.prolong.n_tiles, skip, st);
 }
 
 }  // namespace
