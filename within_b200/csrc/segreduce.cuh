@@ -271,22 +271,22 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     }
 }
 
-// One thread per segment, for a single problem whose segments are all short
-// (at most SEGT_MAX_LEN positions, as the rows of C and the DOFs' slot lists
-// are): each thread sums its segment's positions in order and emits, with no
-// tile barrier, scan or split bookkeeping.  The order is fixed, so results
-// are bitwise reproducible.
+// One thread per segment, for a problem whose segments are all short (at
+// most SEGT_MAX_LEN positions, as the rows of C, the DOFs' slot lists and the
+// factor rows of most elimination rounds are): each thread sums its
+// segment's positions in order and emits, with no tile barrier, scan or split
+// bookkeeping.  The order is fixed, so results are bitwise reproducible.
 constexpr uint32_t SEGT_MAX_LEN = 32;
 constexpr int SEGT_THREADS = 256;
 
 template <class F, int K>
 __global__ void __launch_bounds__(SEGT_THREADS)
-segthread_kernel(F f, uint32_t n_seg, const int* __restrict__ skip) {
+segthread_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ skip) {
     using A = typename F::Acc;
     if (skip && *skip) return;
     const uint32_t sg = blockIdx.x * SEGT_THREADS + threadIdx.x;
     if (sg >= n_seg) return;
-    const typename F::Prob pr = f.probs[0];
+    const typename F::Prob pr = f.probs[prob];
     const uint32_t* ptr = f.seg_ptr(pr);
     const uint32_t a = __ldg(ptr + sg), b = __ldg(ptr + sg + 1);
     A acc[K];

@@ -105,9 +105,10 @@ DevPlan make_plan(Arena& A, const HostPlan& hp, int K) {
 }
 
 template <class F, int K>
-void launch_segthread(const F& f, uint32_t n_seg, const int* skip, cudaStream_t st) {
+void launch_segthread(const F& f, uint32_t prob, uint32_t n_seg, const int* skip, cudaStream_t st) {
     if (!n_seg) return;
-    segthread_kernel<F, K><<<(n_seg + SEGT_THREADS - 1) / SEGT_THREADS, SEGT_THREADS, 0, st>>>(f, n_seg, skip);
+    segthread_kernel<F, K><<<(n_seg + SEGT_THREADS - 1) / SEGT_THREADS, SEGT_THREADS, 0, st>>>(f, prob, n_seg,
+                                                                                                skip);
     ++g_launches;
 }
 
@@ -298,8 +299,10 @@ void ensure_precond_f(within_preconditioner& P) {
 // plans' partial/counter buffers and the work vectors, per column bucket K.
 struct KPlans {
     DevPlan restrict_, ct, kept, dense, fwd, bwd, c, prolong, core;
-    // C and the prolongation on one thread per segment when every segment is short
-    uint32_t c_thread = 0, prolong_thread = 0;   // segment counts (0: segmented reduction)
+    // C, the prolongation and each elimination round on one thread per segment
+    // when every segment is short: segment counts (0: segmented reduction)
+    uint32_t c_thread = 0, prolong_thread = 0;
+    std::vector<uint32_t> fwd_thread, bwd_thread;
     SchwarzWork w;
     SchwarzWorkT<float> wf;   // mixed-precision inner solve, allocated on first use
     bool ready = false;
@@ -358,6 +361,16 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     };
     kp.fwd = rounds(H.fwd_round_ptr, H.fwd_ptr);
     kp.bwd = rounds(H.bwd_round_ptr, H.bwd_ptr);
+    auto round_thread = [&](const std::vector<uint32_t>& rptr, const std::vector<uint32_t>& ptr) {
+        std::vector<uint32_t> nseg;
+        for (size_t r = 0; r + 1 < rptr.size(); ++r) {
+            const uint32_t m = rptr[r + 1] - rptr[r];
+            nseg.push_back(segt_on && m && seg_max_len(ptr.data() + rptr[r], m) <= SEGT_MAX_LEN ? m : 0u);
+        }
+        return nseg;
+    };
+    kp.fwd_thread = round_thread(H.fwd_round_ptr, H.fwd_ptr);
+    kp.bwd_thread = round_thread(H.bwd_round_ptr, H.bwd_ptr);
     size_t nl = H.glob.size(), nr = H.n_red, ns = H.n_sub;
     kp.w.rl = A.alloc<double>(nl * K);
     kp.w.sl = A.alloc<double>(nl * K);
@@ -424,15 +437,19 @@ void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const T* r, T* z, c
     launch_sr<CtFT, K>(CtFT{P.p_ct, S}, kp.ct, 0, kp.ct.n_tiles, skip, st);
     launch_sr<KS, K>(KS{P.p_kept, S}, kp.kept, 0, kp.kept.n_tiles, skip, st);
     if (P.has_dense) launch_sr<DF, K>(DF{P.p_dense, S}, kp.dense, 0, kp.dense.n_tiles, skip, st);
-    for (uint32_t r = 0; r < P.n_rounds; ++r)
-        launch_sr<FF, K>(FF{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
+    for (uint32_t r = 0; r < P.n_rounds; ++r) {
+        if (kp.fwd_thread[r]) launch_segthread<FF, K>(FF{P.p_fwd, S}, r, kp.fwd_thread[r], skip, st);
+        else launch_sr<FF, K>(FF{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
+    }
     if (P.has_core) launch_sr<CoF, K>(CoF{P.p_core, S}, kp.core, 0, kp.core.n_tiles, skip, st);
-    for (uint32_t r = P.n_rounds; r-- > 0;)
-        launch_sr<BF, K>(BF{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
-    if (kp.c_thread) launch_segthread<CFT, K>(CFT{P.p_c, S}, kp.c_thread, skip, st);
+    for (uint32_t r = P.n_rounds; r-- > 0;) {
+        if (kp.bwd_thread[r]) launch_segthread<BF, K>(BF{P.p_bwd, S}, r, kp.bwd_thread[r], skip, st);
+        else launch_sr<BF, K>(BF{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
+    }
+    if (kp.c_thread) launch_segthread<CFT, K>(CFT{P.p_c, S}, 0, kp.c_thread, skip, st);
     else launch_sr<CFT, K>(CFT{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
     launch_sr<MF, K>(MF{P.p_restrict, S}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
-    if (kp.prolong_thread) launch_segthread<PF, K>(PF{P.p_prolong, S, z}, kp.prolong_thread, skip, st);
+    if (kp.prolong_thread) launch_segthread<PF, K>(PF{P.p_prolong, S, z}, 0, kp.prolong_thread, skip, st);
     else launch_sr<PF, K>(PF{P.p_prolong, S, z}, kp.prolong, 0, kp.prolong.n_tiles, skip, st);
 }
 
