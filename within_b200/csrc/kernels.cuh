@@ -158,32 +158,31 @@ __device__ __forceinline__ double warp_col_sum(const double* part, unsigned nblk
     return warp_sum(a);
 }
 
-// Sum over the block; the result is valid in thread 0.
-__device__ __forceinline__ double block_sum(double v, double* sm /* >= 32 */) {
-    v = warp_sum(v);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) sm[wid] = v;
-    __syncthreads();
-    double t = 0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sm[w];
-    return t;
-}
-
 // Publishes NV block partials and returns true in the (single) last block to
-// finish, in which `tot` holds the grand totals summed in block order.
+// finish, in which `tot` (thread 0) holds the grand totals summed in block
+// order.  All NV values share one barrier round, and the last block loads
+// the partials of every value in one pass, so its loads overlap instead of
+// running NV dependent passes; each value's additions keep the order of a
+// per-value block_sum.
 template <int NV>
 __device__ bool grid_reduce(const double (&v)[NV], double* partials, unsigned* counter,
                             double (&tot)[NV]) {
-    __shared__ double sm[32];
+    __shared__ double sm[NV][32];
     __shared__ int is_last;
-    double b[NV];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) b[i] = block_sum(v[i], sm);
+    for (int i = 0; i < NV; ++i) {
+        const double x = warp_sum(v[i]);
+        if (lane == 0) sm[i][wid] = x;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int i = 0; i < NV; ++i) partials[(size_t)blockIdx.x * NV + i] = b[i];
+        for (int i = 0; i < NV; ++i) {
+            double t = 0;
+            for (int w = 0; w < nw; ++w) t += sm[i][w];
+            partials[(size_t)blockIdx.x * NV + i] = t;
+        }
         __threadfence();
         unsigned prev = atomicAdd(counter, 1u);
         is_last = prev == gridDim.x - 1;
@@ -191,14 +190,27 @@ __device__ bool grid_reduce(const double (&v)[NV], double* partials, unsigned* c
     __syncthreads();
     if (!is_last) return false;
     __threadfence();
+    double a[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) a[i] = 0.0;
+    for (unsigned blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) a[i] += __ldcg(&partials[(size_t)blk * NV + i]);
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
-        double a = 0;
-        for (unsigned blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
-            a += __ldcg(&partials[(size_t)blk * NV + i]);
-        tot[i] = block_sum(a, sm);
+        const double x = warp_sum(a[i]);
+        if (lane == 0) sm[i][wid] = x;
     }
-    if (threadIdx.x == 0) *counter = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            double t = 0;
+            for (int w = 0; w < nw; ++w) t += sm[i][w];
+            tot[i] = t;
+        }
+        *counter = 0;
+    }
     return true;
 }
 
