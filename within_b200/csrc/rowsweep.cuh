@@ -354,7 +354,6 @@ __global__ void __launch_bounds__(RW_THREADS, rw_min_blocks<K>())
 k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__ u, ColState* cur, Ctl* ctl,
            const int* skip, int store, const T* __restrict__ rhs, double* sq_out, int sq_stride) {
     using TO = std::conditional_t<MODE == 2, T, double>;
-    constexpr bool NORM = MODE == 1 || MODE == 3;   // the row values' squared norm per column
     constexpr int R = rw_rows<K>();
     constexpr int CH = 32 * R;
     constexpr int MAXCR = rw_max_cols<K>();
@@ -371,8 +370,6 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
     // the mode (FP32 in the FP32 normal operator); every later sum is FP64
     using BinT = std::conditional_t<MODE == 2, T, double>;
     BinT* pbins = reinterpret_cast<BinT*>(rw_sm) + (size_t)wid * nb * 32;
-    double* wsums = reinterpret_cast<double*>(reinterpret_cast<char*>(rw_sm) +
-                                              rw_private_bytes<sizeof(BinT)>(nb)) + (size_t)wid * nb;
     double* bins = rw_sm + (size_t)wid * nb;
     double* stage = rw_sm + (size_t)RW_WARPS * nb + (size_t)wid * 32 * K;
     if (rw.hist_private) {

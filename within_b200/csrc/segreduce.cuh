@@ -308,16 +308,4 @@ inline uint32_t seg_max_len(const uint32_t* ptr, size_t n_seg) {
     return m;
 }
 
-// Host-side plan of one launch (device arrays).
-struct SRPlan {
-    int n_tiles = 0;
-    int n_splits = 0;
-    SRTile* tiles = nullptr;
-    SRSplit* splits = nullptr;
-    double* head_buf = nullptr;   // n_tiles * K
-    double* tail_buf = nullptr;   // n_splits * K
-    unsigned* counters = nullptr; // n_splits
-    int K = 1;
-};
-
 }  // namespace wgpu
