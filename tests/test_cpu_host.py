@@ -123,3 +123,24 @@ def test_replica_timing_is_max_over_ranks_gloo():
         assert p.exitcode == 0
     assert [r[1] for r in res] == [2.0, 2.0]
     assert [r[2][:2] for r in res] == [(0, 2), (1, 2)]
+
+
+@pytest.mark.parametrize("budget", ["150", "0.001"])
+def test_reference_arm_line(budget):
+    """`bench.py --impl reference` (the oracle on the host's threads) honours
+    --steps/--warmup and prints the reference line, with full-solve steps
+    and, under a tiny time budget, bounded iteration samples."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--rows",
+                          "20000", "--steps", "2", "--warmup", "2", "--ref-budget-s", budget],
+                         cwd=root, capture_output=True, text=True, timeout=600, check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 2
+    assert line["value"] > 0 and line["unit"] == "solves/s" and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert ("per step one full solve" in line["cpu_baseline"]["sample"]) == (budget == "150")
