@@ -55,6 +55,20 @@ def test_tile_planner_properties(tmp_path):
     assert "plan ok" in out
 
 
+def test_schwarz_round_schedule_and_index_ranges(tmp_path):
+    """The round-parallel approximate-Cholesky schedule (no row of a round
+    reads a row of the same round, forward or backward) and the index range of
+    every array the Schwarz apply kernels gather through, on random designs
+    (tests/cpp/schwarz_test.cpp)."""
+    exe = tmp_path / "schwarz_test"
+    csrc = os.path.join(ROOT, "within_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", csrc, "-o", str(exe),
+                    os.path.join(ROOT, "tests", "cpp", "schwarz_test.cpp"),
+                    os.path.join(csrc, "host_schwarz.cpp"), os.path.join(csrc, "host_design.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert "schwarz ok" in out
+
+
 def test_config_lowering(wb):
     from within_b200 import _precond_config
     from within_b200.config import (AdditiveSchwarz, ApproxCholConfig, ApproxSchurConfig,
