@@ -1,6 +1,6 @@
 """GPU parity of the CUDA path against the CPU FP64 restatement (oracle).
 
-Tolerance (north star): demeaned vectors agree within 1e-7 relative to ||y||
+Tolerance: demeaned vectors agree within 1e-7 relative to ||y||
 in the infinity norm at tol 1e-8; the tests solve tighter (1e-10) and hold the
 same bound.  Integer work (grouping permutation, layout) must match exactly.
 """
