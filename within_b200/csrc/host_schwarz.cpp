@@ -20,16 +20,49 @@
 //     computed from the same graph and the triangular solves run one round
 //     per parallel step (level scheduling by construction).
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
+#include <exception>
 #include <numeric>
 #include <cstdio>
 #include <cstdlib>
+#include <thread>
 
 #include "host.hpp"
 
 namespace wgpu {
 namespace {
+
+// f(i) for i in [0, n) on up to the host's hardware threads.  Every f(i)
+// writes only its own outputs, so the result does not depend on the
+// schedule; the exception of the lowest failing index is rethrown, as the
+// sequential loop would have thrown it.
+template <class F>
+void par_for_each(size_t n, F&& f) {
+    const size_t nt = std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency()));
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::vector<std::exception_ptr> err(n);
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t i; (i = next.fetch_add(1)) < n;) {
+            try {
+                f(i);
+            } catch (...) {
+                err[i] = std::current_exception();
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
 
 constexpr uint32_t DENSE_MAX = 64;
 
@@ -734,11 +767,18 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         active[t].assign(d.terms[t].n_levels, 0);
         for (uint32_t v : d.codes[t]) active[t][v] = 1;
     }
-    std::vector<Domain> doms;
+    // channel pairs of different terms, each built on its own host thread
+    // and concatenated in pair order
+    std::vector<std::pair<size_t, size_t>> pairs;
     for (size_t a = 0; a < ch.size(); ++a)
-        for (size_t b = a + 1; b < ch.size(); ++b) {
-            Ch R = ch[a], Cc = ch[b];
-            if (R.term == Cc.term) continue;
+        for (size_t b = a + 1; b < ch.size(); ++b)
+            if (ch[a].term != ch[b].term) pairs.push_back({a, b});
+    std::vector<std::vector<Domain>> pair_doms(pairs.size());
+    std::vector<uint64_t> pair_warnings(pairs.size(), 0);
+    par_for_each(pairs.size(), [&](size_t pi) {
+            std::vector<Domain>& doms = pair_doms[pi];
+            uint64_t& n_warnings = pair_warnings[pi];
+            Ch R = ch[pairs[pi].first], Cc = ch[pairs[pi].second];
             const Term& TR = d.terms[R.term];
             const Term& TC = d.terms[Cc.term];
             std::vector<uint32_t> rmap(TR.n_levels, UINT32_MAX), cmap(TC.n_levels, UINT32_MAX), l2g;
@@ -747,7 +787,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 if (active[R.term][j]) { rmap[j] = nr++; l2g.push_back(TR.offset + R.col * TR.n_levels + j); }
             for (uint32_t k = 0; k < TC.n_levels; ++k)
                 if (active[Cc.term][k]) { cmap[k] = nc++; l2g.push_back(TC.offset + Cc.col * TC.n_levels + k); }
-            if (nr == 0 || nc == 0) continue;
+            if (nr == 0 || nc == 0) return;
             // weighted cross-tab, each cell summed in observation order (accumulate.rs)
             const uint32_t* rl = d.codes[R.term].data();
             const uint32_t* cl = d.codes[Cc.term].data();
@@ -868,13 +908,18 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                                                           " column " + std::to_string(R.col) + " and term " +
                                                           std::to_string(Cc.term) + " column " + std::to_string(Cc.col) +
                                                           " is not diagonally scalable to SDDM form");
-                if (warn) ++out.n_warnings;
+                if (warn) ++n_warnings;
                 Domain dm;
                 dm.globals = std::move(globals);
                 dm.comp = std::move(cp);
                 doms.push_back(std::move(dm));
             }
-        }
+        });
+    std::vector<Domain> doms;
+    for (size_t pi = 0; pi < pairs.size(); ++pi) {
+        for (auto& dm : pair_doms[pi]) doms.push_back(std::move(dm));
+        out.n_warnings += pair_warnings[pi];
+    }
     if (doms.empty()) return out;  // no subdomains: unpreconditioned (operator/schwarz.rs:249-252)
 
     if (!any_slope) {  // compute_partition_weights (factor_pairs.rs:154-194)
@@ -890,8 +935,9 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         }
     }
 
-    // ---- local solvers: reduced systems and their factors ----
-    for (auto& dm : doms) {
+    // ---- local solvers: reduced systems and their factors (one domain per host thread) ----
+    par_for_each(doms.size(), [&](size_t di) {
+        Domain& dm = doms[di];
         dm.inv_e = inv_elim(dm.comp);
         if (dm.comp.laplacian) {
             Lap L = reduced_for(dm.comp, dm.inv_e, cfg);
@@ -904,7 +950,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             factor_lap(L, cfg, dm.fac);
             dm.mode = 2;
         }
-    }
+    });
 
     // ---- pack (layout documented on SchwarzHost) ----
     out.kind = 1;
