@@ -5,14 +5,36 @@
 //    only rows of later rounds (solved earlier on the way back) or rows whose
 //    own backward update is empty (core vertices: rewritten unchanged);
 //  - the index range of every array the apply kernels gather through.
+//  - the host image does not depend on the number of host threads that
+//    built it (WITHIN_HOST_THREADS=1 against the default).
 // Random worker/firm/year-like designs, with the round stop rules relaxed so
 // that several rounds are scheduled.
 #include "host.hpp"
 
 #include <cstdio>
+#include <cstdlib>
 #include <random>
 
 using namespace wgpu;
+
+static uint64_t fnv(uint64_t h, const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+template <class T>
+static uint64_t fnv(uint64_t h, const std::vector<T>& v) {
+    return v.empty() ? fnv(h, "", 0) : fnv(h, v.data(), v.size() * sizeof(T));
+}
+static uint64_t image_hash(const SchwarzHost& S) {
+    uint64_t h = 1469598103934665603ull;
+    h = fnv(h, S.glob); h = fnv(h, S.scale); h = fnv(h, S.inv_e); h = fnv(h, S.mode);
+    h = fnv(h, S.ct_ptr); h = fnv(h, S.ct_col); h = fnv(h, S.ct_val); h = fnv(h, S.c_ptr);
+    h = fnv(h, S.c_col); h = fnv(h, S.c_val); h = fnv(h, S.dense_val); h = fnv(h, S.dinv);
+    h = fnv(h, S.fwd_row); h = fnv(h, S.fwd_col); h = fnv(h, S.fwd_val); h = fnv(h, S.bwd_col);
+    h = fnv(h, S.bwd_val); h = fnv(h, S.core_val); h = fnv(h, S.dof_slot);
+    return h;
+}
 
 static int fail(const char* what, int trial) {
     printf("FAIL %s (trial %d)\n", what, trial);
@@ -48,6 +70,13 @@ int main() {
         BuildResult br = build_preconditioner(d, nullptr, cfg);
         if (br.kind != 1) return fail("additive Schwarz expected", trial);
         const SchwarzHost& S = br.schwarz;
+        if (trial % 6 == 0) {
+            setenv("WITHIN_HOST_THREADS", "1", 1);
+            BuildResult one = build_preconditioner(d, nullptr, cfg);
+            unsetenv("WITHIN_HOST_THREADS");
+            if (image_hash(one.schwarz) != image_hash(S) || one.n_warnings != br.n_warnings)
+                return fail("host image depends on the number of host threads", trial);
+        }
         const uint32_t n_loc = (uint32_t)S.glob.size(), n_red = S.n_red;
         // index ranges
         for (uint32_t g : S.glob)

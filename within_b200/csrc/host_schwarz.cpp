@@ -34,13 +34,15 @@
 namespace wgpu {
 namespace {
 
-// f(i) for i in [0, n) on up to the host's hardware threads.  Every f(i)
-// writes only its own outputs, so the result does not depend on the
-// schedule; the exception of the lowest failing index is rethrown, as the
-// sequential loop would have thrown it.
+// f(i) for i in [0, n) on up to the host's hardware threads (WITHIN_HOST_THREADS
+// caps them).  Every f(i) writes only its own outputs, so the result does not
+// depend on the schedule; the exception of the lowest failing index is
+// rethrown, as the sequential loop would have thrown it.
 template <class F>
 void par_for_each(size_t n, F&& f) {
-    const size_t nt = std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency()));
+    size_t cap = std::max(1u, std::thread::hardware_concurrency());
+    if (const char* e = std::getenv("WITHIN_HOST_THREADS")) cap = std::max(1, std::atoi(e));
+    const size_t nt = std::min<size_t>(n, cap);
     if (nt <= 1) {
         for (size_t i = 0; i < n; ++i) f(i);
         return;
