@@ -959,6 +959,30 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
     SchwarzHost& S = out.schwarz;
     S.n_dofs = (uint32_t)d.n_dofs;
     S.n_sub = (uint32_t)doms.size();
+    {   // exact sizes of the concatenated arrays, so the pack below never reallocates
+        size_t nloc = 0, nel = 0, nkp = 0, nnz_c = 0, nnz_ct = 0;
+        for (const Domain& dm : doms) {
+            nloc += dm.comp.m.nr() + dm.comp.m.nc();
+            nel += dm.comp.m.nr();
+            nkp += dm.comp.m.nc();
+            nnz_c += dm.comp.m.c.col.size();
+            nnz_ct += dm.comp.m.ct.col.size();
+        }
+        S.glob.reserve(nloc);
+        S.scale.reserve(nloc);
+        S.slot_sub.reserve(nloc);
+        S.inv_e.reserve(nloc);
+        S.c_ptr.reserve(nel + 1);
+        S.elim_slot.reserve(nel);
+        S.c_col.reserve(nnz_c);
+        S.c_val.reserve(nnz_c);
+        S.ct_ptr.reserve(nkp + 1);
+        S.ct_rowsum.reserve(nkp);
+        S.ct_row_slot.reserve(nkp);
+        S.ct_row_red.reserve(nkp);
+        S.ct_col.reserve(nnz_ct);
+        S.ct_val.reserve(nnz_ct);
+    }
     S.loc_ptr.push_back(0);
     S.kept_ptr.push_back(0);
     S.ct_ptr.push_back(0);
