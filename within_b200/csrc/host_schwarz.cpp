@@ -34,13 +34,14 @@
 namespace wgpu {
 namespace {
 
-// f(i) for i in [0, n) on up to the host's hardware threads (WITHIN_HOST_THREADS
-// caps them).  Every f(i) writes only its own outputs, so the result does not
-// depend on the schedule; the exception of the lowest failing index is
-// rethrown, as the sequential loop would have thrown it.
+// f(i) for i in [0, n) on up to 16 of the host's hardware threads (a build may
+// itself run on one of many threads building designs side by side;
+// WITHIN_HOST_THREADS sets the cap).  Every f(i) writes only its own outputs,
+// so the result does not depend on the schedule; the exception of the lowest
+// failing index is rethrown, as the sequential loop would have thrown it.
 template <class F>
 void par_for_each(size_t n, F&& f) {
-    size_t cap = std::max(1u, std::thread::hardware_concurrency());
+    size_t cap = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
     if (const char* e = std::getenv("WITHIN_HOST_THREADS")) cap = std::max(1, std::atoi(e));
     const size_t nt = std::min<size_t>(n, cap);
     if (nt <= 1) {
