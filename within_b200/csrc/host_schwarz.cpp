@@ -387,32 +387,56 @@ void sample_star(std::vector<std::pair<uint32_t, double>>& e, uint32_t split, Rn
 }
 
 Lap lap_from_edges(std::vector<Edge>& edges, uint32_t n) {
-    std::sort(edges.begin(), edges.end(), [](const Edge& a, const Edge& b) {
-        if (a.lo != b.lo) return a.lo < b.lo;
-        if (a.hi != b.hi) return a.hi < b.hi;
-        return a.w < b.w;
-    });
+    // (lo, hi, w) order: a stable counting sort by lo, then each lo group
+    // sorted by (hi, w) -- the order of one global sort on (lo, hi, w), so
+    // parallel edges are summed in ascending weight
+    std::vector<uint32_t> start(n + 1, 0);
+    for (const Edge& e : edges) ++start[e.lo + 1];
+    for (uint32_t i = 0; i < n; ++i) start[i + 1] += start[i];
+    std::vector<Edge> srt(edges.size());
+    {
+        std::vector<uint32_t> pos(start.begin(), start.end() - 1);
+        for (const Edge& e : edges) srt[pos[e.lo]++] = e;
+    }
+    for (uint32_t i = 0; i < n; ++i)
+        std::sort(srt.begin() + start[i], srt.begin() + start[i + 1], [](const Edge& a, const Edge& b) {
+            if (a.hi != b.hi) return a.hi < b.hi;
+            return a.w < b.w;
+        });
     std::vector<Edge> dd;
-    for (auto& e : edges) {
+    dd.reserve(srt.size());
+    for (auto& e : srt) {
         if (!dd.empty() && dd.back().lo == e.lo && dd.back().hi == e.hi) dd.back().w += e.w;
         else dd.push_back(e);
     }
-    std::vector<std::vector<std::pair<uint32_t, double>>> rows(n);
+    // rows in one flat array: every edge at both ends, then the diagonal,
+    // each row sorted by (column, value)
+    std::vector<uint32_t> rp(n + 1, 0);
+    for (auto& e : dd) {
+        ++rp[e.lo + 1];
+        ++rp[e.hi + 1];
+    }
+    for (uint32_t i = 0; i < n; ++i) rp[i + 1] += rp[i] + 1;
+    std::vector<std::pair<uint32_t, double>> ent(rp[n]);
+    std::vector<uint32_t> fill(rp.begin(), rp.end() - 1);
     std::vector<double> diag(n, 0.0);
     for (auto& e : dd) {
-        rows[e.lo].push_back({e.hi, -e.w});
-        rows[e.hi].push_back({e.lo, -e.w});
+        ent[fill[e.lo]++] = {e.hi, -e.w};
+        ent[fill[e.hi]++] = {e.lo, -e.w};
         diag[e.lo] += e.w;
         diag[e.hi] += e.w;
     }
     Lap L;
     L.n = n;
+    L.col.reserve(rp[n]);
+    L.val.reserve(rp[n]);
+    L.ptr.reserve((size_t)n + 1);
     for (uint32_t i = 0; i < n; ++i) {
-        rows[i].push_back({i, diag[i]});
-        std::sort(rows[i].begin(), rows[i].end());
-        for (auto& p : rows[i]) {
-            L.col.push_back(p.first);
-            L.val.push_back(p.second);
+        ent[fill[i]] = {i, diag[i]};
+        std::sort(ent.begin() + rp[i], ent.begin() + rp[i + 1]);
+        for (uint32_t q = rp[i]; q < rp[i + 1]; ++q) {
+            L.col.push_back(ent[q].first);
+            L.val.push_back(ent[q].second);
         }
         L.ptr.push_back((uint32_t)L.col.size());
     }
