@@ -984,87 +984,91 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
     SchwarzHost& S = out.schwarz;
     S.n_dofs = (uint32_t)d.n_dofs;
     S.n_sub = (uint32_t)doms.size();
-    {   // exact sizes of the concatenated arrays, so the pack below never reallocates
-        size_t nloc = 0, nel = 0, nkp = 0, nnz_c = 0, nnz_ct = 0;
-        for (const Domain& dm : doms) {
-            nloc += dm.comp.m.nr() + dm.comp.m.nc();
-            nel += dm.comp.m.nr();
-            nkp += dm.comp.m.nc();
-            nnz_c += dm.comp.m.c.col.size();
-            nnz_ct += dm.comp.m.ct.col.size();
-        }
-        S.glob.reserve(nloc);
-        S.scale.reserve(nloc);
-        S.slot_sub.reserve(nloc);
-        S.inv_e.reserve(nloc);
-        S.c_ptr.reserve(nel + 1);
-        S.elim_slot.reserve(nel);
-        S.c_col.reserve(nnz_c);
-        S.c_val.reserve(nnz_c);
-        S.ct_ptr.reserve(nkp + 1);
-        S.ct_rowsum.reserve(nkp);
-        S.ct_row_slot.reserve(nkp);
-        S.ct_row_red.reserve(nkp);
-        S.ct_col.reserve(nnz_ct);
-        S.ct_val.reserve(nnz_ct);
-    }
+    // per-subdomain offsets into the concatenated arrays (a sequential scan),
+    // then every subdomain fills its own ranges on a host thread
+    const uint32_t nsub = S.n_sub;
+    std::vector<uint64_t> o_loc(nsub + 1, 0), o_el(nsub + 1, 0), o_kp(nsub + 1, 0), o_c(nsub + 1, 0),
+        o_ct(nsub + 1, 0), o_red(nsub + 1, 0);
+    uint32_t rounds = 0;
     S.loc_ptr.push_back(0);
     S.kept_ptr.push_back(0);
-    S.ct_ptr.push_back(0);
-    S.c_ptr.push_back(0);
-    uint32_t red = 0, rounds = 0;
-    for (uint32_t s = 0; s < S.n_sub; ++s) {
+    for (uint32_t s = 0; s < nsub; ++s) {
         const Domain& dm = doms[s];
-        const uint32_t ne = dm.comp.m.nr(), nk = dm.comp.m.nc(), nloc = ne + nk;
-        const uint32_t lo = S.loc_ptr.back();
-        S.n_elim.push_back(ne);
-        S.n_kept.push_back(nk);
-        S.red_off.push_back(red);
+        o_loc[s + 1] = o_loc[s] + dm.comp.m.nr() + dm.comp.m.nc();
+        o_el[s + 1] = o_el[s] + dm.comp.m.nr();
+        o_kp[s + 1] = o_kp[s] + dm.comp.m.nc();
+        o_c[s + 1] = o_c[s] + dm.comp.m.c.col.size();
+        o_ct[s + 1] = o_ct[s] + dm.comp.m.ct.col.size();
+        o_red[s + 1] = o_red[s] + dm.fac.n;
+        S.n_elim.push_back(dm.comp.m.nr());
+        S.n_kept.push_back(dm.comp.m.nc());
+        S.red_off.push_back((uint32_t)o_red[s]);
         S.red_n.push_back(dm.fac.n);
         S.mode.push_back(dm.mode);
+        S.loc_ptr.push_back((uint32_t)o_loc[s + 1]);
+        S.kept_ptr.push_back((uint32_t)o_kp[s + 1]);
+        S.cross_nnz += 2ull * dm.comp.m.c.nnz();
+        if (!dm.fac.dense) rounds = std::max(rounds, dm.fac.n_rounds);
+    }
+    const uint32_t red = (uint32_t)o_red[nsub];
+    S.glob.resize(o_loc[nsub]);
+    S.scale.resize(o_loc[nsub]);
+    S.slot_sub.resize(o_loc[nsub]);
+    S.inv_e.resize(o_loc[nsub]);
+    S.ct_ptr.resize(o_kp[nsub] + 1);
+    S.ct_rowsum.resize(o_kp[nsub]);
+    S.ct_row_slot.resize(o_kp[nsub]);
+    S.ct_row_red.resize(o_kp[nsub]);
+    S.ct_col.resize(o_ct[nsub]);
+    S.ct_val.resize(o_ct[nsub]);
+    S.c_ptr.resize(o_el[nsub] + 1);
+    S.elim_slot.resize(o_el[nsub]);
+    S.c_col.resize(o_c[nsub]);
+    S.c_val.resize(o_c[nsub]);
+    S.red_sub.resize(red);
+    par_for_each(nsub, [&](size_t si) {
+        const uint32_t s = (uint32_t)si;
+        const Domain& dm = doms[s];
+        const uint32_t ne = dm.comp.m.nr(), nk = dm.comp.m.nc(), nloc = ne + nk;
+        const uint32_t lo = (uint32_t)o_loc[s], rd = (uint32_t)o_red[s];
         for (uint32_t j = 0; j < nloc; ++j) {
             double f = dm.comp.factors.empty() ? (j < ne ? 1.0 : -1.0) : dm.comp.factors[j];
             double pw = dm.pw.empty() ? 1.0 : dm.pw[j];
-            S.glob.push_back(dm.globals[j]);
-            S.scale.push_back(pw * f);
-            S.slot_sub.push_back(s);
-            S.inv_e.push_back(j < ne ? dm.inv_e[j] : 0.0);
+            S.glob[lo + j] = dm.globals[j];
+            S.scale[lo + j] = pw * f;
+            S.slot_sub[lo + j] = s;
+            S.inv_e[lo + j] = j < ne ? dm.inv_e[j] : 0.0;
         }
-        S.loc_ptr.push_back(lo + nloc);
         // C^T rows (kept), columns = local slots of eliminated entries, values
         // pre-divided by D_e (solver.rs:360-371 scales rhs_e by 1/D_e first)
+        const Csr& ct = dm.comp.m.ct;
         for (uint32_t k = 0; k < nk; ++k) {
-            const Csr& ct = dm.comp.m.ct;
             double rs = 0.0;
             for (uint32_t a = ct.ptr[k]; a < ct.ptr[k + 1]; ++a) {
                 const double v = ct.val[a] * dm.inv_e[ct.col[a]];
-                S.ct_col.push_back(lo + ct.col[a]);
-                S.ct_val.push_back(v);
+                S.ct_col[o_ct[s] + a] = lo + ct.col[a];
+                S.ct_val[o_ct[s] + a] = v;
                 rs += v;
             }
-            S.ct_ptr.push_back((uint32_t)S.ct_col.size());
-            S.ct_rowsum.push_back(rs);
-            S.ct_row_slot.push_back(lo + ne + k);
-            S.ct_row_red.push_back(red + k);
+            S.ct_ptr[o_kp[s] + k + 1] = (uint32_t)(o_ct[s] + ct.ptr[k + 1]);
+            S.ct_rowsum[o_kp[s] + k] = rs;
+            S.ct_row_slot[o_kp[s] + k] = lo + ne + k;
+            S.ct_row_red[o_kp[s] + k] = rd + k;
         }
-        S.kept_ptr.push_back(S.kept_ptr.back() + nk);
         // C rows (eliminated), columns = reduced slot of the kept entry (bit 31:
         // gauge/cover read-back needed), values pre-divided by D_e (solver.rs:41-77)
         const uint32_t flag = dm.mode == 0 ? 0u : 0x80000000u;
+        const Csr& c = dm.comp.m.c;
         for (uint32_t e = 0; e < ne; ++e) {
-            const Csr& c = dm.comp.m.c;
             for (uint32_t a = c.ptr[e]; a < c.ptr[e + 1]; ++a) {
-                S.c_col.push_back((red + c.col[a]) | flag);
-                S.c_val.push_back(c.val[a] * dm.inv_e[e]);
+                S.c_col[o_c[s] + a] = (rd + c.col[a]) | flag;
+                S.c_val[o_c[s] + a] = c.val[a] * dm.inv_e[e];
             }
-            S.c_ptr.push_back((uint32_t)S.c_col.size());
-            S.elim_slot.push_back(lo + e);
+            S.c_ptr[o_el[s] + e + 1] = (uint32_t)(o_c[s] + c.ptr[e + 1]);
+            S.elim_slot[o_el[s] + e] = lo + e;
         }
-        S.cross_nnz += 2ull * dm.comp.m.c.nnz();
-        for (uint32_t i = 0; i < dm.fac.n; ++i) S.red_sub.push_back(s);
-        red += dm.fac.n;
-        if (!dm.fac.dense) rounds = std::max(rounds, dm.fac.n_rounds);
-    }
+        for (uint32_t i = 0; i < dm.fac.n; ++i) S.red_sub[rd + i] = s;
+    });
     S.n_red = red;
     S.dinv.assign(red, 0.0);
     // dense blocks
