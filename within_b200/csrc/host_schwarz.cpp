@@ -887,7 +887,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 Comp cp;
                 std::vector<double> diag;
                 if (ncomp == 1) {
-                    cp.m = full;
+                    cp.m = std::move(full);   // the only component: full is not read again
                     diag = rdiag;
                     diag.insert(diag.end(), cdiag.begin(), cdiag.end());
                 } else {
