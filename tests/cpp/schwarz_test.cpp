@@ -7,8 +7,10 @@
 //  - the index range of every array the apply kernels gather through.
 //  - the host image does not depend on the number of host threads that
 //    built it (WITHIN_HOST_THREADS=1 against the default).
-// Random worker/firm/year-like designs, with the round stop rules relaxed so
-// that several rounds are scheduled.
+// Random worker/firm/year-like designs (every fourth with a slope on the second
+// factor and observation weights, which takes the signed / cover routes of the
+// set-up), with the round stop rules relaxed so that several rounds are
+// scheduled.
 #include "host.hpp"
 
 #include <cstdio>
@@ -43,12 +45,13 @@ static int fail(const char* what, int trial) {
 
 int main() {
     std::mt19937_64 rng(11);
-    uint64_t rounds_seen = 0, rows_checked = 0;
+    uint64_t rounds_seen = 0, rows_checked = 0, not_laplacian = 0;
     for (int trial = 0; trial < 24; ++trial) {
         const uint32_t n = 4000 + (uint32_t)(rng() % 20000);
         const uint32_t L0 = 300 + (uint32_t)(rng() % 2000), L1 = 80 + (uint32_t)(rng() % 400),
                        L2 = 3 + (uint32_t)(rng() % 30);
         std::vector<uint32_t> a(n), b(n), c(n);
+        std::vector<double> z(n), w(n);
         // clustered first factor (panel-like runs), random others
         uint32_t cur = 0;
         for (uint32_t i = 0; i < n; ++i) {
@@ -57,22 +60,28 @@ int main() {
             a[i] = cur;
             b[i] = i < L1 ? i : (uint32_t)(rng() % L1);
             c[i] = i < L2 ? i : (uint32_t)(rng() % L2);
+            z[i] = (double)(rng() % 2001) / 1000.0 - 1.0;
+            w[i] = 0.25 + (double)(rng() % 1000) / 500.0;
         }
+        const bool slopes = trial % 4 == 3;
         std::vector<EffectIn> eff;
         eff.push_back(EffectIn{a.data(), true, {}});
-        eff.push_back(EffectIn{b.data(), true, {}});
+        if (slopes) eff.push_back(EffectIn{b.data(), true, {z.data()}});
+        else eff.push_back(EffectIn{b.data(), true, {}});
         if (trial % 3 != 2) eff.push_back(EffectIn{c.data(), true, {}});
         HostDesign d = make_design(n, eff);
+        const double* wp = slopes ? w.data() : nullptr;
+        if (slopes) build_reparam(d, wp);   // loadings whitened in place, as the solver does
         PrecondCfg cfg;
         cfg.core_dense_max = (trial % 2) ? 8 : 64;
         cfg.core_min_frac = (trial % 4 < 2) ? 0.0 : 0.3;
         cfg.max_rounds = 64;
-        BuildResult br = build_preconditioner(d, nullptr, cfg);
+        BuildResult br = build_preconditioner(d, wp, cfg);
         if (br.kind != 1) return fail("additive Schwarz expected", trial);
         const SchwarzHost& S = br.schwarz;
         if (trial % 6 == 0) {
             setenv("WITHIN_HOST_THREADS", "1", 1);
-            BuildResult one = build_preconditioner(d, nullptr, cfg);
+            BuildResult one = build_preconditioner(d, wp, cfg);
             unsetenv("WITHIN_HOST_THREADS");
             if (image_hash(one.schwarz) != image_hash(S) || one.n_warnings != br.n_warnings)
                 return fail("host image depends on the number of host threads", trial);
@@ -126,12 +135,17 @@ int main() {
             }
         }
         rounds_seen += S.n_rounds;
+        for (int32_t m : S.mode) not_laplacian += m != 0;
+    }
+    if (not_laplacian == 0) {
+        printf("FAIL no grounded or cover subdomain was built\n");
+        return 1;
     }
     if (rounds_seen == 0) {
         printf("FAIL no round-scheduled factor was built\n");
         return 1;
     }
-    printf("schwarz ok: %llu rounds, %llu forward rows checked\n", (unsigned long long)rounds_seen,
-           (unsigned long long)rows_checked);
+    printf("schwarz ok: %llu rounds, %llu forward rows checked, %llu grounded or cover subdomains\n",
+           (unsigned long long)rounds_seen, (unsigned long long)rows_checked, (unsigned long long)not_laplacian);
     return 0;
 }
