@@ -19,8 +19,8 @@
 //               ordinal) that a segmented reduction over the level-sorted runs
 //               combines afterwards.  A run that crosses a range boundary
 //               leaves a tail partial (range where it starts) and head
-//               partials (ranges it continues into); the last block adds them
-//               in range order.
+//               partials (ranges it continues into); k_rw_fix, launched after
+//               the sweep, adds them in range order.
 //   hist terms  few coefficients (levels x columns <= 64): bins in shared
 //               memory -- per lane when they fit (each lane adds its rows in
 //               order), else per warp with each 32-row step grouped by level
@@ -292,7 +292,7 @@ __device__ __forceinline__ void rw_finish(const OpParamsT<T>& p, const RwParams&
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    // ---- last block: grand totals in block order, bins -> A^T u, crossing runs
+    // ---- last block: grand totals in block order, bins -> A^T u
     for (int i = wid; i < stride; i += RW_WARPS) {
         if (i < K && !NORM) continue;
         const double a = warp_col_sum(rw.part, gridDim.x, stride, i);
