@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-many", action="store_true", help="skip the many-designs section")
     ap.add_argument("--many", type=int, default=256, help="designs in the many-designs section")
     ap.add_argument("--no-autograd", action="store_true", help="skip the differentiable-demeaning section")
+    ap.add_argument("--no-published", action="store_true",
+                    help="skip the reference's published 1M-row wall-clock configuration")
     ap.add_argument("--kernel-timeline", choices=["fp64", "mixed"], default=None,
                     help="instead of the bench line: per-kernel device times of one solve (torch.profiler "
                          "/ CUPTI timestamps); 'mixed' = weighted panel, k = 4, mixed precision")
@@ -132,6 +134,41 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def demeaned_err(D, Dref, Y):
+    """max|D - Dref| per column, scaled by max|y| ("inf_over_inf") and by
+    ||y||_2 ("inf_over_l2", the scaling the 1e-7 contract is stated in); the
+    worst column of each."""
+    D = D.reshape(D.shape[0], -1)
+    Dref = Dref.reshape(Dref.shape[0], -1)
+    Y = Y.reshape(Y.shape[0], -1)
+    d = (D - Dref).abs().max(dim=0).values
+    return {"inf_over_inf": float((d / Y.abs().max(dim=0).values).max()),
+            "inf_over_l2": float((d / Y.norm(dim=0)).max())}
+
+
+def iteration_bytes(n, nd, Q, k=1, s=8, weighted=False, n_slopes=0, ps=None):
+    """Algorithmic bytes of one LSMR iteration of k columns (value size s):
+    - op_survey: the design-operator pair as a gather pass plus a scatter pass,
+      2 (4 n Q + s n S + s n [w]) + s n (1 + 2k) + s n_dofs 2k;
+    - op_fused: the same with the codes, loadings and sqrt(w) read once (the
+      fused row sweep): 4 n Q + s n S + s n [w] + 2 s n k + 2 s n_dofs k;
+    - precond: every preconditioner non-zero read with its column index and
+      the vector entry it multiplies ((4 + 2s) each: C, C^T, factor, dense
+      blocks and cores), plus restrict / means / prolongation over the local
+      slots (4 + 5s each) and the output (s n_dofs), times k;
+    - vectors: 15 s n_dofs k (p~ update, alpha dot, v scale, solution update)."""
+    w = 1 if weighted else 0
+    op_survey = 2 * (4 * n * Q + s * n * n_slopes + s * n * w) + s * n * (1 + 2 * k) + s * nd * 2 * k
+    op_fused = 4 * n * Q + s * n * n_slopes + s * n * w + 2 * s * n * k + 2 * s * nd * k
+    pm = 0
+    if ps and ps.get("n_subdomains"):
+        nnz = ps["nnz_c"] + ps["nnz_ct"] + ps["nnz_fwd"] + ps["nnz_bwd"] + ps["nnz_dense"] + ps["nnz_core"]
+        pm = k * (nnz * (4 + 2 * s) + ps["n_slots"] * (4 + 5 * s) + s * nd)
+    elif ps:
+        pm = k * 3 * s * nd
+    return {"op_survey": op_survey, "op_fused": op_fused, "precond": pm, "vectors": 15 * s * nd * k}
 
 
 def dist_env():
@@ -280,6 +317,55 @@ def mixed_section(W, codes, dev, stream, args):
     return out
 
 
+def published_section(W, args):
+    """The reference's one published measurement (benches/wallclock_reference.json:5,
+    crates/within/benches/wallclock_1m3fe.rs:21-50): best of 5 wall-clock runs
+    of Solver::new + solve on the 1,000,000-row fixest-like panel with three
+    fixed effects (10 observations per worker, 10 years, firm = i % n_firm,
+    crates/within/benches/shared/fixest_dgp.rs:13-62), y uniform(-1, 1), tol
+    1e-6, maxiter 200, default additive Schwarz: 170.905 ms on a GitHub
+    Actions runner.  Here the timer also covers the design build (locality
+    sort), which the reference builds before its timer, and host numpy y in,
+    demeaned and x out; the oracle (C++ restatement, every host thread) runs
+    the same sequence."""
+    from within_b200 import workloads as WL
+    codes, y = WL.fixest_like()
+    opts = W.LsmrOptions(tol=1e-6, maxiter=200)
+    runs = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        s = W.Solver(codes)
+        t1 = time.perf_counter()
+        r = s.solve(y, opts)
+        t2 = time.perf_counter()
+        runs.append((t2 - t0, t1 - t0, t2 - t1, r.iterations, r.converged))
+        del s
+    best = min(runs, key=lambda x: x[0])
+    out = {"workload": "fixest-like 1,000,000 x 3 FE (indiv 100,000, year 10, firm 4,348 = i % n_firm), "
+                       "tol 1e-6, maxiter 200", "best_of": 5, "best_ms": best[0] * 1e3,
+           "setup_ms": best[1] * 1e3, "solve_ms": best[2] * 1e3, "iterations": best[3], "converged": best[4],
+           "all_ms": [round(x[0] * 1e3, 3) for x in runs], "reference_published_ms": 170.905,
+           "reference_published_hardware": "GitHub Actions ubuntu-latest runner (core count not recorded)"}
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            O.build()
+            O.lib().or_set_threads(os.cpu_count() or 1)
+            orr = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                so = O.OracleSolver(codes)
+                ro = so.solve(y, tol=1e-6, maxiter=200)
+                orr.append((time.perf_counter() - t0, ro.iterations))
+                del so
+            ob = min(orr)
+            out["cpu_restatement"] = {"best_ms": ob[0] * 1e3, "best_of": 3, "iterations": ob[1],
+                                      "cores": os.cpu_count() or 1, "kind": "port"}
+        except Exception as e:  # the baseline must not sink the GPU line
+            out["cpu_restatement"] = {"failed": str(e)}
+    return out
+
+
 def many_section(W, args):
     """Many independent designs: `args.many` designs with n log-uniform in
     [1e4, 2e6], 2-3 uniform factors with level counts log-uniform in
@@ -414,7 +500,7 @@ def run_ours(args):
     # accuracy against the FP64 oracle solve at tol 1e-12 (plain GPU, same design)
     dm = D[:, 0].clone()
     Xr, Dr, st_ref = solver.solve_device(yd, W.LsmrOptions(tol=1e-12, maxiter=5000))
-    err = float((dm - Dr[:, 0]).abs().max() / yd.norm())
+    err = demeaned_err(dm, Dr[:, 0], yd)
     # batched: k = 8 right-hand sides per solve_batch (one multi-RHS LSMR that
     # reads the design once per apply for all columns); solves/s = 8 / time
     from within_b200 import workloads as WL
@@ -435,24 +521,37 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     t_b = b0.elapsed_time(b1) / 1e3 / reps_b
     _, Dref_b, _ = solver.solve_device(Yb, W.LsmrOptions(tol=1e-12, maxiter=5000))
-    err_b = float(((Db - Dref_b).abs().max(dim=0).values / Yb.norm(dim=0)).max())
+    err_b = demeaned_err(Db, Dref_b, Yb)
     batched = {"k": kb, "value": kb / t_b, "unit": UNIT, "ms_per_batch": t_b * 1e3,
                "iterations_max": max(s_[1] for s_ in stb), "demeaned_err_vs_fp64_tol1e-12": err_b,
                "speedup_vs_single": (kb / t_b) / value * world}
     mixed = None if args.no_mixed else mixed_section(W, codes, dev, stream, args)
     many = None if (args.no_many or world > 1) else many_section(W, args)
     autograd = None if (args.no_autograd or world > 1) else autograd_section(W, dev)
-    # e2e through the host API (numpy in, numpy out)
-    for _ in range(1):
-        solver.solve(y, opts)
+    published = None if (args.no_published or world > 1) else published_section(W, args)
+    # e2e through the host API: y from page-locked host memory in, demeaned and
+    # x out to page-locked host buffers, every step (Solver.solve)
+    y_pin = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    y_pin[:] = y
+    x_pin = torch.empty(nd, dtype=torch.float64, pin_memory=True).numpy()
+    d_pin = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(2):
+        solver.solve(y_pin, opts, x_out=x_pin, demeaned_out=d_pin)
     if world > 1:
         torch.distributed.barrier()
     t1 = time.perf_counter()
     for _ in range(args.steps):
-        solver.solve(y, opts)
+        solver.solve(y_pin, opts, x_out=x_pin, demeaned_out=d_pin)
     t_e2e = time.perf_counter() - t1
     t_e2e = max_over_ranks(t_e2e, world, dev)
     e2e = world * args.steps / t_e2e
+    # the same with pageable numpy buffers (staged in chunks by the library)
+    solver.solve(y, opts)
+    t1 = time.perf_counter()
+    reps_pg = max(2, args.steps // 2)
+    for _ in range(reps_pg):
+        solver.solve(y, opts)
+    e2e_pageable = reps_pg / (time.perf_counter() - t1)
     # roofline: the operator pair A v / A^T u (the design operator) timed alone
     v = torch.randn(nd, dtype=torch.float64, device=dev)
     u = torch.randn(n, dtype=torch.float64, device=dev)
@@ -485,6 +584,17 @@ def run_ours(args):
     # dram__bytes_write.sum of k_apply and of the adjoint row sweep; the small run-combine
     # launch is not included): profiles/operator_traffic_akm10m.md
     traffic = (128803072 + 45006848 + 201513472 + 15891200) if n == 10_000_000 else None
+    pc = solver.preconditioner
+    ps = pc.stats() if pc is not None else None
+    ib = iteration_bytes(n, nd, Q, k=1, ps=ps)
+    t_solve = ms / 1e3
+    whole = {"bytes_per_iteration": ib, "iterations": it, "preconditioner": ps,
+             "gbs_survey": (ib["op_survey"] + ib["precond"] + ib["vectors"]) * it / t_solve / 1e9,
+             "gbs_fused": (ib["op_fused"] + ib["precond"] + ib["vectors"]) * it / t_solve / 1e9,
+             "note": "(B_op + B_M + B_vec) x iterations / device time of one solve (set-up and read-back "
+                     "kernels included in the time, not in the bytes)"}
+    whole["frac_survey"] = whole["gbs_survey"] / peaks()[0]
+    whole["frac_fused"] = whole["gbs_fused"] / peaks()[0]
     roof = {"bound": "hbm", "kernel": "design operator pair (gather k_apply D v + row-sweep D^T u and its run combine)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind, "traffic": traffic,
@@ -495,11 +605,14 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(n, nd),
         "iterations": it, "lsmr_iters_per_s": world * sum(iters) / t_max, "setup_s": t_setup,
-        "demeaned_err_vs_fp64_tol1e-12": err, "batched_fp64": batched, "mixed_batched": mixed,
-        "many_designs": many, "autograd": autograd,
+        "demeaned_err_vs_fp64_tol1e-12": err, "whole_solve": whole, "batched_fp64": batched,
+        "mixed_batched": mixed,
+        "many_designs": many, "autograd": autograd, "published_config": published,
         "roofline": roof,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
-                "d2h_bytes_per_step": 8 * (n + nd)},
+                "d2h_bytes_per_step": 8 * (n + nd),
+                "path": "Solver.solve, page-locked numpy y in, demeaned and x out (host clock)",
+                "pageable_numpy_value": e2e_pageable},
         "gpu_launches": launches, "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

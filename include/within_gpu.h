@@ -18,6 +18,24 @@
  *  - Multi-RHS arrays are column-major: column j of Y (n_obs x k) starts at
  *    Y + j*n_obs, as in BatchSolveResult (solver.rs:246-293).
  *  - Non-convergence is not an error: stats.converged = 0 (lsmr.rs:363-370).
+ *  - Streams: NULL selects the solver's own (non-blocking) stream and the call
+ *    returns after its work is done; any other handle (cudaStreamLegacy = 1
+ *    for the legacy default stream included) orders the call after the work
+ *    already queued there, and the operator applies return without waiting.
+ *    Solves and within_preconditioner_apply always wait for their result.
+ *  - Threads: every entry point may be called from any thread.  Calls on one
+ *    within_solver (solve, solve_batch, the operator applies, set_precision)
+ *    take that solver's mutex, so concurrent calls on one handle are safe and
+ *    run one after another: a second caller waits for the whole of the first
+ *    call (for a solve, its set-up, LSMR loop and result copies).  That
+ *    mirrors the reference's Solver::solve(&self) (solver.rs:503-527, shared
+ *    across threads in tests/test_free_threaded.py:32-58) without a per-call
+ *    workspace pool: a workspace is sized for the whole design (for the 10M-
+ *    row panel ~0.7 GB per column bucket), so one per caller would multiply
+ *    the memory.  For device overlap, give each thread its own solver, or use
+ *    within_solvers_solve_batch.  A preconditioner handle shared by several
+ *    solvers is read-only during solves; its per-solver plans live in each
+ *    solver.
  */
 #ifndef WITHIN_GPU_H
 #define WITHIN_GPU_H
@@ -151,6 +169,35 @@ int within_solver_solve_batch_device(within_solver* s, const double* Y_dev, uint
                                      const within_lsmr_options* opts, double* X_dev,
                                      double* D_dev, within_solve_stats* stats, void* stream);
 
+/* MlsmrOptions warm start and escalation (crates/schwarz-precond/src/lsmr.rs:
+ * 83-171, 206-297) on the FP64 solve of a design without slope terms.
+ * x0_dev (NULL = cold) is a device warm start in x's layout (n_dofs x k
+ * column-major): the solve runs on b - A x0 with the tolerances relative to
+ * the original ||b|| and returns x0 + the correction; b - A x0 = 0 returns x0
+ * at once (WITHIN_STOP_WARM_START_EXACT).  stale_window > 0 ends a column
+ * after that many consecutive iterations whose relative normal-equation
+ * residual shrank by less than stale_threshold (in [0, 1)) per iteration
+ * (Staleness, lsmr.rs:95-153): converged = 0, WITHIN_STOP_ESCALATED, x the
+ * iterate so far -- the warm start of the next rung of a preconditioner
+ * ladder.  stop_reason (k entries, may be NULL) receives the
+ * LsmrStopReason of each column (lsmr.rs:54-73). */
+#define WITHIN_STOP_ZERO_RHS 0
+#define WITHIN_STOP_INITIAL_NORMAL_RESIDUAL_ZERO 1
+#define WITHIN_STOP_RESIDUAL_TOLERANCE 2
+#define WITHIN_STOP_NORMAL_EQUATION_TOLERANCE 3
+#define WITHIN_STOP_WARM_START_EXACT 4
+#define WITHIN_STOP_MAX_ITERATIONS 5
+#define WITHIN_STOP_ESCALATED 6
+typedef struct {
+    const double* x0_dev;
+    uint64_t stale_window;
+    double stale_threshold;
+} within_solve_ext;
+int within_solver_solve_batch_device_ext(within_solver* s, const double* Y_dev, uint64_t k,
+                                         const within_lsmr_options* opts, const within_solve_ext* ext,
+                                         double* X_dev, double* D_dev, within_solve_stats* stats,
+                                         int32_t* stop_reason, void* stream);
+
 /* One-shot solve / solve_batch (solver.rs:611-646): Solver::new + solve. */
 int within_solve(const within_design* design, const double* y, const double* weights,
                  const within_lsmr_options* opts, const within_precond_config* cfg,
@@ -187,7 +234,10 @@ int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, 
  *    the size needed.
  *  - The first call on a device looks up the array's device address (with
  *    that device current) and caches it; make that first call before any
- *    stream capture that includes this entry point.
+ *    stream capture that includes this entry point.  The cache lives for the
+ *    process: after cudaDeviceReset (or any teardown of the device's primary
+ *    context) the cached address is stale, so do not call this entry point
+ *    again in that process.
  *  - Every call on a device shares the one array and leaves its contents
  *    behind; the call clears the counters it needs.  Calls that overlap on
  *    the GPU (other streams, other threads, other solvers) race on it and
@@ -220,6 +270,37 @@ void within_preconditioner_free(within_preconditioner* p);
 uint64_t within_preconditioner_n(const within_preconditioner* p);
 /* "Additive" or "Diagonal" */
 const char* within_preconditioner_variant_name(const within_preconditioner* p);
+/* Sizes of a built preconditioner (no counterpart in the reference, whose
+ * Preconditioner exposes only its dimension): the counts the per-iteration
+ * algorithmic bytes of its apply are computed from.  Zeros for the diagonal
+ * variant apart from n. */
+typedef struct {
+    uint64_t n;              /* DOFs */
+    uint64_t n_subdomains;
+    uint64_t n_slots;        /* local slots over all subdomains (restrict / prolong entries) */
+    uint64_t nnz_c;          /* C: eliminated x kept cross-block entries */
+    uint64_t nnz_ct;         /* C^T */
+    uint64_t nnz_fwd, nnz_bwd;   /* approximate-Cholesky factor, forward and backward pull forms */
+    uint64_t nnz_dense;      /* dense pseudo-inverse blocks of small reduced systems */
+    uint64_t nnz_core;       /* dense cores of round-scheduled factors */
+    uint64_t n_reduced;      /* reduced (kept + ground/cover) slots */
+    uint64_t n_rounds;       /* elimination rounds of the round-scheduled factor */
+} within_precond_stats;
+int within_preconditioner_stats(const within_preconditioner* p, within_precond_stats* out);
+/* Persisted preconditioner: Preconditioner pickling (__reduce__,
+ * crates/within-py/src/config.rs:366-389; Serialize/Deserialize,
+ * operator/schwarz.rs:115-183) in this library's own byte format -- the host
+ * image of the diagonal or Schwarz preconditioner with a magic, a version and
+ * a checksum (the reference's postcard bytes embed approx-chol's private
+ * layout, so the formats are not interchangeable).  serialize: buf NULL
+ * returns the size in *len; otherwise cap must hold it.  deserialize uploads
+ * the image to `device` (< 0: the current device); the handle is then
+ * PreconditionerInput::Prebuilt for within_solver_new on a design with the
+ * same DOF count, and solves with it are bitwise those of the original. */
+int within_preconditioner_serialize(const within_preconditioner* p, uint8_t* buf, uint64_t cap,
+                                    uint64_t* len);
+int within_preconditioner_deserialize(const uint8_t* buf, uint64_t len, int32_t device,
+                                      within_preconditioner** out);
 /* Preconditioner::apply: y = M^{-1} x on device buffers (n each). */
 int within_preconditioner_apply(const within_preconditioner* p, const double* x_dev,
                                 double* y_dev, void* stream);

@@ -71,6 +71,46 @@ def normal_equation_residual(cats, y, demeaned, weights=None):
     return num ** 0.5 / max(den ** 0.5, 1e-300)
 
 
+def demeaned_errors(a, ref, y):
+    """The difference of two demeaned vectors in both scalings the accuracy
+    figures use: ``inf_over_inf`` = max|a - ref| / max|y| and
+    ``inf_over_l2`` = max|a - ref| / ||y||_2.  The contract (1e-7 at tol
+    1e-8) is stated on ``inf_over_l2``; on n rows of unit-scale data the
+    second is about sqrt(n) / max|y| times smaller than the first."""
+    d = float(np.max(np.abs(np.asarray(a) - np.asarray(ref)))) if np.size(a) else 0.0
+    y = np.asarray(y)
+    return {"inf_over_inf": d / max(float(np.max(np.abs(y))) if y.size else 0.0, 1e-300),
+            "inf_over_l2": d / max(float(np.linalg.norm(y)), 1e-300)}
+
+
+def check_slope_drop_case(case, x, demeaned, unidentified, iterations, y):
+    """The expectations of one golden ``slope_drops`` case (tests/slopes.rs:157-326)
+    on one solve: unidentified triples in ascending (level, column) order,
+    exact zeros at the dropped slots, closed-form values (|got - exp| <=
+    1e-6 (1 + |exp|), the reference's assert_close), and for the collinear
+    case the iteration bound and residual orthogonality to every column of
+    every level plus the fitted values."""
+    assert [list(t) for t in unidentified] == case["drops"]
+    for slot in case["zero_slots"]:
+        assert x[slot] == 0.0, (slot, x[slot])
+    assert np.all(np.isfinite(x))
+    for slot, exp in case["checks"]:
+        assert abs(x[slot] - exp) <= 1e-6 * (1 + abs(exp)), (slot, x[slot], exp)
+    if "max_iterations" in case:
+        assert iterations <= case["max_iterations"]
+        lv = np.array(case["levels"])
+        zs = [np.array(z) for z in case["slopes"]]
+        nl = int(lv.max()) + 1
+        for lvl in range(nl):
+            m = lv == lvl
+            for col in [None] + zs:
+                dot = float(np.sum(demeaned[m] * (1.0 if col is None else col[m])))
+                assert abs(dot) < case["projection_tol"], (lvl, dot)
+        fitted = x[lv] + sum(x[(c + 1) * nl + lv] * zs[c] for c in range(len(zs)))
+        exp = y - demeaned
+        assert np.all(np.abs(fitted - exp) <= 1e-6 * (1 + np.abs(exp)))
+
+
 def dense_demeaned(cats, y, weights=None, slopes=None):
     """Exact demeaned vector via dense least squares (small n only)."""
     n = len(y)

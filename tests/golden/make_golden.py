@@ -98,6 +98,88 @@ def slope_cases():
     ]
 
 
+def weighted_per_level_ols(levels, z, y, w, n_levels):
+    """tests/slopes.rs:19-45 with weights: per-level weighted OLS of y on [1, z]."""
+    a, b = [], []
+    for lv in range(n_levels):
+        m = levels == lv
+        sw = w[m].sum()
+        sz = (w[m] * z[m]).sum()
+        szz = (w[m] * z[m] * z[m]).sum()
+        sy = (w[m] * y[m]).sum()
+        szy = (w[m] * z[m] * y[m]).sum()
+        den = sw * szz - sz * sz
+        bb = (sw * szy - sz * sy) / den if den != 0 else float("nan")
+        a.append(float((sy - bb * sz) / sw) if sw != 0 else float("nan"))
+        b.append(float(bb))
+    return a, b
+
+
+def slope_drop_cases():
+    """tests/slopes.rs:157-326 -- rank drops with exact zeros, zero-weight
+    masking, batch sharing and three collinear slopes.  Each case gives the
+    reference's expected unidentified (term, level, column) triples, the x
+    slots that must read exactly 0.0, and closed-form values for the
+    identified slots ("checks": [slot, expected])."""
+    synthetic_y = lambda n: np.array([math.sin(i * 0.9 - 1.0) * 2.0 + 0.5 for i in range(n)])  # noqa: E731
+    cases = []
+    # rank_drops_report_deterministically_with_exact_zeros: level 1 never
+    # occurs, level 2's slope is constant
+    lv = np.array([0, 0, 0, 2, 2, 2, 3, 3, 3])
+    z = np.array([1.0, 2.0, -1.5, 2.5, 2.5, 2.5, -2.0, 0.7, 1.3])
+    y = synthetic_y(9)
+    a, b = weighted_per_level_ols(lv, z, y, np.ones(9), 4)
+    checks = [[2, float(y[3:6].mean())]] + [[l, a[l]] for l in (0, 3)] + [[4 + l, b[l]] for l in (0, 3)]
+    cases.append({"source": "tests/slopes.rs rank_drops_report_deterministically_with_exact_zeros",
+                  "levels": lv.tolist(), "slopes": [z.tolist()], "y": [y.tolist()], "weights": None,
+                  "drops": [[0, 1, 0], [0, 1, 1], [0, 2, 1]], "zero_slots": [1, 5, 6], "checks": checks,
+                  "also_diagonal": True})
+    # weighted_solve_matches_closed_form_and_masks_zero_weight_rows
+    lv = np.array([0, 1, 0, 1, 0, 1, 2, 2, 2])
+    z = np.array([0.5, -1.2, 3.3, 1.5, 0.7, -2.1, 5.0, 5.0, 7.0])
+    w = np.array([1.0, 0.5, 2.0, 1.5, 3.0, 1.0, 1.0, 1.0, 0.0])
+    y = synthetic_y(9)
+    a, b = weighted_per_level_ols(lv, z, y, w, 3)
+    checks = [[l, a[l]] for l in (0, 1)] + [[3 + l, b[l]] for l in (0, 1)] + [[2, float((y[6] + y[7]) / 2)]]
+    cases.append({"source": "tests/slopes.rs weighted_solve_matches_closed_form_and_masks_zero_weight_rows",
+                  "levels": lv.tolist(), "slopes": [z.tolist()], "y": [y.tolist()], "weights": w.tolist(),
+                  "drops": [[0, 2, 1]], "zero_slots": [5], "checks": checks, "also_diagonal": False})
+    # zero_weight_garbage_does_not_poison_identification
+    lv = np.array([0, 0, 0, 1, 1, 1])
+    z = np.array([1.0, 2.0, 3.0, 5.0, 7.0, 1e300])
+    w = np.array([1.0, 1.0, 1.0, 1.0, 1.0, 0.0])
+    y = synthetic_y(6)
+    keep = w > 0
+    a, b = weighted_per_level_ols(lv[keep], z[keep], y[keep], w[keep], 2)
+    checks = [[l, a[l]] for l in (0, 1)] + [[2 + l, b[l]] for l in (0, 1)]
+    cases.append({"source": "tests/slopes.rs zero_weight_garbage_does_not_poison_identification",
+                  "levels": lv.tolist(), "slopes": [z.tolist()], "y": [y.tolist()], "weights": w.tolist(),
+                  "drops": [], "zero_slots": [], "checks": checks, "also_diagonal": True})
+    # batch_solve_shares_unidentified_and_back_transforms_each_rhs
+    lv = np.array([0, 0, 0, 1, 1, 1])
+    z = np.array([1.0, 2.0, 3.0, 2.5, 2.5, 2.5])
+    y1 = synthetic_y(6)
+    y2 = y1 * -1.5 + 0.3
+    cases.append({"source": "tests/slopes.rs batch_solve_shares_unidentified_and_back_transforms_each_rhs",
+                  "levels": lv.tolist(), "slopes": [z.tolist()], "y": [y1.tolist(), y2.tolist()],
+                  "weights": None, "drops": [[0, 1, 1]], "zero_slots": [3], "checks": [],
+                  "also_diagonal": False})
+    # three_slopes_solve_bounded_with_exact_rank_drops: level 1's z2 and z3
+    # are exactly collinear; the pivot keeps z3, so z2's slot reads 0
+    n = 24
+    lv = np.array([i % 3 for i in range(n)])
+    z1 = np.array([math.sin(i * 0.37) * 2.0 for i in range(n)])
+    z2 = np.array([0.95 * z1[i] + 0.1 * math.cos(i * 0.9 + 0.2) for i in range(n)])
+    z3 = np.array([2.0 * z2[i] if i % 3 == 1 else -0.8 * z1[i] + 0.15 * math.sin(i * 1.7) + 0.1
+                   for i in range(n)])
+    y = synthetic_y(n)
+    cases.append({"source": "tests/slopes.rs three_slopes_solve_bounded_with_exact_rank_drops",
+                  "levels": lv.tolist(), "slopes": [z1.tolist(), z2.tolist(), z3.tolist()], "y": [y.tolist()],
+                  "weights": None, "drops": [[0, 1, 2]], "zero_slots": [2 * 3 + 1], "checks": [],
+                  "max_iterations": 30, "projection_tol": 1e-6, "also_diagonal": False})
+    return cases
+
+
 def lsmr_cases():
     """crates/schwarz-precond/src/lsmr/fixtures.rs and lsmr/tests/solve.rs."""
     over = [[1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0]]
@@ -143,6 +225,7 @@ def main():
                         "categories": [0, 0, 1, 1, 1, 2], "y": [1.0, 3.0, 2.0, 4.0, 6.0, 5.0],
                         "x": [2.0, 4.0, 5.0]},
         "slopes": slope_cases(),
+        "slope_drops": slope_drop_cases(),
         "lsmr": lsmr_cases(),
         "vec_norm": {"source": "solve.rs vec_norm_is_overflow_safe_and_propagates_nan",
                      "cases": [[[], 0.0], [[3.0, 4.0], 5.0]]},

@@ -170,3 +170,21 @@ def test_threaded_timing_mode_matches_reference_order(oracle):
     assert np.array_equal(a.demeaned, b.demeaned)
     assert c.converged
     assert np.max(np.abs(a.demeaned - c.demeaned)) / np.max(np.abs(y)) < 1e-8
+
+
+@pytest.mark.parametrize("case", GOLDEN["slope_drops"], ids=lambda c: c["source"].split()[-1])
+def test_slope_rank_drops(oracle, case):
+    """Rank drops, exact zeros and closed forms of tests/slopes.rs:157-326 on
+    the restatement (the GPU runs the same cases in test_gpu_slopes.py)."""
+    from conftest import check_slope_drop_case
+    lv = np.array(case["levels"], np.uint32)
+    zs = tuple(np.array(z) for z in case["slopes"])
+    w = None if case["weights"] is None else np.array(case["weights"])
+    kinds = ["additive", "diagonal"] if case["also_diagonal"] else ["additive"]
+    for kind in kinds:
+        s = oracle.OracleSolver([oracle.Effect(lv, True, zs)], weights=w, cfg=oracle.precond_cfg(kind))
+        for yv in case["y"]:
+            y = np.array(yv)
+            r = s.solve(y)
+            assert r.converged
+            check_slope_drop_case(case, r.x, r.demeaned, s.unidentified(), r.iterations, y)

@@ -1,24 +1,31 @@
 """GPU parity of the CUDA path against the CPU FP64 restatement (oracle).
 
-Tolerance: demeaned vectors agree within 1e-7 relative to ||y||
-in the infinity norm at tol 1e-8; the tests solve tighter (1e-10) and hold the
-same bound.  Integer work (grouping permutation, layout) must match exactly.
+Tolerances: demeaned vectors agree within 1e-7 in max|difference| / ||y||_2
+(the contract's scaling, stated at tol 1e-8) and within 1e-6 in
+max|difference| / max|y|; these tests solve tighter (tol 1e-10 to 1e-11) and
+hold both bounds.  The contract tolerance itself, on the benchmark designs, is
+tested in test_gpu_contract.py.  Integer work (grouping permutation, layout)
+must match exactly.
 """
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
-from conftest import (as_solver_categories, dense_demeaned, generate_synthetic_data,
+from conftest import (as_solver_categories, demeaned_errors, dense_demeaned, generate_synthetic_data,
                       normal_equation_residual)
 
 pytestmark = pytest.mark.gpu
 
-DEMEAN_TOL = 1e-7
+DEMEAN_TOL = 1e-7        # max|difference| / ||y||_2
+DEMEAN_TOL_INF = 1e-6    # max|difference| / max|y|
 
 
 def rel_inf(a, b, y):
-    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.linalg.norm(y), 1e-300))
+    """max|a - b| / ||y||_2, after checking max|a - b| / max|y| <= DEMEAN_TOL_INF."""
+    e = demeaned_errors(a, b, y)
+    assert e["inf_over_inf"] <= DEMEAN_TOL_INF, e
+    return e["inf_over_l2"]
 
 
 def two_factor(n=5000, l0=50, l1=30, seed=1):

@@ -43,6 +43,12 @@ __all__ = [
     "demean",
     "SolverSet",
     "solve_many",
+    "fwl",
+    "FwlResult",
+    "Staleness",
+    "MlsmrResult",
+    "solve_ladder",
+    "LadderResult",
     "config",
 ]
 
@@ -83,6 +89,36 @@ class LsmrOptions:
 
     def _c(self) -> _ffi.LsmrOptionsC:
         return _ffi.LsmrOptionsC(float(self.tol), int(self.maxiter), int(self.local_size or 0))
+
+
+@dataclass(frozen=True)
+class Staleness:
+    """Escalation rule (crates/schwarz-precond/src/lsmr.rs:95-153): hand off
+    after ``window`` consecutive iterations whose relative normal-equation
+    residual contracted by a ratio above ``threshold`` (in [0, 1))."""
+
+    window: int
+    threshold: float
+
+    def __post_init__(self):
+        if int(self.window) <= 0:
+            raise ValueError("staleness window must be positive")
+        if not 0.0 <= float(self.threshold) < 1.0:
+            raise ValueError(f"staleness threshold must be in [0, 1), got {self.threshold}")
+
+
+@dataclass
+class MlsmrResult:
+    """Device result of :meth:`Solver.mlsmr_device`: X (n_dofs, k) and D
+    (n_obs, k) CUDA tensors, per-column convergence and stop reasons
+    (LsmrStopReason names, lsmr.rs:54-73)."""
+
+    x: object
+    demeaned: object
+    converged: list
+    iterations: list
+    residual: list
+    stop_reason: list
 
 
 class Effect:
@@ -223,17 +259,44 @@ class Preconditioner:
     def ncols(self) -> int:
         return self.nrows()
 
+    def stats(self) -> dict:
+        """Sizes of the built preconditioner (subdomains, local slots and the
+        non-zeros of C, C^T, the factor and the dense blocks)."""
+        st = _ffi.PrecondStatsC()
+        _ffi.check(_ffi.lib().within_preconditioner_stats(self._h, C.byref(st)))
+        return {f: int(getattr(st, f)) for f, _ in _ffi.PrecondStatsC._fields_}
+
     def apply_device(self, x, y, stream=None) -> None:
-        """``y = M^-1 x`` on CUDA float64 tensors of length n (Preconditioner::apply)."""
+        """``y = M^-1 x`` on CUDA float64 tensors of length n (Preconditioner::apply),
+        on ``stream`` (a cudaStream_t as int; default torch's current stream, so
+        the call is ordered with the torch work that produced ``x``)."""
         _ffi.check(_ffi.lib().within_preconditioner_apply(
-            self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
-            None if stream is None else C.c_void_p(stream)))
+            self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(_stream_of(x, stream))))
 
     def __repr__(self) -> str:
         return f"Preconditioner({self.variant_name}, n={self.nrows()})"
 
+    def to_bytes(self) -> bytes:
+        """The preconditioner's host image in this library's byte format."""
+        L = _ffi.lib()
+        n = C.c_uint64()
+        _ffi.check(L.within_preconditioner_serialize(self._h, None, 0, C.byref(n)))
+        buf = (C.c_uint8 * max(1, n.value))()
+        _ffi.check(L.within_preconditioner_serialize(self._h, buf, n.value, C.byref(n)))
+        return bytes(buf[:n.value])
+
+    @classmethod
+    def from_bytes(cls, data: bytes, device: int = -1) -> "Preconditioner":
+        """Uploads a serialised preconditioner to ``device`` (default: current)."""
+        data = bytes(data)
+        h = C.c_void_p()
+        buf = (C.c_uint8 * max(1, len(data))).from_buffer_copy(data or b"\0")
+        _ffi.check(_ffi.lib().within_preconditioner_deserialize(buf, len(data), device, C.byref(h)))
+        return cls(h)
+
     def __reduce__(self):
-        raise TypeError("within_b200.Preconditioner lives in GPU memory and is not picklable")
+        # pickling (crates/within-py/src/config.rs:366-389): the host image as bytes
+        return (Preconditioner.from_bytes, (self.to_bytes(),))
 
 
 # ---------------------------------------------------------------------------
@@ -315,11 +378,31 @@ class _Design:
             self.h = None
 
 
+def _stream_of(t, stream):
+    """The cudaStream_t to run on: ``stream`` if given, else torch's current
+    stream on the tensor's device.  Handle 0 (torch's default stream) becomes
+    cudaStreamLegacy: the C ABI reads NULL as "the solver's own stream", which
+    is not ordered with torch's work."""
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream(t.device).cuda_stream
+    return int(stream) or _ffi.CUDA_STREAM_LEGACY
+
+
 def _as_f64_1d(name, a):
     arr = np.asarray(a)
     if arr.ndim != 1 or arr.dtype != np.float64:
         raise TypeError(f"{name} must be a 1-D float64 array, got dtype {arr.dtype}")
     return np.ascontiguousarray(arr)
+
+
+def _out_f64_1d(name, a, n):
+    if not isinstance(a, np.ndarray) or a.ndim != 1 or a.dtype != np.float64 or not a.flags.c_contiguous \
+            or not a.flags.writeable:
+        raise TypeError(f"{name} must be a writeable contiguous 1-D float64 array")
+    if a.shape[0] != n:
+        raise ValueError(f"{name} has length {a.shape[0]}, expected {n}")
+    return a
 
 
 def _as_f64_2d(name, a):
@@ -412,13 +495,19 @@ class Solver:
         out = np.zeros(self._n_obs, np.uint32)
         return out if _ffi.lib().within_solver_obs_perm(self._h, _ffi.ptr(out)) else None
 
-    def solve(self, y, options: LsmrOptions | None = None) -> SolveResult:
+    def solve(self, y, options: LsmrOptions | None = None, *, x_out=None, demeaned_out=None) -> SolveResult:
+        """Solver::solve (solver.rs:503-527).  ``x_out`` / ``demeaned_out``
+        (optional, 1-D float64 of n_dofs / n_obs) receive the results in
+        place; page-locked buffers (e.g. ``torch.empty(n, dtype=torch.float64,
+        pin_memory=True).numpy()``), like a page-locked ``y``, are copied by
+        DMA directly, pageable ones through the library's staging slots."""
         y = _as_f64_1d("y", y)
         if y.shape[0] != self._n_obs:
             raise ValueError(f"response vector length ({y.shape[0]}) does not match number of "
                              f"observations ({self._n_obs})")
-        x = np.zeros(self._n_dofs)
-        dm = np.zeros(self._n_obs)
+        x = np.zeros(self._n_dofs) if x_out is None else _out_f64_1d("x_out", x_out, self._n_dofs)
+        dm = np.zeros(self._n_obs) if demeaned_out is None else _out_f64_1d("demeaned_out", demeaned_out,
+                                                                             self._n_obs)
         st = _ffi.SolveStatsC()
         opts = (options or LsmrOptions())._c()
         _ffi.check(_ffi.lib().within_solver_solve(self._h, _ffi.ptr(y), C.byref(opts), _ffi.ptr(x),
@@ -459,24 +548,61 @@ class Solver:
             D = torch.empty((k, self._n_obs), dtype=torch.float64, device=Y.device).t()
         st = (_ffi.SolveStatsC * k)()
         opts = (options or LsmrOptions())._c()
-        if stream is None:
-            stream = torch.cuda.current_stream(Y.device).cuda_stream
         _ffi.check(_ffi.lib().within_solver_solve_batch_device(
             self._h, C.c_void_p(Y.data_ptr()), k, C.byref(opts), C.c_void_p(X.data_ptr()),
-            C.c_void_p(D.data_ptr()), st, C.c_void_p(stream)))
+            C.c_void_p(D.data_ptr()), st, C.c_void_p(_stream_of(Y, stream))))
         stats = [(bool(st[i].converged), int(st[i].iterations), float(st[i].residual)) for i in range(k)]
         return X, D, stats
 
-    # Operator trait plumbing (internal observation order, device buffers)
+    def mlsmr_device(self, Y, options: LsmrOptions | None = None, warm_start=None,
+                     escalation: Staleness | None = None, X=None, D=None, stream=None) -> MlsmrResult:
+        """solve_device with the MlsmrOptions extras (lsmr.rs:155-171):
+        ``warm_start`` a CUDA float64 (n_dofs,) or (n_dofs, k) tensor in x's
+        layout (column-major storage for k > 1), ``escalation`` a Staleness
+        rule.  Designs with slope terms take no warm start."""
+        import torch
+        if Y.dtype != torch.float64 or not Y.is_cuda:
+            raise TypeError("Y must be a CUDA float64 tensor")
+        k = 1 if Y.dim() == 1 else Y.shape[1]
+        if X is None:
+            X = torch.empty((k, self._n_dofs), dtype=torch.float64, device=Y.device).t()
+        if D is None:
+            D = torch.empty((k, self._n_obs), dtype=torch.float64, device=Y.device).t()
+        ext = _ffi.SolveExtC(None, 0, 0.0)
+        if warm_start is not None:
+            x0 = warm_start
+            if x0.dtype != torch.float64 or not x0.is_cuda:
+                raise TypeError("warm_start must be a CUDA float64 tensor")
+            if (x0.dim() == 1 and (k != 1 or x0.shape[0] != self._n_dofs)) or \
+                    (x0.dim() == 2 and tuple(x0.shape) != (self._n_dofs, k)):
+                raise ValueError(f"warm-start shape {tuple(x0.shape)} does not match ({self._n_dofs}, {k})")
+            if x0.dim() == 2 and not (x0.stride(0) == 1 and x0.stride(1) == self._n_dofs):
+                x0 = x0.t().contiguous().t()
+            ext.x0_dev = x0.data_ptr()
+        if escalation is not None:
+            ext.stale_window = int(escalation.window)
+            ext.stale_threshold = float(escalation.threshold)
+        st = (_ffi.SolveStatsC * k)()
+        stops = (C.c_int32 * k)()
+        opts = (options or LsmrOptions())._c()
+        _ffi.check(_ffi.lib().within_solver_solve_batch_device_ext(
+            self._h, C.c_void_p(Y.data_ptr()), k, C.byref(opts), C.byref(ext), C.c_void_p(X.data_ptr()),
+            C.c_void_p(D.data_ptr()), st, stops, C.c_void_p(_stream_of(Y, stream))))
+        return MlsmrResult(X, D, [bool(st[i].converged) for i in range(k)], [int(st[i].iterations) for i in range(k)],
+                           [float(st[i].residual) for i in range(k)],
+                           [_ffi.STOP_REASONS[stops[i]] if 0 <= stops[i] < len(_ffi.STOP_REASONS) else "None"
+                            for i in range(k)])
+
+    # Operator trait plumbing (internal observation order, device buffers), on
+    # ``stream`` (default torch's current stream: ordered with the torch work
+    # around the call, and asynchronous like any torch op)
     def operator_apply_device(self, x, y, stream=None) -> None:
         _ffi.check(_ffi.lib().within_solver_operator_apply(
-            self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
-            None if stream is None else C.c_void_p(stream)))
+            self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(_stream_of(x, stream))))
 
     def operator_apply_adjoint_device(self, u, y, stream=None) -> None:
         _ffi.check(_ffi.lib().within_solver_operator_apply_adjoint(
-            self._h, C.c_void_p(u.data_ptr()), C.c_void_p(y.data_ptr()),
-            None if stream is None else C.c_void_p(stream)))
+            self._h, C.c_void_p(u.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(_stream_of(u, stream))))
 
 
 def solve(design, y, weights=None, options: LsmrOptions | None = None, preconditioner=None) -> SolveResult:
@@ -593,6 +719,107 @@ def solve_many(designs, Ys, weights=None, options: LsmrOptions | None = None, pr
                threads: int = 8, precision: str = "fp64"):
     """One-shot ``SolverSet(designs, weights, preconditioner).solve_batch(Ys)``."""
     return SolverSet(designs, weights, preconditioner, threads=threads, precision=precision).solve_batch(Ys, options)
+
+
+@dataclass
+class LadderResult:
+    """Result of :func:`solve_ladder`: x / demeaned (host, (n_dofs, k) and
+    (n_obs, k)), per column the rung that finished it, its convergence, the
+    iterations of every rung summed, and the stop reason of the last rung."""
+
+    x: np.ndarray
+    demeaned: np.ndarray
+    rung: list
+    converged: list
+    iterations: list
+    stop_reason: list
+
+
+def solve_ladder(design, Y, weights=None, options: LsmrOptions | None = None,
+                 escalation: Staleness = Staleness(4, 0.7), device: int = -1) -> LadderResult:
+    """A two-rung preconditioner ladder (warm starts and escalation,
+    crates/schwarz-precond/src/lsmr.rs:83-171, the pattern of its
+    test_mlsmr_ladder_warm_starts_and_escalates): every column is solved with
+    the diagonal preconditioner under the staleness rule; the columns that
+    escalate continue on the additive Schwarz preconditioner (built only if
+    needed), warm-started from the diagonal rung's iterate.  Both rungs run on
+    the GPU; the tolerance stays relative to each column's original ||b||."""
+    import torch
+    Ya = np.asarray(Y, dtype=np.float64)
+    Ya = Ya.reshape(-1, 1) if Ya.ndim == 1 else Ya
+    opts = options or LsmrOptions()
+    dev = torch.device("cuda", torch.cuda.current_device() if device < 0 else device)
+    weak = Solver(design, weights, PreconditionerConfig.Diagonal, device=dev.index)
+    Yd = torch.from_numpy(np.ascontiguousarray(Ya.T)).to(dev).t()
+    r1 = weak.mlsmr_device(Yd, opts, escalation=escalation)
+    X = r1.x.clone()
+    D = r1.demeaned.clone()
+    k = Ya.shape[1]
+    rung = ["Diagonal"] * k
+    conv, its, stops = list(r1.converged), list(r1.iterations), list(r1.stop_reason)
+    esc = [j for j in range(k) if r1.stop_reason[j] == "Escalated"]
+    if esc:
+        strong = Solver(design, weights, None, device=dev.index)
+        Ye = Yd[:, esc].t().contiguous().t()
+        X0 = r1.x[:, esc].t().contiguous().t()
+        r2 = strong.mlsmr_device(Ye, opts, warm_start=X0)
+        for i, j in enumerate(esc):
+            X[:, j] = r2.x[:, i]
+            D[:, j] = r2.demeaned[:, i]
+            rung[j] = "Additive"
+            conv[j] = r2.converged[i]
+            its[j] += r2.iterations[i]
+            stops[j] = r2.stop_reason[i]
+    return LadderResult(X.cpu().numpy(), D.cpu().numpy(), rung, conv, its, stops)
+
+
+@dataclass
+class FwlResult:
+    """Frisch-Waugh-Lovell regression of y on X absorbing the fixed effects:
+    ``beta`` (p,), the demeaned response and covariates, and the solve's
+    per-column convergence."""
+
+    beta: np.ndarray
+    demeaned_y: np.ndarray
+    demeaned_X: np.ndarray
+    converged: list
+    iterations: list
+
+
+def fwl(design, y, X, weights=None, options: LsmrOptions | None = None, preconditioner=None,
+        solver: "Solver | None" = None, device: int = -1) -> FwlResult:
+    """The FWL regression step after solve_batch (README.md:54-65 of the
+    reference): demean [y, X] in one multi-RHS solve on the GPU, then solve the
+    least-squares problem min ||W^{1/2} (y~ - X~ beta)|| on the GPU by a QR
+    factorisation of the weighted demeaned covariates (FP64), so the n x p
+    columns never leave the device.  ``solver`` reuses a built Solver of the
+    same design and weights."""
+    import torch
+    y = _as_f64_1d("y", y)
+    Xa = np.asarray(X, dtype=np.float64)
+    if Xa.ndim == 1:
+        Xa = Xa.reshape(-1, 1)
+    if Xa.shape[0] != y.shape[0]:
+        raise ValueError(f"X has {Xa.shape[0]} rows, y has {y.shape[0]}")
+    s = solver if solver is not None else Solver(design, weights, preconditioner, device=device)
+    if s.n_obs != y.shape[0]:
+        raise ValueError(f"y has {y.shape[0]} rows but the solver has {s.n_obs} observations")
+    dev = torch.device("cuda", torch.cuda.current_device() if device < 0 else device)
+    p = Xa.shape[1]
+    Y = torch.empty((p + 1, s.n_obs), dtype=torch.float64, device=dev)
+    Y[0].copy_(torch.from_numpy(y))
+    Y[1:].copy_(torch.from_numpy(np.ascontiguousarray(Xa.T)))
+    _, D, stats = s.solve_device(Y.t(), options)
+    yt, Xt = D[:, 0], D[:, 1:]
+    if weights is not None:
+        sw = torch.from_numpy(np.sqrt(_as_f64_1d("weights", weights))).to(dev)
+        yw, Xw = yt * sw, Xt * sw[:, None]
+    else:
+        yw, Xw = yt, Xt
+    Qm, Rm = torch.linalg.qr(Xw, mode="reduced")
+    beta = torch.linalg.solve_triangular(Rm, (Qm.t() @ yw).unsqueeze(1), upper=True).squeeze(1)
+    return FwlResult(beta.cpu().numpy(), yt.cpu().numpy(), Xt.cpu().numpy(),
+                     [c for c, _, _ in stats], [it for _, it, _ in stats])
 
 
 from .autograd import demean  # noqa: E402  (differentiable demeaning; imports torch lazily)

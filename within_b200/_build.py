@@ -16,7 +16,8 @@ LIB = os.path.join(LIB_DIR, "libwithin_gpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["solver.cu", "host_design.cpp", "host_schwarz.cpp"]
-HEADERS = ["host.hpp", "kernels.cuh", "segreduce.cuh", "segplan.hpp", "refine.cuh", "rowsweep.cuh"]
+HEADERS = ["host.hpp", "kernels.cuh", "segreduce.cuh", "segplan.hpp", "refine.cuh", "rowsweep.cuh",
+           "bulk.cuh", "tsweep.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -27,6 +27,9 @@ PRECOND_DIAGONAL = 2
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+# cudaStreamLegacy: the legacy default stream (torch's default stream) as a
+# non-NULL handle, so a call on it is ordered with torch's work
+CUDA_STREAM_LEGACY = 1
 
 
 class PrecondConfigC(C.Structure):
@@ -58,6 +61,19 @@ class SolveStatsC(C.Structure):
         ("time_setup", C.c_double),
         ("time_solve", C.c_double),
     ]
+
+
+class SolveExtC(C.Structure):
+    _fields_ = [("x0_dev", C.c_void_p), ("stale_window", C.c_uint64), ("stale_threshold", C.c_double)]
+
+
+STOP_REASONS = ["ZeroRhs", "InitialNormalEquationResidualZero", "ResidualTolerance", "NormalEquationTolerance",
+                "WarmStartExact", "MaxIterations", "Escalated"]
+
+
+class PrecondStatsC(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in ("n", "n_subdomains", "n_slots", "nnz_c", "nnz_ct", "nnz_fwd",
+                                          "nnz_bwd", "nnz_dense", "nnz_core", "n_reduced", "n_rounds")]
 
 
 # (name, restype, argtypes) of every exported entry point in within_gpu.h
@@ -95,6 +111,10 @@ _SIGNATURES = [
     ("within_preconditioner_free", None, [P]),
     ("within_preconditioner_n", U64, [P]),
     ("within_preconditioner_variant_name", C.c_char_p, [P]),
+    ("within_preconditioner_stats", C.c_int, [P, P]),
+    ("within_solver_solve_batch_device_ext", C.c_int, [P, P, U64, P, P, P, P, P, P, P]),
+    ("within_preconditioner_serialize", C.c_int, [P, P, U64, P]),
+    ("within_preconditioner_deserialize", C.c_int, [P, U64, C.c_int32, P]),
     ("within_preconditioner_apply", C.c_int, [P, P, P, P]),
     ("within_adjoint_rhs", C.c_int, [U64, U64, P, P, P, P]),
     ("within_demean_vjp", C.c_int, [U64, U64, P, P, P, P, P, P, P]),

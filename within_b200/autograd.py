@@ -33,7 +33,9 @@ def _colmajor(t):
 
 def _stream(dev):
     import torch
-    return C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    # torch's default stream (handle 0) is passed as cudaStreamLegacy: NULL
+    # would select the solver's own stream, unordered with torch's work
+    return C.c_void_p(torch.cuda.current_stream(dev).cuda_stream or _ffi.CUDA_STREAM_LEGACY)
 
 
 def _check_f64_cuda(name, t):

@@ -45,6 +45,11 @@ struct ColState {
     double b_norm;
     long long itn, maxiter;
     int done, stop, upd, err;
+    // Staleness escalation (lsmr.rs:83-153): stale_window consecutive ratios
+    // |zeta_bar_k| / |zeta_bar_{k-1}| above stale_thr end the column with
+    // STOP_ESCALATED; window 0 = never
+    double stale_thr, stale_prev;
+    int stale_window, stale_n;
 };
 
 struct Ctl {
@@ -67,8 +72,10 @@ __global__ void k_loop_cond(Ctl* ctl, cudaGraphConditionalHandle h) {
     cudaGraphSetConditional(h, (!ctl->all_done && !ctl->err && left > 0) ? 1u : 0u);
 }
 
+// LsmrStopReason (lsmr.rs:54-73), same order
 enum Stop { STOP_NONE = -1, STOP_ZERO_RHS = 0, STOP_INIT_ZERO = 1, STOP_RESID = 2, STOP_NORMAL = 3,
-            STOP_MAXITER = 5 };
+            STOP_WARM_EXACT = 4, STOP_MAXITER = 5, STOP_ESCALATED = 6 };
+constexpr int ERR_WARM_NONFINITE = 10;   // device error: b - A x0 has a non-finite norm
 
 // ---------------------------------------------------------------------------
 // fixed-order block reduction helpers
@@ -928,7 +935,8 @@ k_alpha_step(uint32_t n, const double* __restrict__ v, const double* __restrict_
         s.beta_prev_inv = beta == 0.0 ? 0.0 : 1.0 / beta;
         s.itn += 1;
         s.upd = 1;
-        // ConvergenceState::check
+        // ConvergenceState::check, then the escalation rule, then the budget
+        // (lsmr_from_bidiag, lsmr.rs:324-370)
         const double residual = fabs(s.phi_bar);
         if (residual <= s.abs_tol) {
             s.done = 1;
@@ -938,10 +946,20 @@ k_alpha_step(uint32_t n, const double* __restrict__ v, const double* __restrict_
             if (fabs(s.zeta_bar) / (an * fmax(residual, DBL_MIN)) <= s.rel_tol) {
                 s.done = 1;
                 s.stop = STOP_NORMAL;
-            } else if (s.itn >= s.maxiter) {
-                s.done = 1;
-                s.stop = STOP_MAXITER;
             }
+        }
+        if (!s.done && s.stale_window > 0) {   // Staleness::should_escalate (lsmr.rs:138-152)
+            const double ne = fabs(s.zeta_bar) / s.zeta0;
+            if (isfinite(s.stale_prev) && s.stale_prev > 0.0) s.stale_n = ne / s.stale_prev > s.stale_thr ? s.stale_n + 1 : 0;
+            s.stale_prev = ne;
+            if (s.stale_n >= s.stale_window) {
+                s.done = 1;
+                s.stop = STOP_ESCALATED;
+            }
+        }
+        if (!s.done && s.itn >= s.maxiter) {
+            s.done = 1;
+            s.stop = STOP_MAXITER;
         }
         nxt[k] = s;
         all = all && s.done;
@@ -1130,7 +1148,8 @@ k_load_rhs(uint32_t n, uint32_t k_used, const double* __restrict__ Y, const uint
 template <int K>
 __global__ void __launch_bounds__(RED_THREADS)
 k_norm_b(uint32_t n, const double* __restrict__ b, const double* bmax, ColState* st, double tol,
-         long long maxiter, uint32_t k_used, Ctl* ctl, double* partials, unsigned* counter) {
+         long long maxiter, uint32_t k_used, Ctl* ctl, double* partials, unsigned* counter, int warm = 0,
+         int stale_window = 0, double stale_thr = 0.0) {
     double acc[K];
     double sc[K];
 #pragma unroll
@@ -1146,22 +1165,36 @@ k_norm_b(uint32_t n, const double* __restrict__ b, const double* bmax, ColState*
         }
     double tot[K];
     if (!grid_reduce<K>(acc, partials, counter, tot) || threadIdx.x != 0) return;
+    // warm: b holds b - A x0; the tolerances stay relative to the original
+    // ||b|| of the previous call (mlsmr, lsmr.rs:232-292), a zero residual
+    // returns x0 (STOP_WARM_EXACT) and a non-finite one is an input error
     for (int k = 0; k < K; ++k) {
+        const double b_orig = st[k].b_norm;
         ColState s;
         memset(&s, 0, sizeof(s));
         const double beta = bmax[k] == 0.0 ? 0.0 : bmax[k] * sqrt(tot[k]);
         s.beta = beta;
-        s.b_norm = beta;
+        s.b_norm = warm ? b_orig : beta;
         s.maxiter = maxiter;
-        s.abs_tol = tol * beta;
+        s.abs_tol = tol * s.b_norm;
         s.rel_tol = tol;
         s.stop = STOP_NONE;
         s.prev_rho = 1.0;
         s.prev_rho_bar = 1.0;
         s.beta_prev_inv = 1.0;
-        if ((uint32_t)k >= k_used || beta == 0.0) {
+        s.stale_window = stale_window;
+        s.stale_thr = stale_thr;
+        s.stale_prev = __longlong_as_double(0x7ff8000000000000ll);   // NaN: no ratio before the first step
+        if ((uint32_t)k >= k_used) {
             s.done = 1;
             s.stop = STOP_ZERO_RHS;
+        } else if (warm && !isfinite(beta)) {
+            s.done = 1;
+            s.err = ERR_WARM_NONFINITE;
+            atomicCAS(&ctl->err, 0, ERR_WARM_NONFINITE);
+        } else if (beta == 0.0) {
+            s.done = 1;
+            s.stop = warm ? STOP_WARM_EXACT : STOP_ZERO_RHS;
         }
         st[k] = s;
     }
@@ -1169,6 +1202,100 @@ k_norm_b(uint32_t n, const double* __restrict__ b, const double* bmax, ColState*
     ctl->k5_skip = 0;
     ctl->bodies_left = (int)min((long long)maxiter / 2 + 2, (long long)INT_MAX);
     ctl->bodies_run = 0;
+}
+
+// Warm start (mlsmr, lsmr.rs:232-292): x0 (column-major n_dofs x k_used)
+// into the interleaved layout, with a check that every entry is finite.
+template <int K>
+__global__ void k_load_x0(uint32_t nd, uint32_t k_used, const double* __restrict__ x0, double* __restrict__ out,
+                          int* nonfinite) {
+    int bad = 0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nd; j += gridDim.x * blockDim.x) {
+        double v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            v[k] = (uint32_t)k < k_used ? x0[(size_t)k * nd + j] : 0.0;
+            if (!isfinite(v[k])) bad = 1;
+        }
+        stk<K, double>(out + (size_t)j * K, v);
+    }
+    if (bad) atomicExch(nonfinite, 1);
+}
+
+// b <- b - A x0 (A = W^{1/2} D; operator apply, gather.rs:10-109) and the new
+// max |b| per column for the scaled norm of k_norm_b
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS)
+k_warm_rhs(OpParams p, const double* __restrict__ x0, double* __restrict__ b, double* partials, unsigned* counter,
+           double* out_max) {
+    double mx[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) mx[k] = 0.0;
+    const uint32_t stride = gridDim.x * blockDim.x * 4;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * 4; base < p.n; base += stride) {
+        const int nr = (int)min(4u, p.n - base);
+        double s[4][K];
+        rows4_dx<K>(p, base, nr, x0, s);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (r >= nr) continue;
+            const double w = p.sqrt_w ? p.sqrt_w[base + r] : 1.0;
+            double o[K];
+            ldk<K, double>(b + (size_t)(base + r) * K, o);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                o[k] -= p.sqrt_w ? w * s[r][k] : s[r][k];
+                mx[k] = fmax(mx[k], fabs(o[k]));   // NaN-free unless A x0 overflowed
+                if (!isfinite(o[k])) mx[k] = o[k];
+            }
+            stk<K, double>(b + (size_t)(base + r) * K, o);
+        }
+    }
+    __shared__ double sm[32][K];
+    __shared__ int is_last;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double m = mx[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double q = __shfl_xor_sync(0xffffffffu, m, o);
+            m = isfinite(m) ? (isfinite(q) ? fmax(m, q) : q) : m;
+        }
+        if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5][k] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < K; ++k) {
+            double m = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = isfinite(m) ? (isfinite(sm[w][k]) ? fmax(m, sm[w][k]) : sm[w][k]) : m;
+            partials[(size_t)blockIdx.x * K + k] = m;
+        }
+        __threadfence();
+        is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (int k = wid; k < K; k += (int)(blockDim.x >> 5)) {
+            double m = 0;
+            for (unsigned blk = lane; blk < gridDim.x; blk += 32) {
+                const double q = __ldcg(&partials[(size_t)blk * K + k]);
+                m = isfinite(m) ? (isfinite(q) ? fmax(m, q) : q) : m;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double q = __shfl_xor_sync(0xffffffffu, m, o);
+                m = isfinite(m) ? (isfinite(q) ? fmax(m, q) : q) : m;
+            }
+            if (lane == 0) out_max[k] = m;
+        }
+        if (threadIdx.x == 0) *counter = 0;
+    }
+}
+
+// x <- x + x0 after a warm-started solve (mlsmr, lsmr.rs:293-297)
+template <int K>
+__global__ void k_add_x0(uint32_t nd, double* __restrict__ x, const double* __restrict__ x0) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nd * K; j += gridDim.x * blockDim.x) x[j] += x0[j];
 }
 
 template <int K>

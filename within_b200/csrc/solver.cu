@@ -33,6 +33,7 @@
 #include "kernels.cuh"
 #include "refine.cuh"
 #include "rowsweep.cuh"
+#include "tsweep.cuh"
 
 using namespace wgpu;
 
@@ -121,6 +122,14 @@ void launch_sr(const F& f, const DevPlan& p, uint32_t lo, uint32_t hi, const int
 }
 
 int k_bucket(uint64_t k) { return k <= 1 ? 1 : k <= 2 ? 2 : k <= 4 ? 4 : 8; }
+
+// MlsmrOptions extras of one solve (lsmr.rs:155-171): warm start (device,
+// column-major n_dofs x k) and the Staleness escalation rule
+struct SolveExt {
+    const double* x0 = nullptr;
+    uint64_t stale_window = 0;
+    double stale_threshold = 0.0;
+};
 
 }  // namespace
 
@@ -483,6 +492,7 @@ struct within_solver {
     struct Work {
         bool ready = false;
         double *u, *b, *yint, *v, *p, *h, *hb, *x, *dm;
+        double* x0 = nullptr;   // warm start, interleaved (allocated on first use)
         double* partials;
         unsigned* counter;
         double* bmax;
@@ -530,7 +540,14 @@ struct within_solver {
         bool simple = false;                 // every term intercept-only: the specialised sweep
         double* atu = nullptr;               // n_dofs * K raw A^T u (LSMR)
         size_t smem_f = 0;                   // shared memory of the FP32 normal-operator mode
+        int grid = 0;                        // blocks of every sweep launch (the ranges are cut for it)
+        // staged sweep (tsweep.cuh): used for the FP64 adjoint and LSMR-step modes
+        bool ts = false;
+        TsSlots ts_slots{};
+        int ts_nq = 0;
+        size_t ts_smem = 0;
     } rsw[4];
+    int* sweep_err = nullptr;   // device flag of a timed-out wait in a sweep outside the LSMR loop
     // per column bucket, the LSMR step's operator path:
     // 0 gather + full segmented-reduction scatter, 2 warp-range row sweep (rowsweep.cuh)
     int path[4] = {0, 0, 0, 0};
@@ -571,6 +588,96 @@ void ensure_scatter(within_solver& s, int K) {
     s.scatter_ready[ki] = true;
 }
 
+// The staged sweep instantiations (K = 1): mode 0 (adjoint) and 1 (LSMR
+// step) for every class layout of at most three terms; nullptr when the
+// layout has none.
+using TsKernel = void (*)(OpParams, RwParams, TsSlots, const double*, double*, ColState*, Ctl*, int*);
+template <int MODE, int NQ, int NRUN, int NHIST, bool WTD>
+TsKernel ts_pick() {
+    if constexpr (NRUN + NHIST <= NQ) return k_tsweep<1, MODE, NQ, NRUN, NHIST, WTD>;
+    else return nullptr;
+}
+template <int MODE, int NQ, int NRUN, bool WTD>
+TsKernel ts_pick_h(int nhist) {
+    switch (nhist) {
+        case 0: return ts_pick<MODE, NQ, NRUN, 0, WTD>();
+        case 1: return ts_pick<MODE, NQ, NRUN, 1, WTD>();
+        default: return ts_pick<MODE, NQ, NRUN, 2, WTD>();
+    }
+}
+template <int MODE, int NQ, bool WTD>
+TsKernel ts_pick_r(int nrun, int nhist) {
+    return nrun == 1 ? ts_pick_h<MODE, NQ, 1, WTD>(nhist) : ts_pick_h<MODE, NQ, 2, WTD>(nhist);
+}
+template <int MODE, bool WTD>
+TsKernel ts_pick_q(int nq, int nrun, int nhist) {
+    switch (nq) {
+        case 1: return ts_pick_r<MODE, 1, WTD>(nrun, nhist);
+        case 2: return ts_pick_r<MODE, 2, WTD>(nrun, nhist);
+        default: return ts_pick_r<MODE, 3, WTD>(nrun, nhist);
+    }
+}
+TsKernel ts_kernel(int mode, int nq, int nrun, int nhist, bool wtd) {
+    if (nq < 1 || nq > TS_MAXQ || nrun < 1 || nrun > RW_MAX_RUN || nhist < 0 || nhist > RW_MAX_HIST) return nullptr;
+    if (mode == 0) return wtd ? ts_pick_q<0, true>(nq, nrun, nhist) : ts_pick_q<0, false>(nq, nrun, nhist);
+    return wtd ? ts_pick_q<1, true>(nq, nrun, nhist) : ts_pick_q<1, false>(nq, nrun, nhist);
+}
+
+// The staged gather / demeaning instantiations (K = 1, intercept-only, at
+// most three terms); nullptr outside them.
+using TgKernel = void (*)(OpParams, const double*, const double*, double*, const int*, int*);
+template <bool WTD, bool DEMEAN>
+TgKernel tg_pick(int nq) {
+    switch (nq) {
+        case 1: return k_tgather<1, WTD, DEMEAN>;
+        case 2: return k_tgather<2, WTD, DEMEAN>;
+        case 3: return k_tgather<3, WTD, DEMEAN>;
+        default: return nullptr;
+    }
+}
+TgKernel tg_kernel(int nq, bool wtd, bool demean) {
+    if (demean) return tg_pick<false, true>(nq);
+    return wtd ? tg_pick<true, false>(nq) : tg_pick<false, false>(nq);
+}
+size_t tg_smem(int nq, bool wtd, bool demean) {
+    const size_t stage = (size_t)TG_CH * (4 * nq + (demean ? 8 : 0) + (wtd && !demean ? 8 : 0));
+    return (size_t)RW_WARPS * TS_STAGES * (stage + sizeof(uint64_t));
+}
+// whether the staged gather applies to this solver's design (WITHIN_TSWEEP=0: never)
+bool tg_applies(const within_solver& s) {
+    if (const char* e = getenv("WITHIN_TSWEEP"))
+        if (atoi(e) == 0) return false;
+    if (s.design.terms.size() > (size_t)TS_MAXQ || s.design.terms.empty()) return false;
+    for (const Term& T : s.design.terms)
+        if (T.cols.size() != 1 || T.cols[0] >= 0) return false;
+    return true;
+}
+// y = W^{1/2} D x (demean: out = yint - D x) through the staged gather when it
+// applies and the output is 16-byte aligned; returns false otherwise
+bool launch_tgather(within_solver& s, const double* x, const double* yint, double* out, bool demean,
+                    const int* skip, int* err, cudaStream_t st) {
+    if (!tg_applies(s) || ((uintptr_t)out & 15) != 0) return false;
+    const int nq = (int)s.design.terms.size();
+    const bool wtd = s.op.sqrt_w != nullptr && !demean;
+    TgKernel f = tg_kernel(nq, wtd, demean);
+    if (!f) return false;
+    const size_t sm = tg_smem(nq, wtd, demean);
+    {
+        static std::mutex mu;
+        static std::vector<std::pair<int, TgKernel>> done;
+        std::lock_guard<std::mutex> g(mu);
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        if (std::find(done.begin(), done.end(), std::make_pair(dev, f)) == done.end()) {
+            CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tg_smem(3, true, true)));
+            done.emplace_back(dev, f);
+        }
+    }
+    f<<<TG_GRID, RW_THREADS, sm, st>>>(s.op, x, yint, out, skip, err);
+    ++g_launches;
+    return true;
+}
+
 // Classifies the terms for the warp-range row sweep and builds its tables
 // (rowsweep.cuh): range bases of the run ordinals, the crossing-run fix-ups,
 // the level-sorted run combines and the remaining full-resolution terms.
@@ -582,34 +689,87 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
     const uint64_t n = D.n_obs;
     Arena& A = s.arena;
     RwParams& rp = rk.rp;
-    const uint64_t G = (uint64_t)rw_grid<K>() * RW_WARPS;
+    const int Q = (int)D.terms.size();
+    // term classes: hist (few coefficients), run (sorted, or few runs), rest
+    enum { CLS_REST = 0, CLS_RUN = 1, CLS_HIST = 2 };
+    std::vector<int> cls(Q, CLS_REST);
+    std::vector<uint64_t> n_runs(Q, 0);
+    {
+        int nh = 0, nr = 0, nbk = 0;
+        for (int t = 0; t < Q; ++t) {
+            const Term& T = D.terms[t];
+            const auto& codes = D.codes[t];
+            const int ncol = (int)T.cols.size();
+            if (nh < RW_MAX_HIST && (uint64_t)nbk + (uint64_t)T.n_levels * ncol <= RW_MAX_BUCKETS) {
+                cls[t] = CLS_HIST;
+                ++nh;
+                nbk += (int)(T.n_levels * ncol);
+                continue;
+            }
+            uint64_t runs = 0;
+            for (uint64_t i = 0; i < n; ++i) runs += (i == 0 || codes[i] != codes[i - 1]) ? 1 : 0;
+            n_runs[t] = runs;
+            if (nr < RW_MAX_RUN && ncol <= rw_max_cols<K>() && (T.sorted != 0 || runs * 3 <= n)) {
+                cls[t] = CLS_RUN;
+                ++nr;
+            }
+        }
+    }
+    bool simple = true;
+    for (const Term& T : D.terms)
+        if (T.cols.size() != 1 || T.cols[0] >= 0) simple = false;
+    // the staged sweep: intercept-only, at most three terms, one run term or
+    // more, its shared memory within two blocks per SM (WITHIN_TSWEEP=0: never)
+    {
+        int nrun = 0, nhist = 0, nbk = 0;
+        for (int t = 0; t < Q; ++t) {
+            nrun += cls[t] == CLS_RUN;
+            nhist += cls[t] == CLS_HIST;
+            if (cls[t] == CLS_HIST) nbk += (int)D.terms[t].n_levels;
+        }
+        bool ok = K == 1 && simple && Q <= TS_MAXQ && nrun >= 1;
+        if (const char* e = getenv("WITHIN_TSWEEP"))
+            if (atoi(e) == 0) ok = false;
+        const size_t sm = ts_smem_bytes<K>(nbk, nhist, Q, s.op.sqrt_w != nullptr);
+        if (ok && sm <= TS_SMEM_CAP) {
+            rk.ts = true;
+            rk.ts_nq = Q;
+            rk.ts_smem = sm;
+            int k = 0;
+            for (int t = 0; t < Q; ++t)
+                if (cls[t] == CLS_RUN) rk.ts_slots.term[k++] = t;
+            for (int t = 0; t < Q; ++t)
+                if (cls[t] == CLS_HIST) rk.ts_slots.term[k++] = t;
+            for (int t = 0; t < Q; ++t)
+                if (cls[t] == CLS_REST) rk.ts_slots.term[k++] = t;
+        }
+    }
+    rk.grid = rk.ts ? TS_GRID : rw_grid<K>();
+    const uint64_t G = (uint64_t)rk.grid * RW_WARPS;
     const uint64_t CH = rw_chunk<K>();
     uint64_t rpr = (n + G - 1) / G;
     rpr = std::max<uint64_t>(CH, (rpr + CH - 1) / CH * CH);
     rp.rows_per_range = (uint32_t)rpr;
     std::vector<RwFix> fixes;
     size_t first_prob = 0;
-    for (int t = 0; t < (int)D.terms.size(); ++t) {
+    for (int t = 0; t < Q; ++t) {
         const Term& T = D.terms[t];
         const auto& codes = D.codes[t];
         const int ncol = (int)T.cols.size();
         const size_t probs_before = first_prob;
         first_prob += (size_t)ncol;
-        if (rp.n_hist < RW_MAX_HIST && (uint64_t)rp.n_buckets + (uint64_t)T.n_levels * ncol <= RW_MAX_BUCKETS) {
+        if (cls[t] == CLS_HIST) {
             rp.hist[rp.n_hist++] = RwHist{t, rp.n_buckets};
             rp.n_buckets += (int)(T.n_levels * ncol);
             continue;
         }
-        // run heads per range
-        std::vector<uint32_t> cnt(G, 0);
-        uint64_t runs = 0;
-        for (uint64_t i = 0; i < n; ++i)
-            if (i == 0 || codes[i] != codes[i - 1]) {
-                ++cnt[i / rpr];
-                ++runs;
-            }
-        const bool sorted_runs = T.sorted != 0;
-        if (rp.n_run < RW_MAX_RUN && ncol <= rw_max_cols<K>() && (sorted_runs || runs * 3 <= n)) {
+        if (cls[t] == CLS_RUN) {
+            // run heads per range
+            std::vector<uint32_t> cnt(G, 0);
+            const uint64_t runs = n_runs[t];
+            for (uint64_t i = 0; i < n; ++i)
+                if (i == 0 || codes[i] != codes[i - 1]) ++cnt[i / rpr];
+            const bool sorted_runs = T.sorted != 0;
             const int j = rp.n_run++;
             RwRun& rr = rp.run[j];
             rr.term = t;
@@ -678,7 +838,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
     rk.simple = true;
     for (const Term& T : D.terms)
         if (T.cols.size() != 1 || T.cols[0] >= 0) rk.simple = false;
-    rp.part = A.alloc<double>((size_t)rw_grid<K>() * (K + (size_t)rp.n_buckets * K));
+    rp.part = A.alloc<double>((size_t)rk.grid * (K + (size_t)rp.n_buckets * K));
     rp.counter = A.alloc<unsigned>(1);
     // histogram shared memory per bin type (FP64 modes / the FP32 normal operator)
     bool pv;
@@ -715,6 +875,15 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
             CK(cudaFuncSetAttribute(k_rowsweep<K, 1, double, true>, attr, cap));
             CK(cudaFuncSetAttribute(k_rowsweep<K, 2, float, true>, attr, cap));
             CK(cudaFuncSetAttribute(k_rowsweep<K, 3, double, true>, attr, cap));
+            if constexpr (K == 1) {
+                for (int mode = 0; mode < 2; ++mode)
+                    for (int nq = 1; nq <= TS_MAXQ; ++nq)
+                        for (int nrun = 1; nrun <= RW_MAX_RUN; ++nrun)
+                            for (int nhist = 0; nhist <= RW_MAX_HIST; ++nhist)
+                                for (int wtd = 0; wtd < 2; ++wtd)
+                                    if (auto f = ts_kernel(mode, nq, nrun, nhist, wtd != 0))
+                                        CK(cudaFuncSetAttribute(f, attr, (int)TS_SMEM_CAP));
+            }
             done.emplace_back(dev, K);
         }
     }
@@ -737,22 +906,39 @@ void ensure_rowsweep_f(within_solver& s) {
     rk.rest_probs_f = s.arena.upload(pf);
 }
 
+// `err`: device flag of a timed-out wait of the staged sweep (the LSMR
+// loop's ctl->err, or the solver's sweep_err)
 template <int K, int MODE, class T>
 void launch_rowsweep(within_solver& s, within_solver::RowSweepK& rk, const OpParamsT<T>& op, void* atu, const T* v,
                      T* u, ColState* cur, Ctl* ctl, const int* skip, int store, cudaStream_t st,
-                     const T* rhs = nullptr, double* sq_out = nullptr, int sq_stride = 0) {
+                     const T* rhs = nullptr, double* sq_out = nullptr, int sq_stride = 0, int* err = nullptr) {
     RwParams rp = rk.rp;
     rp.atu = atu;
     constexpr int BIN_BYTES = MODE == 2 ? (int)sizeof(T) : 8;
     bool priv;
     const size_t smem = rw_smem_bytes<K, BIN_BYTES>(rp.n_buckets, rp.n_hist, priv);
     rp.hist_private = priv ? 1 : 0;
-    if (rk.simple)
-        k_rowsweep<K, MODE, T, true><<<rw_grid<K>(), RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
+    bool staged = false;
+    if constexpr (K == 1 && (MODE == 0 || MODE == 1) && sizeof(T) == 8) {
+        // bulk copies read u from 16-byte aligned chunk starts
+        if (rk.ts && ((uintptr_t)u & 15) == 0 && (MODE == 1 || !skip)) {
+            TsKernel f = ts_kernel(MODE, rk.ts_nq, rp.n_run, rp.n_hist, op.sqrt_w != nullptr);
+            if (f) {
+                rp.hist_private = 1;
+                int* e = err ? err : (ctl ? &ctl->err : s.sweep_err);
+                f<<<rk.grid, RW_THREADS, rk.ts_smem, st>>>(op, rp, rk.ts_slots, v, u, cur, ctl, e);
+                staged = true;
+            }
+        }
+    }
+    if (!staged) {
+        if (rk.simple)
+            k_rowsweep<K, MODE, T, true><<<rk.grid, RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
+                                                                            rhs, sq_out, sq_stride);
+        else
+            k_rowsweep<K, MODE, T, false><<<rk.grid, RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
                                                                              rhs, sq_out, sq_stride);
-    else
-        k_rowsweep<K, MODE, T, false><<<rw_grid<K>(), RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
-                                                                              rhs, sq_out, sq_stride);
+    }
     ++g_launches;
     if (rp.n_fix) {   // the runs crossing range boundaries, after every range has written its partials
         const unsigned fb = (rp.n_fix + 255) / 256;
@@ -937,24 +1123,40 @@ bool build_loop_graph(within_solver& s, within_solver::Work& w) {
 template <int K>
 void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_t k_used, double tol,
               uint64_t maxiter, double* X_out, double* D_out, within_solve_stats* stats, cudaStream_t st,
-              double t_setup0) {
+              double t_setup0, const SolveExt& ext = SolveExt{}, int32_t* stop_out = nullptr) {
     const uint32_t n = (uint32_t)s.n_obs, nd = (uint32_t)s.n_dofs;
     CK(cudaMemsetAsync(w.nonfinite, 0, sizeof(int), st));
     CK(cudaMemsetAsync(w.ctl, 0, sizeof(Ctl), st));
     k_load_rhs<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, k_used, Y, s.perm, s.op.sqrt_w, w.yint, w.b,
                                                     w.partials, w.counter, w.bmax, w.nonfinite);
+    if (ext.x0) {   // warm start: x0 into the interleaved layout (finite check)
+        if (!w.x0) w.x0 = s.arena.alloc<double>(s.n_dofs * K);
+        k_load_x0<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, k_used, ext.x0, w.x0, w.nonfinite);
+        ++g_launches;
+    }
     int nonfinite = 0;
     CK(cudaMemcpyAsync(&nonfinite, w.nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (nonfinite) throw WError(ERR_INVALID, "response must be finite (a non-finite value was found)");
+    if (nonfinite)
+        throw WError(ERR_INVALID, ext.x0 ? "response and warm start must be finite (a non-finite value was found)"
+                                         : "response must be finite (a non-finite value was found)");
     const double t_solve0 = now_s();
     k_norm_b<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
-                                                  w.ctl, w.partials, w.counter);
+                                                  w.ctl, w.partials, w.counter, 0, (int)ext.stale_window,
+                                                  ext.stale_threshold);
+    if (ext.x0) {   // b <- b - A x0, tolerances kept relative to the original ||b||
+        k_warm_rhs<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, w.x0, w.b, w.partials, w.counter, w.bmax);
+        k_norm_b<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
+                                                      w.ctl, w.partials, w.counter, 1, (int)ext.stale_window,
+                                                      ext.stale_threshold);
+        g_launches += 2;
+    }
     k_scale_u<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, w.b, w.u, w.st);
     if (s.path[kidx(K)] == 2) {   // p~ = A^T u through the row sweep (adjoint mode) and its rest
         auto& rk = s.rsw[kidx(K)];
         CK(cudaMemsetAsync(w.p, 0, (size_t)nd * K * sizeof(double), st));   // levels no row reaches stay 0
-        launch_rowsweep<K, 0, double>(s, rk, s.op, w.p, nullptr, w.u, nullptr, nullptr, nullptr, 0, st);
+        launch_rowsweep<K, 0, double>(s, rk, s.op, w.p, nullptr, w.u, nullptr, nullptr, nullptr, 0, st, nullptr,
+                                      nullptr, 0, &w.ctl->err);
         rowsweep_rest<K, double>(s, rk, w.u, w.p, nullptr, st);
     } else {
         scatter<K, 0>(s, w.u, w.p, w.st, nullptr, st);
@@ -1005,10 +1207,20 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
     }
     if (ctl.err == 5)
         throw WError(ERR_INDEFINITE, "mlsmr: preconditioner not positive definite (<v, Mv> < 0)");
+    if (ctl.err == ERR_WAIT_TIMEOUT)
+        throw WError(ERR_CUDA, "row sweep: a bulk copy into shared memory did not complete within 1 s");
+    if (ctl.err == ERR_WARM_NONFINITE)
+        throw WError(ERR_INVALID, "warm-start residual b - A x0 has a non-finite norm");
     const double t_solve1 = now_s();
     // results
-    k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, w.x, w.yint, w.dm);
-    ++g_launches;
+    if (ext.x0) {
+        k_add_x0<K><<<grid_for((uint64_t)nd * K, 256, 148 * 8), 256, 0, st>>>(nd, w.x, w.x0);
+        ++g_launches;
+    }
+    if (K != 1 || !launch_tgather(s, w.x, w.yint, w.dm, true, nullptr, s.sweep_err, st)) {
+        k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, w.x, w.yint, w.dm);
+        ++g_launches;
+    }
     if (D_out) {
         k_store_obs<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, k_used, w.dm, s.perm, D_out);
         ++g_launches;
@@ -1022,19 +1234,25 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
     // both buffers hold identical done states for finished columns, so read
     // the one with the larger iteration count.
     ColState a[8], b2[8];
+    int werr = 0;
     CK(cudaMemcpyAsync(a, w.st, sizeof(ColState) * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(b2, w.st + 8, sizeof(ColState) * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&werr, s.sweep_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (werr) throw WError(ERR_CUDA, "staged gather: a bulk copy into shared memory did not complete within 1 s");
     for (int k = 0; k < 8; ++k) fin[k] = a[k].itn >= b2[k].itn ? a[k] : b2[k];
+    if (stop_out)
+        for (uint32_t k = 0; k < k_used; ++k) stop_out[k] = fin[k].stop;
     const double t_end = now_s();
     if (stats)
         for (uint32_t k = 0; k < k_used; ++k) {
             const ColState& c = fin[k];
             within_solve_stats& o = stats[k];
             o.converged = (c.stop == STOP_RESID || c.stop == STOP_NORMAL || c.stop == STOP_ZERO_RHS ||
-                           c.stop == STOP_INIT_ZERO) ? 1 : 0;
+                           c.stop == STOP_INIT_ZERO || c.stop == STOP_WARM_EXACT) ? 1 : 0;
             o.iterations = (uint64_t)c.itn;
-            o.residual = (c.stop == STOP_ZERO_RHS || c.stop == STOP_INIT_ZERO) ? 0.0 : fabs(c.zeta_bar) / c.zeta0;
+            o.residual = (c.stop == STOP_ZERO_RHS || c.stop == STOP_INIT_ZERO || c.stop == STOP_WARM_EXACT)
+                             ? 0.0 : fabs(c.zeta_bar) / c.zeta0;
             o.time_setup = t_solve0 - t_setup0;
             o.time_solve = t_solve1 - t_solve0;
             o.time_total = t_end - t_setup0;
@@ -1316,8 +1534,10 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
     if (ctl.err == 5)
         throw WError(ERR_INDEFINITE, "mixed solve: preconditioner not positive definite (<g, M g> < 0)");
     const double t_solve1 = now_s();
-    k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, m.x64, w.yint, w.dm);
-    ++g_launches;
+    if (K != 1 || !launch_tgather(s, m.x64, w.yint, w.dm, true, nullptr, s.sweep_err, st)) {
+        k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, m.x64, w.yint, w.dm);
+        ++g_launches;
+    }
     if (D_out) {
         k_store_obs<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, k_used, w.dm, s.perm, D_out);
         ++g_launches;
@@ -1326,7 +1546,10 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
         k_store_dofs<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, k_used, m.x64, X_out);
         ++g_launches;
     }
+    int werr = 0;
+    CK(cudaMemcpyAsync(&werr, s.sweep_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (werr) throw WError(ERR_CUDA, "staged gather: a bulk copy into shared memory did not complete within 1 s");
     const double t_end = now_s();
     if (stats)
         for (uint32_t k = 0; k < k_used; ++k) {
@@ -1364,11 +1587,13 @@ void set_ring(within_solver& s, within_solver::Work& w, int K, uint64_t local_si
 
 void dispatch_solve(within_solver& s, const double* Y_dev, uint64_t k, double tol, uint64_t maxiter,
                     double* X_dev, double* D_dev, within_solve_stats* stats, cudaStream_t st,
-                    uint64_t local_size = 0) {
+                    uint64_t local_size = 0, const SolveExt& ext = SolveExt{}, int32_t* stop_out = nullptr) {
     const double t0 = now_s();
     if (local_size && s.precision == WITHIN_PRECISION_MIXED)
         throw WError(ERR_UNSUPPORTED, "local_size (windowed reorthogonalisation) applies to the FP64 LSMR solve; "
                                       "the mixed-precision solve refines instead");
+    if ((ext.x0 || ext.stale_window) && s.precision == WITHIN_PRECISION_MIXED)
+        throw WError(ERR_UNSUPPORTED, "warm starts and escalation apply to the FP64 LSMR solve");
     for (uint64_t c0 = 0; c0 < k; c0 += 8) {
         const uint32_t kk = (uint32_t)std::min<uint64_t>(8, k - c0);
         const int K = k_bucket(kk);
@@ -1378,6 +1603,9 @@ void dispatch_solve(within_solver& s, const double* Y_dev, uint64_t k, double to
         double* X = X_dev ? X_dev + c0 * s.n_dofs : nullptr;
         double* D = D_dev ? D_dev + c0 * s.n_obs : nullptr;
         within_solve_stats* S = stats ? stats + c0 : nullptr;
+        SolveExt e = ext;
+        if (e.x0) e.x0 += c0 * s.n_dofs;
+        int32_t* so = stop_out ? stop_out + c0 : nullptr;
         if (s.precision == WITHIN_PRECISION_MIXED) {
             switch (K) {
                 case 1: run_mixed<1>(s, Y, kk, tol, maxiter, X, D, S, st, t0); break;
@@ -1388,10 +1616,10 @@ void dispatch_solve(within_solver& s, const double* Y_dev, uint64_t k, double to
             continue;
         }
         switch (K) {
-            case 1: run_lsmr<1>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
-            case 2: run_lsmr<2>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
-            case 4: run_lsmr<4>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
-            default: run_lsmr<8>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0); break;
+            case 1: run_lsmr<1>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0, e, so); break;
+            case 2: run_lsmr<2>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0, e, so); break;
+            case 4: run_lsmr<4>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0, e, so); break;
+            default: run_lsmr<8>(s, w, Y, kk, tol, maxiter, X, D, S, st, t0, e, so); break;
         }
     }
 }
@@ -1435,6 +1663,7 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
     auto s = std::make_unique<within_solver>();
     s->device = device;
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->sweep_err = s->arena.alloc<int>(1);
     std::vector<EffectIn> effs;
     for (size_t e = 0; e < d->levels.size(); ++e) {
         EffectIn ef;
@@ -1580,6 +1809,86 @@ void par_memcpy(void* dst, const void* src, size_t bytes) {
     for (auto& th : pool) th.join();
 }
 
+// Whether a host pointer is page-locked memory the DMA engines can read or
+// write directly (cudaHostAlloc / cudaHostRegister, torch pin_memory).
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Host <-> device copies of the host entry points.  A page-locked caller
+// buffer is copied directly by one cudaMemcpyAsync; a pageable one goes
+// through the solver's two pinned staging slots in chunks, the host copy of
+// one chunk (on host threads) overlapping the DMA of the other.
+struct Staging {
+    within_solver& s;
+    cudaStream_t st;
+    static constexpr size_t CHUNK = (size_t)16 << 20;   // bytes per slot
+    char* slot[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    Staging(within_solver& s_, cudaStream_t st_) : s(s_), st(st_) {}
+    ~Staging() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    void ensure() {
+        if (!s.pin) {
+            CK(cudaMallocHost(&s.pin, 2 * CHUNK));
+            s.pin_n = 2 * CHUNK / sizeof(double);
+        }
+        slot[0] = (char*)s.pin;
+        slot[1] = (char*)s.pin + CHUNK;
+        for (auto& e : ev)
+            if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    void h2d(void* dst, const void* src, size_t bytes) {
+        if (!bytes) return;
+        if (is_pinned(src)) {
+            CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+            return;
+        }
+        ensure();
+        for (size_t off = 0, i = 0; off < bytes; off += CHUNK, ++i) {
+            const int j = (int)(i & 1);
+            const size_t len = std::min(CHUNK, bytes - off);
+            if (i >= 2) CK(cudaEventSynchronize(ev[j]));   // the slot's previous DMA has read it
+            par_memcpy(slot[j], (const char*)src + off, len);
+            CK(cudaMemcpyAsync((char*)dst + off, slot[j], len, cudaMemcpyHostToDevice, st));
+            CK(cudaEventRecord(ev[j], st));
+        }
+    }
+    // device -> host; returns after the data is in dst
+    void d2h(void* dst, const void* src, size_t bytes) {
+        if (!bytes) return;
+        if (is_pinned(dst)) {
+            CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            return;
+        }
+        ensure();
+        const size_t n_chunks = (bytes + CHUNK - 1) / CHUNK;
+        auto issue = [&](size_t i) {
+            const int j = (int)(i & 1);
+            const size_t off = i * CHUNK, len = std::min(CHUNK, bytes - off);
+            CK(cudaMemcpyAsync(slot[j], (const char*)src + off, len, cudaMemcpyDeviceToHost, st));
+            CK(cudaEventRecord(ev[j], st));
+        };
+        issue(0);
+        if (n_chunks > 1) issue(1);
+        for (size_t i = 0; i < n_chunks; ++i) {
+            const int j = (int)(i & 1);
+            const size_t off = i * CHUNK, len = std::min(CHUNK, bytes - off);
+            CK(cudaEventSynchronize(ev[j]));
+            par_memcpy((char*)dst + off, slot[j], len);
+            if (i + 2 < n_chunks) issue(i + 2);   // the slot is free again
+        }
+    }
+};
+
 void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr_options* opts, double* X,
                 double* Dm, within_solve_stats* stats) {
     double tol;
@@ -1588,17 +1897,6 @@ void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr
     std::lock_guard<std::mutex> g(s.mu);
     set_device(s.device);
     const uint64_t n = s.n_obs, nd = s.n_dofs;
-    size_t need = (size_t)k * (2 * n + nd);
-    if (s.pin_n < need) {
-        if (s.pin) cudaFreeHost(s.pin);
-        s.pin = nullptr;
-        CK(cudaMallocHost(&s.pin, need * sizeof(double)));
-        s.pin_n = need;
-    }
-    double* pY = s.pin;
-    double* pD = s.pin + k * n;
-    double* pX = s.pin + 2 * k * n;
-    par_memcpy(pY, Y, k * n * sizeof(double));
     double* dY = nullptr;
     double* dX = nullptr;
     double* dD = nullptr;
@@ -1614,14 +1912,12 @@ void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr
             cudaFreeAsync(c, st);
         }
     } fr{s.stream, dY, dX, dD};
-    CK(cudaMemcpyAsync(dY, pY, k * n * sizeof(double), cudaMemcpyHostToDevice, s.stream));
-    dispatch_solve(s, dY, k, tol, maxiter, dX, dD, stats, s.stream, ls);
-    CK(cudaMemcpyAsync(pD, dD, k * n * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
-    CK(cudaMemcpyAsync(pX, dX, k * nd * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
-    CK(cudaStreamSynchronize(s.stream));
-    if (Dm) par_memcpy(Dm, pD, k * n * sizeof(double));
+    Staging io(s, s.stream);
+    io.h2d(dY, Y, k * n * sizeof(double));
+    dispatch_solve(s, dY, k, tol, maxiter, X ? dX : nullptr, Dm ? dD : nullptr, stats, s.stream, ls);
+    if (Dm) io.d2h(Dm, dD, k * n * sizeof(double));
     if (X) {
-        par_memcpy(X, pX, k * nd * sizeof(double));
+        io.d2h(X, dX, k * nd * sizeof(double));
         if (s.reparam.active())
             for (uint64_t j = 0; j < k; ++j) s.reparam.back_transform(X + j * nd);
     }
@@ -1876,6 +2172,42 @@ int within_solver_solve_batch_device(within_solver* s, const double* Y_dev, uint
     });
 }
 
+int within_solver_solve_batch_device_ext(within_solver* s, const double* Y_dev, uint64_t k,
+                                         const within_lsmr_options* opts, const within_solve_ext* ext,
+                                         double* X_dev, double* D_dev, within_solve_stats* stats,
+                                         int32_t* stop_reason, void* stream) {
+    return guarded([&] {
+        double tol;
+        uint64_t maxiter, ls;
+        validate_opts(opts, tol, maxiter, ls);
+        SolveExt e;
+        if (ext) {
+            e.x0 = ext->x0_dev;
+            e.stale_window = ext->stale_window;
+            e.stale_threshold = ext->stale_threshold;
+            if (e.stale_window && !(e.stale_threshold >= 0.0 && e.stale_threshold < 1.0))
+                throw WError(ERR_INVALID, "staleness threshold must be in [0, 1), got " +
+                                              std::to_string(e.stale_threshold));
+            if (e.stale_window > (uint64_t)INT_MAX) throw WError(ERR_INVALID, "staleness window too large");
+        }
+        if (k == 0) return;
+        std::lock_guard<std::mutex> g(s->mu);
+        set_device(s->device);
+        if (e.x0 && s->reparam.active())
+            throw WError(ERR_UNSUPPORTED, "warm starts are supported for designs without slope terms");
+        cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+        dispatch_solve(*s, Y_dev, k, tol, maxiter, X_dev, D_dev, stats, st, ls, e, stop_reason);
+        if (X_dev && s->reparam.active()) {
+            std::vector<double> hx(k * s->n_dofs);
+            CK(cudaMemcpyAsync(hx.data(), X_dev, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (uint64_t j = 0; j < k; ++j) s->reparam.back_transform(hx.data() + j * s->n_dofs);
+            CK(cudaMemcpyAsync(X_dev, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+    });
+}
+
 int within_solve(const within_design* design, const double* y, const double* weights,
                  const within_lsmr_options* opts, const within_precond_config* cfg, double* x_out,
                  double* demeaned_out, within_solve_stats* stats) {
@@ -1905,10 +2237,17 @@ int within_solver_operator_apply(within_solver* s, const double* x_dev, double* 
         std::lock_guard<std::mutex> g(s->mu);
         set_device(s->device);
         cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
-        k_apply<1><<<grid_for(s->n_obs, 256, 148 * 16), 256, 0, st>>>(s->op, x_dev, y_dev);
-        ++g_launches;
+        if (!launch_tgather(*s, x_dev, nullptr, y_dev, false, nullptr, s->sweep_err, st)) {
+            k_apply<1><<<grid_for(s->n_obs, 256, 148 * 16), 256, 0, st>>>(s->op, x_dev, y_dev);
+            ++g_launches;
+        }
         CK(cudaGetLastError());
-        if (!stream) CK(cudaStreamSynchronize(st));
+        if (!stream) {
+            CK(cudaStreamSynchronize(st));
+            int e = 0;
+            CK(cudaMemcpy(&e, s->sweep_err, sizeof(int), cudaMemcpyDeviceToHost));
+            if (e) throw WError(ERR_CUDA, "staged gather: a bulk copy into shared memory did not complete within 1 s");
+        }
     });
 }
 
@@ -1926,7 +2265,12 @@ int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, 
                                           nullptr, nullptr, 0, st);
             rowsweep_rest<1, double>(*s, rk, u_dev, y_dev, nullptr, st);
             CK(cudaGetLastError());
-            if (!stream) CK(cudaStreamSynchronize(st));
+            if (!stream) {
+                CK(cudaStreamSynchronize(st));
+                int e = 0;
+                CK(cudaMemcpy(&e, s->sweep_err, sizeof(int), cudaMemcpyDeviceToHost));
+                if (e) throw WError(ERR_CUDA, "row sweep: a bulk copy into shared memory did not complete within 1 s");
+            }
             return;
         }
         scatter<1, 0>(*s, u_dev, y_dev, nullptr, nullptr, st);
@@ -1939,6 +2283,182 @@ void within_preconditioner_free(within_preconditioner* p) {
     if (p && --p->refs == 0) delete p;
 }
 uint64_t within_preconditioner_n(const within_preconditioner* p) { return p ? p->n : 0; }
+// ---- persisted preconditioner: the host image in this library's own byte
+// format (magic, version, kind, DOF count, then every field of the diagonal
+// or Schwarz image as a length-prefixed little-endian array in a fixed order,
+// then an FNV-1a checksum of everything before it).  It plays the part of the
+// reference's pickled Preconditioner (crates/within-py/src/config.rs:366-389,
+// operator/schwarz.rs:115-183); the reference's postcard bytes embed
+// approx-chol's private factor layout, so the two formats are not
+// interchangeable.
+}  // extern "C"
+namespace {
+
+constexpr char PC_MAGIC[8] = {'W', 'G', 'P', 'U', 'P', 'C', 'N', 'D'};
+constexpr uint32_t PC_VERSION = 1;
+
+#define WGPU_SCHWARZ_FIELDS(X)                                                                          \
+    X(n_dofs) X(n_sub) X(loc_ptr) X(n_elim) X(red_off) X(n_kept) X(red_n) X(mode) X(kept_ptr) X(glob)   \
+    X(scale) X(slot_sub) X(inv_e) X(ct_ptr) X(ct_col) X(ct_val) X(ct_rowsum) X(ct_row_slot)             \
+    X(ct_row_red) X(elim_slot) X(c_ptr) X(c_col) X(c_val) X(n_red) X(red_sub) X(dense_rows_ptr)         \
+    X(dense_row_slot) X(dense_col) X(dense_val) X(n_rounds) X(dinv) X(fwd_round_ptr) X(fwd_row)         \
+    X(fwd_ptr) X(fwd_col) X(fwd_val) X(bwd_round_ptr) X(bwd_row) X(bwd_ptr) X(bwd_col) X(bwd_val)       \
+    X(core_rows_ptr) X(core_row_slot) X(core_col) X(core_val) X(max_core) X(dof_ptr) X(dof_slot)        \
+    X(factor_nnz) X(cross_nnz) X(max_round_rows)
+
+uint64_t fnv1a(const uint8_t* p, size_t n) {
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+struct PcWriter {
+    std::vector<uint8_t> b;
+    template <class T>
+    void put(const T& v) {
+        static_assert(std::is_trivially_copyable<T>::value, "pod");
+        const auto* q = reinterpret_cast<const uint8_t*>(&v);
+        b.insert(b.end(), q, q + sizeof(T));
+    }
+    template <class T>
+    void io(const T& v) { put(v); }
+    template <class T>
+    void io(const std::vector<T>& v) {
+        put((uint64_t)v.size());
+        const auto* q = reinterpret_cast<const uint8_t*>(v.data());
+        b.insert(b.end(), q, q + v.size() * sizeof(T));
+    }
+};
+
+struct PcReader {
+    const uint8_t* p;
+    size_t n, off = 0;
+    void need(size_t k) {
+        if (k > n - off) throw WError(ERR_INVALID, "preconditioner bytes are truncated");
+    }
+    template <class T>
+    void get(T& v) {
+        need(sizeof(T));
+        std::memcpy(&v, p + off, sizeof(T));
+        off += sizeof(T);
+    }
+    template <class T>
+    void io(T& v) { get(v); }
+    template <class T>
+    void io(std::vector<T>& v) {
+        uint64_t len = 0;
+        get(len);
+        if (len > (n - off) / sizeof(T)) throw WError(ERR_INVALID, "preconditioner bytes are truncated");
+        v.resize(len);
+        std::memcpy(v.data(), p + off, len * sizeof(T));
+        off += len * sizeof(T);
+    }
+};
+
+template <class IO, class H>
+void schwarz_io(IO& io, H& h) {
+#define WGPU_IO_FIELD(f) io.io(h.f);
+    WGPU_SCHWARZ_FIELDS(WGPU_IO_FIELD)
+#undef WGPU_IO_FIELD
+}
+
+std::vector<uint8_t> serialize_precond(const within_preconditioner& P) {
+    PcWriter w;
+    w.b.insert(w.b.end(), PC_MAGIC, PC_MAGIC + 8);
+    w.put(PC_VERSION);
+    w.put((int32_t)P.kind);
+    w.put((uint32_t)P.n);
+    if (P.kind == 2) w.io(P.host_inv_diag);
+    else schwarz_io(w, P.host);
+    w.put(fnv1a(w.b.data(), w.b.size()));
+    return std::move(w.b);
+}
+
+within_preconditioner* deserialize_precond(const uint8_t* buf, size_t len, int device) {
+    if (!buf || len < 8 + 4 + 4 + 4 + 8) throw WError(ERR_INVALID, "preconditioner bytes are truncated");
+    if (std::memcmp(buf, PC_MAGIC, 8) != 0) throw WError(ERR_INVALID, "not a serialised within_b200 preconditioner");
+    uint64_t sum = 0;
+    std::memcpy(&sum, buf + len - 8, 8);
+    if (sum != fnv1a(buf, len - 8)) throw WError(ERR_INVALID, "preconditioner bytes are corrupt (checksum)");
+    PcReader r{buf, len - 8, 8};
+    uint32_t ver = 0, n = 0;
+    int32_t kind = 0;
+    r.get(ver);
+    if (ver != PC_VERSION)
+        throw WError(ERR_UNSUPPORTED, "preconditioner format version " + std::to_string(ver) + " (this build reads " +
+                                          std::to_string(PC_VERSION) + ")");
+    r.get(kind);
+    r.get(n);
+    if (kind != 1 && kind != 2) throw WError(ERR_INVALID, "preconditioner bytes hold an unknown kind");
+    if (device < 0) CK(cudaGetDevice(&device));
+    set_device(device);
+    auto P = std::make_unique<within_preconditioner>();
+    P->device = device;
+    P->kind = kind;
+    P->n = n;
+    if (kind == 2) {
+        r.io(P->host_inv_diag);
+        if (P->host_inv_diag.size() != n) throw WError(ERR_INVALID, "preconditioner bytes: diagonal size mismatch");
+        P->inv_diag = P->arena.upload(P->host_inv_diag);
+    } else {
+        SchwarzHost H;
+        schwarz_io(r, H);
+        if (H.n_dofs != n) throw WError(ERR_INVALID, "preconditioner bytes: DOF count mismatch");
+        upload_schwarz(*P, std::move(H));
+    }
+    if (r.off != r.n) throw WError(ERR_INVALID, "preconditioner bytes have trailing data");
+    CK(cudaDeviceSynchronize());
+    return P.release();
+}
+
+}  // namespace
+extern "C" {
+
+int within_preconditioner_serialize(const within_preconditioner* p, uint8_t* buf, uint64_t cap, uint64_t* len) {
+    return guarded([&] {
+        if (!p || !len) throw WError(ERR_INVALID, "within_preconditioner_serialize: NULL argument");
+        std::lock_guard<std::mutex> g(const_cast<within_preconditioner*>(p)->mu);
+        const std::vector<uint8_t> b = serialize_precond(*p);
+        *len = b.size();
+        if (!buf) return;
+        if (cap < b.size())
+            throw WError(ERR_INVALID, "within_preconditioner_serialize: buffer of " + std::to_string(cap) +
+                                          " bytes, " + std::to_string(b.size()) + " needed");
+        std::memcpy(buf, b.data(), b.size());
+    });
+}
+
+int within_preconditioner_deserialize(const uint8_t* buf, uint64_t len, int32_t device,
+                                      within_preconditioner** out) {
+    return guarded([&] {
+        if (!out) throw WError(ERR_INVALID, "within_preconditioner_deserialize: NULL output");
+        *out = nullptr;
+        *out = deserialize_precond(buf, (size_t)len, device);
+    });
+}
+
+int within_preconditioner_stats(const within_preconditioner* p, within_precond_stats* out) {
+    return guarded([&] {
+        if (!p || !out) throw WError(ERR_INVALID, "within_preconditioner_stats: NULL argument");
+        *out = within_precond_stats{};
+        out->n = p->n;
+        if (p->kind != 1) return;
+        const SchwarzHost& H = p->host;
+        out->n_subdomains = H.n_sub;
+        out->n_slots = H.glob.size();
+        out->nnz_c = H.c_col.size();
+        out->nnz_ct = H.ct_col.size();
+        out->nnz_fwd = H.fwd_col.size();
+        out->nnz_bwd = H.bwd_col.size();
+        out->nnz_dense = H.dense_col.size();
+        out->nnz_core = H.core_col.size();
+        out->n_reduced = H.n_red;
+        out->n_rounds = H.n_rounds;
+    });
+}
 const char* within_preconditioner_variant_name(const within_preconditioner* p) {
     return p && p->kind == 2 ? "Diagonal" : "Additive";
 }
