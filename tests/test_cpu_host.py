@@ -69,6 +69,44 @@ def test_schwarz_round_schedule_and_index_ranges(tmp_path):
     assert "schwarz ok" in out
 
 
+def test_dense_generalised_inverse(tmp_path):
+    """The dense route's generalised inverse (LDL^T with a null pivot zeroed,
+    host_schwarz.cpp dense_pinv) of connected and two-component Laplacians and
+    of an SDD matrix (tests/cpp/pinv_test.cpp): symmetric, A G A = A, the
+    inverse of the SDD matrix, and for the connected Laplacian the inverse
+    grounded at the last vertex (natural order puts the null pivot there);
+    relative to the largest entry, 1e-8."""
+    import numpy as np
+    exe = tmp_path / "pinv_test"
+    csrc = os.path.join(ROOT, "within_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-I", csrc, "-o", str(exe),
+                    os.path.join(ROOT, "tests", "cpp", "pinv_test.cpp"),
+                    os.path.join(csrc, "host_schwarz.cpp"), os.path.join(csrc, "host_design.cpp")], check=True)
+    lines = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert lines[-1] == "pinv done"
+    cases = 0
+    for i in range(0, len(lines) - 1, 3):
+        _, n, kind, size = lines[i].split()
+        n = int(n)
+        a = np.array(lines[i + 1].split(), float).reshape(n, n)
+        g = np.array(lines[i + 2].split(), float).reshape(n, n)
+        assert int(size) == n * n
+        scale = np.max(np.abs(g))
+        assert np.max(np.abs(g - g.T)) <= 1e-12 * scale
+        assert np.max(np.abs(a @ g @ a - a)) <= 1e-8 * np.max(np.abs(a)), (n, kind)
+        if kind == "2":
+            ref = np.linalg.inv(a)
+        elif kind == "0":
+            ref = np.zeros_like(a)
+            ref[:-1, :-1] = np.linalg.inv(a[:-1, :-1])
+        else:
+            ref = None
+        if ref is not None:
+            assert np.max(np.abs(g - ref)) <= 1e-8 * np.max(np.abs(ref)), (n, kind)
+        cases += 1
+    assert cases == 9
+
+
 def test_config_lowering(wb):
     from within_b200 import _precond_config
     from within_b200.config import (AdditiveSchwarz, ApproxCholConfig, ApproxSchurConfig,

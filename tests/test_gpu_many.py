@@ -53,3 +53,25 @@ def test_solver_set_errors(wb):
     bad[3, 0] = np.nan
     with pytest.raises(ValueError):
         ss.solve_batch([cases[0][1], bad])
+
+
+def test_solver_set_mixed_precision_matches_single_mixed_solvers(wb):
+    """The FP32-with-FP64-refinement variant of the many-designs batch: every
+    design equals its own mixed-precision Solver bit for bit, and lies within
+    1e-7 (max|d| / max|y|) of the FP64 solve at tol 1e-11."""
+    cases = small_designs(count=5, seed=2)
+    opts = wb.LsmrOptions(tol=1e-10, maxiter=5000)
+    ss = wb.SolverSet([c for c, _ in cases], threads=4, precision="mixed")
+    out = ss.solve_batch([Y for _, Y in cases], opts)
+    for i, (codes, Y) in enumerate(cases):
+        single = wb.Solver(codes, precision="mixed").solve_batch(Y, opts)
+        x, dm, conv, its = out[i]
+        assert all(conv)
+        np.testing.assert_array_equal(dm, single.demeaned)
+        ref = wb.Solver(codes).solve_batch(Y, wb.LsmrOptions(tol=1e-11, maxiter=5000))
+        for c in range(Y.shape[1]):
+            assert np.max(np.abs(dm[:, c] - ref.demeaned[:, c])) <= 1e-7 * np.max(np.abs(Y[:, c]))
+    ss.set_precision("fp64")
+    out64 = ss.solve_batch([Y for _, Y in cases], opts)
+    single64 = wb.Solver(cases[0][0]).solve_batch(cases[0][1], opts)
+    np.testing.assert_array_equal(out64[0][1], single64.demeaned)

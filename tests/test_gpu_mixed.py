@@ -25,26 +25,35 @@ def panel(n, seed=5):
 
 @pytest.mark.parametrize("k", [1, 4])
 def test_mixed_matches_fp64_oracle_solve(wb, k):
+    """The mixed-precision accuracy target: at a tolerance where the plain FP64
+    solve is within 1e-8 (max|d| / max|y|) of the FP64 solve at tol 1e-12
+    (tol 1e-11: plain ~3e-10 on this panel), the mixed solve is too (measured
+    ~5e-10 to 1.4e-9).  At the contract tolerance 1e-8 the two stopping tests
+    leave the mixed solve 1.2 to 2.4x the plain one's error on this 300k-row
+    panel (and below it on the 10M-row panel), so that case holds 3x."""
     codes, w = panel(300_000)
     n = codes.shape[0]
     rng = np.random.default_rng(k)
     Y = np.asfortranarray(rng.standard_normal((n, k)))
     s64 = wb.Solver(codes, weights=w)
     ref = s64.solve_batch(Y, wb.LsmrOptions(tol=1e-12, maxiter=10000))
-    plain = s64.solve_batch(Y, wb.LsmrOptions(tol=1e-8))
     smx = wb.Solver(codes, weights=w, precision="mixed")
     assert smx.precision == "mixed"
-    mx = smx.solve_batch(Y, wb.LsmrOptions(tol=1e-8))
     cats = [codes[:, j] for j in range(3)]
-    for c in range(k):
-        assert mx.converged[c]
-        e_mx = rel_inf(mx.demeaned[:, c], ref.demeaned[:, c], Y[:, c])
-        e_plain = rel_inf(plain.demeaned[:, c], ref.demeaned[:, c], Y[:, c])
-        # the accuracy of the plain FP64 solve at the same tolerance
-        assert e_mx <= max(3.0 * e_plain, 1e-8), (e_mx, e_plain)
-        ne_mx = normal_equation_residual(cats, Y[:, c], mx.demeaned[:, c], w)
-        ne_plain = normal_equation_residual(cats, Y[:, c], plain.demeaned[:, c], w)
-        assert ne_mx <= max(3.0 * ne_plain, 1e-7), (ne_mx, ne_plain)
+    for tol in (1e-11, 1e-8):
+        plain = s64.solve_batch(Y, wb.LsmrOptions(tol=tol))
+        mx = smx.solve_batch(Y, wb.LsmrOptions(tol=tol))
+        for c in range(k):
+            assert mx.converged[c]
+            e_mx = rel_inf(mx.demeaned[:, c], ref.demeaned[:, c], Y[:, c])
+            e_plain = rel_inf(plain.demeaned[:, c], ref.demeaned[:, c], Y[:, c])
+            if tol == 1e-11:
+                assert e_plain <= 1e-8 and e_mx <= 1e-8, (e_mx, e_plain)
+            else:
+                assert e_mx <= 3.0 * e_plain, (e_mx, e_plain)
+                ne_mx = normal_equation_residual(cats, Y[:, c], mx.demeaned[:, c], w)
+                ne_plain = normal_equation_residual(cats, Y[:, c], plain.demeaned[:, c], w)
+                assert ne_mx <= max(3.0 * ne_plain, 1e-7), (ne_mx, ne_plain)
 
 
 def test_mixed_against_restatement_with_slopes_and_diagonal(wb, oracle):

@@ -671,6 +671,14 @@ class SolverSet:
     def __len__(self) -> int:
         return len(self._h)
 
+    def set_precision(self, precision: str) -> None:
+        """Solver.set_precision on every design of the set."""
+        code = {"fp64": _ffi.PRECISION_FP64, "mixed": _ffi.PRECISION_MIXED}.get(precision)
+        if code is None:
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        for h in self._h:
+            _ffi.check(_ffi.lib().within_solver_set_precision(h, code))
+
     def __del__(self):
         for h in getattr(self, "_h", []):
             if h:

@@ -80,9 +80,12 @@ struct PrecondCfg {
     uint64_t scaling_max_sweeps = 2048;
     bool scaling_error = false;
     // round-parallel factor: when to stop the rounds (host_schwarz.cpp ac_rounds)
-    uint32_t core_dense_max = 2048;
-    double core_min_frac = 0.3;
+    uint32_t core_dense_max = 2048;   // a reduced system this small is inverted densely at once
+    double core_min_frac = 0.3;       // a large graph stops when a round eliminates less than this
     uint32_t max_rounds = 64;
+    uint32_t core_small = 16384;      // at or below: rounds continue past core_min_frac ...
+    uint32_t core_dense_late = 512;   // ... until this many vertices remain (dense core)
+    double core_min_frac_small = 0.005;   // (or a round eliminates less than this)
 };
 
 // Host image of the additive Schwarz preconditioner in the layout the apply
@@ -162,5 +165,8 @@ struct HostPlan {
     std::vector<SRSplit> splits;
     void add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, int tile);
 };
+
+// dense generalised inverse of a symmetric PSD matrix (the preconditioner's dense route)
+std::vector<double> dense_pseudo_inverse(uint32_t n, const std::vector<double>& a);
 
 }  // namespace wgpu

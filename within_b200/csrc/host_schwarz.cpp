@@ -480,10 +480,13 @@ struct Factor {
 };
 
 // Dense LDL^T in natural order with pseudo-inverse pivots, materialised as
-// G = L^-T D^+ L^-1 (n <= DENSE_MAX).  Returns false on a clearly negative pivot.
+// G = L^-T D^+ L^-1.  Returns false on a clearly negative pivot.  Laid out
+// for the cache and the vector units: the factorisation updates the lower
+// triangle row by row (contiguous), L^-1 is formed row by row from earlier
+// rows, and the rows of G are independent sums spread over host threads.
 bool dense_pinv(const Lap& m, Factor& f) {
     const uint32_t n = m.n;
-    std::vector<double> a((size_t)n * n, 0.0);
+    std::vector<double> a((size_t)n * n, 0.0);   // lower triangle (row-major) used
     double maxd = 0;
     for (uint32_t i = 0; i < n; ++i)
         for (uint32_t k = m.ptr[i]; k < m.ptr[i + 1]; ++k) {
@@ -491,9 +494,9 @@ bool dense_pinv(const Lap& m, Factor& f) {
             if (m.col[k] == i) maxd = std::max(maxd, std::fabs(m.val[k]));
         }
     const double fl = 1e-13 * std::max(maxd, DBL_MIN) * std::max<uint32_t>(n, 1);
-    std::vector<double> piv(n, 0.0);
+    std::vector<double> piv(n, 0.0), c(n);
     for (uint32_t k = 0; k < n; ++k) {
-        double d = a[(size_t)k * n + k];
+        const double d = a[(size_t)k * n + k];
         if (d < -fl) return false;
         if (d <= fl) {
             piv[k] = 0.0;
@@ -501,36 +504,51 @@ bool dense_pinv(const Lap& m, Factor& f) {
             continue;
         }
         piv[k] = d;
+        const double inv = 1.0 / d;
+        for (uint32_t i = k + 1; i < n; ++i) c[i] = a[(size_t)i * n + k];   // column k, before scaling
         for (uint32_t i = k + 1; i < n; ++i) {
-            double lik = a[(size_t)i * n + k];
-            if (lik == 0.0) continue;
-            for (uint32_t j = k + 1; j < n; ++j) a[(size_t)i * n + j] -= lik * a[(size_t)k * n + j] / d;
+            const double ci = c[i];
+            if (ci == 0.0) continue;
+            const double li = ci * inv;
+            double* row = &a[(size_t)i * n];
+            for (uint32_t j = k + 1; j <= i; ++j) row[j] -= li * c[j];
+            row[k] = li;   // L below the diagonal
         }
-        for (uint32_t i = k + 1; i < n; ++i) a[(size_t)i * n + k] /= d;  // L below diagonal
     }
+    // L^-1 (unit lower), row i from the rows before it: Li[i] = e_i - sum_k L[i][k] Li[k]
+    std::vector<double> li((size_t)n * n, 0.0);
+    for (uint32_t i = 0; i < n; ++i) {
+        double* ri = &li[(size_t)i * n];
+        ri[i] = 1.0;
+        const double* lrow = &a[(size_t)i * n];
+        for (uint32_t k = 0; k < i; ++k) {
+            const double l = lrow[k];
+            if (l == 0.0) continue;
+            const double* rk = &li[(size_t)k * n];
+            for (uint32_t j = 0; j <= k; ++j) ri[j] -= l * rk[j];
+        }
+    }
+    // G[r][c] = sum_k D^+_k Li[k][r] Li[k][c] (k >= max(r, c)), one row of G per task
     f.n = n;
     f.dense = true;
     f.pinv.assign((size_t)n * n, 0.0);
-    std::vector<double> x(n);
-    for (uint32_t c = 0; c < n; ++c) {
-        std::fill(x.begin(), x.end(), 0.0);
-        x[c] = 1.0;
-        for (uint32_t k = 0; k < n; ++k)
-            for (uint32_t i = k + 1; i < n; ++i) x[i] -= a[(size_t)i * n + k] * x[k];
-        for (uint32_t k = 0; k < n; ++k) x[k] = piv[k] > 0.0 ? x[k] / piv[k] : 0.0;
-        for (uint32_t k = n; k-- > 0;) {
-            double s = x[k];
-            for (uint32_t i = k + 1; i < n; ++i) s -= a[(size_t)i * n + k] * x[i];
-            x[k] = s;
+    std::vector<double> dp(n);
+    for (uint32_t k = 0; k < n; ++k) dp[k] = piv[k] > 0.0 ? 1.0 / piv[k] : 0.0;
+    par_for_each(n, [&](size_t r) {
+        double* g = &f.pinv[r * n];
+        for (uint32_t k = (uint32_t)r; k < n; ++k) {
+            const double* rk = &li[(size_t)k * n];
+            const double w = dp[k] * rk[r];
+            if (w == 0.0) continue;
+            for (uint32_t cc = 0; cc <= k; ++cc) g[cc] += w * rk[cc];
         }
-        for (uint32_t r = 0; r < n; ++r) f.pinv[(size_t)r * n + c] = x[r];
-    }
+    });
     // symmetrise the roundoff
     for (uint32_t r = 0; r < n; ++r)
-        for (uint32_t c = r + 1; c < n; ++c) {
-            double v = 0.5 * (f.pinv[(size_t)r * n + c] + f.pinv[(size_t)c * n + r]);
-            f.pinv[(size_t)r * n + c] = v;
-            f.pinv[(size_t)c * n + r] = v;
+        for (uint32_t cc = r + 1; cc < n; ++cc) {
+            double v = 0.5 * (f.pinv[(size_t)r * n + cc] + f.pinv[(size_t)cc * n + r]);
+            f.pinv[(size_t)r * n + cc] = v;
+            f.pinv[(size_t)cc * n + r] = v;
         }
     return true;
 }
@@ -593,8 +611,15 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
         // core_min_frac of the vertices eliminated) or at max_rounds, keeps
         // only its diagonal -- its intra-core edges are dropped, which leaves
         // an SDD (positive semi-definite) approximation of the core.
-        const bool small = live.size() <= cfg.core_dense_max && live.size() > 1;
-        const bool stalled = last_frac < cfg.core_min_frac || r >= cfg.max_rounds;
+        // A graph of at most core_small vertices (a few thousand kept levels
+        // with a dense or banded Schur complement, where every round removes
+        // only a few per cent) keeps eliminating until core_dense_late remain:
+        // its diagonal alone would leave the preconditioner far from exact.
+        const bool tiny_graph = live.size() <= cfg.core_small;
+        const uint32_t dense_at = r == 0 ? cfg.core_dense_max : std::min(cfg.core_dense_max, cfg.core_dense_late);
+        const bool small = live.size() <= dense_at && live.size() > 1;
+        const bool stalled = (tiny_graph ? last_frac < cfg.core_min_frac_small : last_frac < cfg.core_min_frac) ||
+                             r >= (tiny_graph ? 4 * cfg.max_rounds : cfg.max_rounds);
         if (small || (stalled && live.size() > 1)) {
             f.core = live;
             std::sort(f.core.begin(), f.core.end());
@@ -1156,6 +1181,26 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         for (uint32_t j = 0; j < S.glob.size(); ++j) S.dof_slot[cur[S.glob[j]]++] = j;
     }
     return out;
+}
+
+// The dense generalised inverse of a symmetric positive semi-definite n x n
+// matrix (row-major), as the dense route of the preconditioner builds it;
+// empty when a pivot is clearly negative.
+std::vector<double> dense_pseudo_inverse(uint32_t n, const std::vector<double>& a) {
+    Lap m;
+    m.n = n;
+    m.ptr.assign(1, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t j = 0; j < n; ++j)
+            if (a[(size_t)i * n + j] != 0.0) {
+                m.col.push_back(j);
+                m.val.push_back(a[(size_t)i * n + j]);
+            }
+        m.ptr.push_back((uint32_t)m.col.size());
+    }
+    Factor f;
+    if (!dense_pinv(m, f)) return {};
+    return f.pinv;
 }
 
 }  // namespace wgpu

@@ -32,6 +32,18 @@ template <int K>
 constexpr int sr_items() { return K >= 8 ? 2 : 4; }
 template <int K>
 constexpr int sr_tile() { return SR_THREADS * sr_items<K>(); }
+// Wide tiles (4x the items per thread, K <= 2) for problems of long segments
+// (restrict / means / kept sums of a few huge subdomains, C^T rows of kept
+// levels with many eliminated neighbours, the level-sorted rest terms): a
+// tile of mostly interior positions pays the fixed per-tile cost (barriers,
+// segment-start table, split bookkeeping) once per 4x more positions, and
+// each thread keeps 4x more independent loads in flight.
+template <int K>
+constexpr int sr_items_wide() { return K == 1 ? 16 : (K == 2 ? 8 : sr_items<K>()); }
+template <int K>
+constexpr int sr_tile_wide() { return SR_THREADS * sr_items_wide<K>(); }
+// a problem takes wide tiles when its segments average at least this many positions
+constexpr uint32_t SR_WIDE_MEAN_LEN = 64;
 // resident CTAs per SM the register budget is sized for (no spills at K = 8)
 // (the register footprint scales with K x the accumulator width)
 template <int K, class A = double>
@@ -54,13 +66,12 @@ constexpr int sr_min_blocks() {
 // a segment's last position emits it straight from registers; the scan's
 // combine is "a segment start resets the sum", and the id >= 0 of the last
 // start doubles as the reset flag.
-template <class F, int K>
-__global__ void __launch_bounds__(SR_THREADS, sr_min_blocks<K, typename F::Acc>())
+template <class F, int K, int ITEMS = sr_items<K>()>
+__global__ void __launch_bounds__(SR_THREADS, (ITEMS > sr_items<K>() ? 2 : sr_min_blocks<K, typename F::Acc>()))
 segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
                  const SRSplit* __restrict__ splits, double* __restrict__ head_buf,
                  double* __restrict__ tail_buf, unsigned* __restrict__ counters,
                  const int* __restrict__ skip) {
-    constexpr int ITEMS = sr_items<K>();
     constexpr int T = SR_THREADS * ITEMS;
     using Prob = typename F::Prob;
     using A = typename F::Acc;
@@ -299,6 +310,45 @@ segthread_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ ski
         for (int k = 0; k < K; ++k) acc[k] += v[k];
     }
     f.emit(pr, sg, acc);
+}
+
+// A run of consecutive elimination rounds whose segments are all short and
+// few (the small tail of a round-scheduled factor: rounds of a few hundred
+// rows each): one block walks the rounds in order (forward) or in reverse
+// (backward), one thread per segment as in segthread_kernel, with a block
+// barrier between rounds -- one launch instead of one per round.  The rounds
+// are problems r_lo..r_hi-1 of f.probs; round_rows[r] is round r's segment
+// count.  Each segment is summed in the order segthread_kernel uses, so the
+// results are bitwise the same.
+constexpr int RF_THREADS = 1024;
+constexpr uint32_t RF_MAX_ROWS = 4 * RF_THREADS;   // rows of a round the fused launch takes
+
+template <class F, int K>
+__global__ void __launch_bounds__(RF_THREADS)
+rounds_fused_kernel(F f, const uint32_t* __restrict__ round_rows, uint32_t r_lo, uint32_t r_hi, int backward,
+                    const int* __restrict__ skip) {
+    using A = typename F::Acc;
+    if (skip && *skip) return;
+    for (uint32_t i = 0; i < r_hi - r_lo; ++i) {
+        const uint32_t r = backward ? r_hi - 1 - i : r_lo + i;
+        const typename F::Prob pr = f.probs[r];
+        const uint32_t* ptr = f.seg_ptr(pr);
+        const uint32_t n_seg = round_rows[r];
+        for (uint32_t sg = threadIdx.x; sg < n_seg; sg += RF_THREADS) {
+            const uint32_t a = __ldg(ptr + sg), b = __ldg(ptr + sg + 1);
+            A acc[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = (A)0;
+            for (uint32_t q = a; q < b; ++q) {
+                A v[K];
+                f.value(pr, q, v);
+#pragma unroll
+                for (int k = 0; k < K; ++k) acc[k] += v[k];
+            }
+            f.emit(pr, sg, acc);
+        }
+        __syncthreads();   // the next round reads this round's results
+    }
 }
 
 // the longest segment of a pointer array (host)

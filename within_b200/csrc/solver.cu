@@ -90,8 +90,23 @@ struct DevPlan {
     unsigned* counters = nullptr;
     uint32_t n_tiles = 0;
     uint32_t n_splits = 0;
+    bool wide = false;   // tiles of sr_tile_wide<K>() positions (else sr_tile<K>())
     std::vector<uint32_t> range_lo, range_hi;   // tile ranges (per round, for round plans)
 };
+
+// Tile size of a plan: wide tiles when K <= 2 and its segments average
+// SR_WIDE_MEAN_LEN positions or more.  Fixed by the design, so the summation
+// order is too.  WITHIN_WIDE_TILES=0: never.
+bool plan_wide(int K, uint64_t positions, uint64_t segments) {
+    if (K > 2) return false;
+    if (const char* e = getenv("WITHIN_WIDE_TILES"))
+        if (atoi(e) == 0) return false;
+    return segments > 0 && positions >= (uint64_t)SR_WIDE_MEAN_LEN * segments;
+}
+int plan_tile(int K, bool wide) {
+    if (wide) return K == 1 ? sr_tile_wide<1>() : sr_tile_wide<2>();
+    return K == 1 ? sr_tile<1>() : K == 2 ? sr_tile<2>() : K == 4 ? sr_tile<4>() : sr_tile<8>();
+}
 
 DevPlan make_plan(Arena& A, const HostPlan& hp, int K) {
     DevPlan d;
@@ -116,6 +131,14 @@ void launch_segthread(const F& f, uint32_t prob, uint32_t n_seg, const int* skip
 template <class F, int K>
 void launch_sr(const F& f, const DevPlan& p, uint32_t lo, uint32_t hi, const int* skip, cudaStream_t st) {
     if (hi <= lo) return;
+    if constexpr (K <= 2) {
+        if (p.wide) {
+            segreduce_kernel<F, K, sr_items_wide<K>()><<<hi - lo, SR_THREADS, 0, st>>>(
+                f, p.tiles, lo, p.splits, p.head, p.tail, p.counters, skip);
+            ++g_launches;
+            return;
+        }
+    }
     segreduce_kernel<F, K><<<hi - lo, SR_THREADS, 0, st>>>(f, p.tiles, lo, p.splits, p.head, p.tail,
                                                            p.counters, skip);
     ++g_launches;
@@ -312,6 +335,11 @@ struct KPlans {
     // when every segment is short: segment counts (0: segmented reduction)
     uint32_t c_thread = 0, prolong_thread = 0;
     std::vector<uint32_t> fwd_thread, bwd_thread;
+    // rounds [fuse_lo, n_rounds) run as one single-block launch per direction
+    // (rounds_fused_kernel) when each has at most RF_MAX_ROWS short rows
+    uint32_t fuse_lo = 0, fuse_hi = 0;
+    uint32_t* fwd_rows = nullptr;
+    uint32_t* bwd_rows = nullptr;
     SchwarzWork w;
     SchwarzWorkT<float> wf;   // mixed-precision inner solve, allocated on first use
     bool ready = false;
@@ -333,11 +361,14 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     if (kp.ready) return kp;
     const SchwarzHost& H = P.host;
     Arena& A = U.arena;
-    const int T = K == 1 ? sr_tile<1>() : K == 2 ? sr_tile<2>() : K == 4 ? sr_tile<4>() : sr_tile<8>();
+    const int T = plan_tile(K, false);
     auto one = [&](const std::vector<uint32_t>& ptr) {
         HostPlan hp;
-        hp.add(0, ptr.data(), (uint32_t)ptr.size() - 1, T);
+        const uint32_t n_seg = (uint32_t)ptr.size() - 1;
+        const bool wide = plan_wide(K, n_seg ? ptr[n_seg] - ptr[0] : 0, n_seg);
+        hp.add(0, ptr.data(), n_seg, plan_tile(K, wide));
         DevPlan d = make_plan(A, hp, K);
+        d.wide = wide;
         d.range_lo = {0};
         d.range_hi = {d.n_tiles};
         return d;
@@ -380,6 +411,32 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     };
     kp.fwd_thread = round_thread(H.fwd_round_ptr, H.fwd_ptr);
     kp.bwd_thread = round_thread(H.bwd_round_ptr, H.bwd_ptr);
+    // the fused tail: the longest suffix of rounds that are one-thread rounds
+    // in both directions with at most RF_MAX_ROWS rows (WITHIN_FUSE_ROUNDS=0: none)
+    {
+        const char* fz = getenv("WITHIN_FUSE_ROUNDS");
+        const bool fuse_on = segt_on && !(fz && atoi(fz) == 0);
+        const uint32_t nr = H.n_rounds;
+        uint32_t lo = nr;
+        auto ok = [&](uint32_t r) {
+            const uint32_t fr = H.fwd_round_ptr[r + 1] - H.fwd_round_ptr[r];
+            const uint32_t br = H.bwd_round_ptr[r + 1] - H.bwd_round_ptr[r];
+            return (fr == 0 || kp.fwd_thread[r]) && (br == 0 || kp.bwd_thread[r]) && fr <= RF_MAX_ROWS &&
+                   br <= RF_MAX_ROWS;
+        };
+        while (fuse_on && lo > 0 && ok(lo - 1)) --lo;
+        if (nr - lo >= 2) {
+            kp.fuse_lo = lo;
+            kp.fuse_hi = nr;
+            std::vector<uint32_t> fr(nr), br(nr);
+            for (uint32_t r = 0; r < nr; ++r) {
+                fr[r] = H.fwd_round_ptr[r + 1] - H.fwd_round_ptr[r];
+                br[r] = H.bwd_round_ptr[r + 1] - H.bwd_round_ptr[r];
+            }
+            kp.fwd_rows = A.upload(fr);
+            kp.bwd_rows = A.upload(br);
+        }
+    }
     size_t nl = H.glob.size(), nr = H.n_red, ns = H.n_sub;
     kp.w.rl = A.alloc<double>(nl * K);
     kp.w.sl = A.alloc<double>(nl * K);
@@ -446,12 +503,24 @@ void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const T* r, T* z, c
     launch_sr<CtFT, K>(CtFT{P.p_ct, S}, kp.ct, 0, kp.ct.n_tiles, skip, st);
     launch_sr<KS, K>(KS{P.p_kept, S}, kp.kept, 0, kp.kept.n_tiles, skip, st);
     if (P.has_dense) launch_sr<DF, K>(DF{P.p_dense, S}, kp.dense, 0, kp.dense.n_tiles, skip, st);
-    for (uint32_t r = 0; r < P.n_rounds; ++r) {
+    const bool fused = kp.fuse_hi > kp.fuse_lo;
+    const uint32_t r_fwd_end = fused ? kp.fuse_lo : P.n_rounds;
+    for (uint32_t r = 0; r < r_fwd_end; ++r) {
         if (kp.fwd_thread[r]) launch_segthread<FF, K>(FF{P.p_fwd, S}, r, kp.fwd_thread[r], skip, st);
         else launch_sr<FF, K>(FF{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
     }
+    if (fused) {
+        rounds_fused_kernel<FF, K><<<1, RF_THREADS, 0, st>>>(FF{P.p_fwd, S}, kp.fwd_rows, kp.fuse_lo, kp.fuse_hi, 0,
+                                                              skip);
+        ++g_launches;
+    }
     if (P.has_core) launch_sr<CoF, K>(CoF{P.p_core, S}, kp.core, 0, kp.core.n_tiles, skip, st);
-    for (uint32_t r = P.n_rounds; r-- > 0;) {
+    if (fused) {
+        rounds_fused_kernel<BF, K><<<1, RF_THREADS, 0, st>>>(BF{P.p_bwd, S}, kp.bwd_rows, kp.fuse_lo, kp.fuse_hi, 1,
+                                                              skip);
+        ++g_launches;
+    }
+    for (uint32_t r = r_fwd_end; r-- > 0;) {
         if (kp.bwd_thread[r]) launch_segthread<BF, K>(BF{P.p_bwd, S}, r, kp.bwd_thread[r], skip, st);
         else launch_sr<BF, K>(BF{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
     }
@@ -847,11 +916,18 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
     rk.atu = A.alloc<double>(s.n_dofs * K);
     rk.n_rest = (uint32_t)rk.rest_host.size();
     if (rk.n_rest) {
-        const int Ttile = sr_tile<K>();
+        uint64_t pos = 0, segs = 0;
+        for (const auto& lp : rk.rest_ptrs) {
+            pos += lp.back() - lp.front();
+            segs += lp.size() - 1;
+        }
+        const bool wide = plan_wide(K, pos, segs);
+        const int Ttile = plan_tile(K, wide);
         HostPlan hp;
         for (size_t i = 0; i < rk.rest_host.size(); ++i)
             hp.add((uint32_t)i, rk.rest_ptrs[i].data(), (uint32_t)rk.rest_ptrs[i].size() - 1, Ttile);
         rk.rest = make_plan(A, hp, K);
+        rk.rest.wide = wide;
         rk.rest_probs = A.upload(rk.rest_host);
     }
     // dynamic shared memory above the default needs the opt-in (set outside any capture)
@@ -1715,6 +1791,8 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         if (const char* e = getenv("WITHIN_CORE_DENSE_MAX")) pc.core_dense_max = (uint32_t)atol(e);
         if (const char* e = getenv("WITHIN_CORE_MIN_FRAC")) pc.core_min_frac = atof(e);
         if (const char* e = getenv("WITHIN_MAX_ROUNDS")) pc.max_rounds = (uint32_t)atol(e);
+        if (const char* e = getenv("WITHIN_CORE_SMALL")) pc.core_small = (uint32_t)atol(e);
+        if (const char* e = getenv("WITHIN_CORE_DENSE_LATE")) pc.core_dense_late = (uint32_t)atol(e);
         BuildResult br = build_preconditioner(D, weights ? w.data() : nullptr, pc);
         s->n_warnings = br.n_warnings;
         if (br.kind != 0) {
