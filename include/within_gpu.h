@@ -132,6 +132,30 @@ uint64_t within_design_n_dofs(const within_design* d);
 int within_solver_new(const within_design* design, const double* weights,
                       const within_precond_config* cfg, const within_preconditioner* prebuilt,
                       int32_t device, within_solver** out);
+/* Solver::new with an explicit tuning record (no counterpart in the reference,
+ * whose strategy thresholds are constants, e.g. operator/design.rs:20 and
+ * operator/design/scatter.rs:97): the kernel variants and the stop rules of
+ * the round-parallel factor.  Every choice is a function of the design and
+ * this record, so results stay bitwise reproducible.  within_tuning_default
+ * fills the defaults; within_solver_new uses them (or the WITHIN_*
+ * environment overrides).  within_b200.autotune writes a table of records
+ * keyed on design statistics, from which the Python binding picks one. */
+typedef struct {
+    int32_t staged_sweep;       /* 1: staged (bulk-copy) row sweep / gather where they apply; 0: never */
+    uint32_t wide_mean_len;     /* reduction plans whose segments average this many positions take wide
+                                   tiles (default UINT32_MAX: never) */
+    int32_t fuse_rounds;        /* 1: the short tail of elimination rounds runs as one launch */
+    int32_t thread_per_segment; /* 1: one thread per segment where every segment is short */
+    uint32_t core_dense_max;    /* a reduced system of at most this many vertices is inverted densely */
+    double core_min_frac;       /* a large graph's rounds stop below this eliminated fraction */
+    uint32_t max_rounds;        /* round budget (4x for graphs of at most core_small vertices) */
+    uint32_t core_small;        /* graphs this small keep eliminating ... */
+    uint32_t core_dense_late;   /* ... until this many vertices remain (then a dense core) */
+} within_tuning;
+void within_tuning_default(within_tuning* t);
+int within_solver_new_tuned(const within_design* design, const double* weights,
+                            const within_precond_config* cfg, const within_preconditioner* prebuilt,
+                            int32_t device, const within_tuning* tuning, within_solver** out);
 void within_solver_free(within_solver* s);
 uint64_t within_solver_n_obs(const within_solver* s);
 uint64_t within_solver_n_dofs(const within_solver* s);

@@ -196,3 +196,18 @@ def test_reference_arm_line(budget):
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert ("per step one full solve" in line["cpu_baseline"]["sample"]) == (budget == "150")
+
+
+def test_tuning_table_lookup():
+    """The autotuner's table lookup (within_b200/autotune.py): nearest entry by
+    weighted key distance, None beyond the distance limit or for an empty
+    table; the design key of a worker/firm/year panel."""
+    from within_b200 import autotune as A
+    k = A.design_key(10_000_000, [1_000_000, 100_000, 20], False, False)
+    assert k == [pytest.approx(23.2534966), 3.0, pytest.approx(19.9315686), pytest.approx(16.6096405), 0.0, 0.0]
+    table = [{"key": A.design_key(2_000_000, [200_000, 20_000, 20], False, False), "tuning": {"fuse_rounds": 0}},
+             {"key": A.design_key(100_000, [500, 200], False, False), "tuning": {"fuse_rounds": 1}}]
+    assert A.lookup(k, table) == {"fuse_rounds": 0}
+    assert A.lookup(A.design_key(120_000, [600, 150], False, False), table) == {"fuse_rounds": 1}
+    assert A.lookup(A.design_key(1_000, [10], True, True), table) is None
+    assert A.lookup(k, []) is None

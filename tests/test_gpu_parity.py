@@ -374,3 +374,34 @@ def test_windowed_reorthogonalisation_matches_restatement(wb, oracle, local_size
     assert abs(r1.iterations - b.iterations[0]) <= max(2, 0.02 * b.iterations[0])
     plain = s.solve(np.ascontiguousarray(Y[:, 0]), wb.LsmrOptions(tol=1e-10, maxiter=5000))
     assert rel_inf(r1.demeaned, plain.demeaned, Y[:, 0]) < DEMEAN_TOL
+
+
+@pytest.mark.parametrize("tuning", [
+    {"staged_sweep": 0},
+    {"wide_mean_len": 32, "fuse_rounds": 0},
+    {"wide_mean_len": 0xFFFFFFFF, "thread_per_segment": 0},
+    {"core_small": 0, "core_min_frac": 0.1},
+    {"core_dense_late": 256, "core_dense_max": 256},
+])
+def test_tuning_records_match_oracle(wb, oracle, tuning):
+    """Every kernel variant and factor rule a tuning record can select gives
+    the oracle's demeaned vector: a worker-sorted panel (staged sweep, run and
+    histogram terms, wide-tile plans, a round-scheduled factor with a fused
+    tail) and a 3,000-level uniform design (its reduced system between the
+    dense limits, which takes the small-graph rounds)."""
+    from within_b200 import workloads as WL
+    codes = WL.akm_panel(n=400_000, n_workers=40_000, n_firms=4_000, seed=21)
+    y = np.random.default_rng(22).standard_normal(codes.shape[0])
+    r = wb.Solver(codes, tuning=tuning).solve(y, wb.LsmrOptions(tol=1e-10, maxiter=3000))
+    o = oracle.OracleSolver(codes).solve(y, tol=1e-10, maxiter=3000)
+    assert r.converged
+    assert rel_inf(r.demeaned, o.demeaned, y) < DEMEAN_TOL
+    rng = np.random.default_rng(23)
+    n = 150_000
+    cats = [rng.integers(0, 20_000, n), rng.integers(0, 3_000, n), rng.integers(0, 12, n)]
+    C = as_solver_categories(cats)
+    y2 = rng.standard_normal(n)
+    r2 = wb.Solver(C, tuning=tuning).solve(y2, wb.LsmrOptions(tol=1e-10, maxiter=3000))
+    o2 = oracle.OracleSolver(C).solve(y2, tol=1e-10, maxiter=3000)
+    assert r2.converged
+    assert rel_inf(r2.demeaned, o2.demeaned, y2) < DEMEAN_TOL

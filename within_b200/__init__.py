@@ -45,6 +45,7 @@ __all__ = [
     "solve_many",
     "fwl",
     "FwlResult",
+    "default_tuning",
     "Staleness",
     "MlsmrResult",
     "solve_ladder",
@@ -414,11 +415,57 @@ def _as_f64_2d(name, a):
 
 # ---------------------------------------------------------------------------
 
+def default_tuning() -> dict:
+    """The default within_tuning record (within_tuning_default) as a dict."""
+    t = _ffi.TuningC()
+    _ffi.lib().within_tuning_default(C.byref(t))
+    return {f: getattr(t, f) for f, _ in _ffi.TuningC._fields_}
+
+
+def _tuning_struct(tuning, design, weights):
+    """The within_tuning record of a Solver: None (the defaults and the WITHIN_*
+    environment overrides), "auto" (the autotuner's table entry nearest to the
+    design, else None), or a dict of within_tuning fields over the defaults."""
+    if tuning is None:
+        return None
+    if isinstance(tuning, str):
+        if tuning != "auto":
+            raise ValueError(f"tuning must be None, 'auto' or a dict, got {tuning!r}")
+        from . import autotune
+        table = autotune.load_table()
+        if not table:
+            return None
+        if isinstance(design, np.ndarray) or hasattr(design, "__array_interface__"):
+            cats = np.asarray(design)
+            levels = [int(cats[:, t].max()) + 1 if cats.shape[0] else 0 for t in range(cats.shape[1])]
+            n, slopes = cats.shape[0], False
+        else:
+            effects = list(design)
+            levels = [int(e.levels.max()) + 1 if e.levels.size else 0 for e in effects]
+            n, slopes = effects[0].levels.shape[0], any(e.slopes for e in effects)
+        rec = autotune.lookup(autotune.design_key(n, levels, slopes, weights is not None), table)
+        if rec is None:
+            return None
+        tuning = rec
+    t = _ffi.TuningC()
+    _ffi.lib().within_tuning_default(C.byref(t))
+    for k, v in dict(tuning).items():
+        if k not in dict(_ffi.TuningC._fields_):
+            raise ValueError(f"unknown tuning field {k!r}")
+        setattr(t, k, v)
+    return t
+
+
 class Solver:
-    """Persistent solver owning its preconditioner (crates/within/src/solver.rs:295-593)."""
+    """Persistent solver owning its preconditioner (crates/within/src/solver.rs:295-593).
+
+    ``tuning``: "auto" (default) takes the kernel variants and factor stop
+    rules of the autotuner's table entry nearest to the design
+    (within_b200/autotune.py), None the built-in defaults (with the WITHIN_*
+    environment overrides), or a dict of within_tuning fields."""
 
     def __init__(self, design, weights=None, preconditioner=None, device: int = -1,
-                 precision: str = "fp64"):
+                 precision: str = "fp64", tuning="auto"):
         L = _ffi.lib()
         d = _Design(design)
         w = None if weights is None else _as_f64_1d("weights", weights)
@@ -426,9 +473,15 @@ class Solver:
             raise ValueError(f"weights has length {w.shape[0]}, expected {d.n_obs}")
         prebuilt = preconditioner._h if isinstance(preconditioner, Preconditioner) else None
         cfg = None if prebuilt is not None else _precond_config(preconditioner)
+        tn = _tuning_struct(tuning, design, w)
+        self.tuning = None if tn is None else {f: getattr(tn, f) for f, _ in _ffi.TuningC._fields_}
         h = C.c_void_p()
-        _ffi.check(L.within_solver_new(d.h, _ffi.ptr(w), None if cfg is None else C.byref(cfg),
-                                       prebuilt, device, C.byref(h)))
+        if tn is None:
+            _ffi.check(L.within_solver_new(d.h, _ffi.ptr(w), None if cfg is None else C.byref(cfg),
+                                           prebuilt, device, C.byref(h)))
+        else:
+            _ffi.check(L.within_solver_new_tuned(d.h, _ffi.ptr(w), None if cfg is None else C.byref(cfg),
+                                                 prebuilt, device, C.byref(tn), C.byref(h)))
         self._h = h
         self._n_obs = int(L.within_solver_n_obs(h))
         self._n_dofs = int(L.within_solver_n_dofs(h))

@@ -71,6 +71,12 @@ STOP_REASONS = ["ZeroRhs", "InitialNormalEquationResidualZero", "ResidualToleran
                 "WarmStartExact", "MaxIterations", "Escalated"]
 
 
+class TuningC(C.Structure):
+    _fields_ = [("staged_sweep", C.c_int32), ("wide_mean_len", C.c_uint32), ("fuse_rounds", C.c_int32),
+                ("thread_per_segment", C.c_int32), ("core_dense_max", C.c_uint32), ("core_min_frac", C.c_double),
+                ("max_rounds", C.c_uint32), ("core_small", C.c_uint32), ("core_dense_late", C.c_uint32)]
+
+
 class PrecondStatsC(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in ("n", "n_subdomains", "n_slots", "nnz_c", "nnz_ct", "nnz_fwd",
                                           "nnz_bwd", "nnz_dense", "nnz_core", "n_reduced", "n_rounds")]
@@ -112,6 +118,8 @@ _SIGNATURES = [
     ("within_preconditioner_n", U64, [P]),
     ("within_preconditioner_variant_name", C.c_char_p, [P]),
     ("within_preconditioner_stats", C.c_int, [P, P]),
+    ("within_tuning_default", None, [P]),
+    ("within_solver_new_tuned", C.c_int, [P, P, P, P, C.c_int32, P, P]),
     ("within_solver_solve_batch_device_ext", C.c_int, [P, P, U64, P, P, P, P, P, P, P]),
     ("within_preconditioner_serialize", C.c_int, [P, P, U64, P]),
     ("within_preconditioner_deserialize", C.c_int, [P, U64, C.c_int32, P]),

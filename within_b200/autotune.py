@@ -1,0 +1,158 @@
+"""Offline autotuner of the kernel variants and the factor stop rules.
+
+It writes ``tuning_table.json`` beside this file: one entry per
+representative design, keyed on statistics the binding can compute from a
+design before building it (observations, terms, the two largest level
+counts, slopes, weights), with the ``within_tuning`` record that was fastest
+for that design.  ``Solver(..., tuning="auto")`` (the default) picks the
+entry nearest to its own design and passes the record to
+``within_solver_new_tuned``: the choice is a deterministic function of the
+design, so results stay bitwise reproducible from run to run -- a timed
+choice made at run time would not be.
+
+The search is one pass of coordinate descent per design from the defaults:
+each knob in turn over its candidate values, keeping the best.  The cost of a
+record is the set-up time plus five solves (a preconditioner reused five
+times), each solve one FP64 right-hand side at tol 1e-8 timed on the device.
+
+Run on a GPU:  python -m within_b200.autotune [--out PATH] [--quick]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE = os.path.join(HERE, "tuning_table.json")
+
+# candidate values per knob (within_tuning fields); UINT32_MAX = never
+U32_MAX = 0xFFFFFFFF
+CANDIDATES = {
+    "staged_sweep": [1, 0],
+    "wide_mean_len": [U32_MAX, 64, 256],
+    "fuse_rounds": [1, 0],
+    "core_min_frac": [0.3, 0.1, 0.5],
+    "core_dense_late": [512, 256, 1024],
+    "core_small": [16384, 0],
+}
+
+
+def design_key(n_obs: int, levels: list[int], slopes: bool, weighted: bool) -> list[float]:
+    """The lookup key: log2 of the observation count and of the two largest
+    level counts, the term count, and the slope / weight flags."""
+    lv = sorted(levels, reverse=True) + [1, 1]
+    return [math.log2(max(1, n_obs)), float(len(levels)), math.log2(max(1, lv[0])), math.log2(max(1, lv[1])),
+            1.0 if slopes else 0.0, 1.0 if weighted else 0.0]
+
+
+def key_distance(a, b) -> float:
+    w = [1.0, 2.0, 1.0, 1.0, 4.0, 1.0]
+    return sum(wi * abs(x - y) for wi, x, y in zip(w, a, b))
+
+
+def load_table(path: str = TABLE) -> list:
+    try:
+        with open(path) as f:
+            return json.load(f)["entries"]
+    except (OSError, ValueError, KeyError):
+        return []
+
+
+def lookup(key, table=None, max_distance: float = 8.0):
+    """The tuning record of the nearest table entry, or None beyond max_distance."""
+    table = load_table() if table is None else table
+    best, bd = None, float("inf")
+    for e in table:
+        d = key_distance(key, e["key"])
+        if d < bd:
+            best, bd = e, d
+    return dict(best["tuning"]) if best is not None and bd <= max_distance else None
+
+
+def _designs(quick: bool):
+    from . import workloads as WL
+    out = []
+    rng = np.random.default_rng(101)
+    n2 = 2_000_000
+    out.append(("akm panel 2M (worker / firm Pareto / year)", WL.akm_panel(n=n2, n_workers=n2 // 10, n_firms=n2 // 100),
+                None))
+    if not quick:
+        out.append(("akm panel 10M", WL.akm_panel(), None))
+    codes, _ = WL.fixest_like()
+    out.append(("fixest-like 1M x 3 FE (firm = i % n_firm)", codes, None))
+    codes, _ = WL.small_two_factor()
+    out.append(("two factor 100k uniform (500, 200)", codes, None))
+    n = 1_000_000
+    out.append(("three factor 1M uniform (20000, 3000, 40)",
+                np.asfortranarray(np.column_stack([rng.integers(0, 20_000, n), rng.integers(0, 3_000, n),
+                                                   rng.integers(0, 40, n)]).astype(np.uint32)), None))
+    out.append(("akm panel 2M weighted lognormal(0,1)", WL.akm_panel(n=n2, n_workers=n2 // 10, n_firms=n2 // 100),
+                rng.lognormal(0.0, 1.0, n2)))
+    return out
+
+
+def _cost(W, codes, weights, rec, y, reps=3):
+    import torch
+    t0 = time.perf_counter()
+    s = W.Solver(codes, weights=weights, tuning=rec)
+    setup = time.perf_counter() - t0
+    yd = torch.tensor(y, device="cuda")
+    opts = W.LsmrOptions(tol=1e-8)
+    s.solve_device(yd, opts)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        _, _, st = s.solve_device(yd, opts)
+    b.record()
+    torch.cuda.synchronize()
+    solve = a.elapsed_time(b) / 1e3 / reps
+    del s
+    return setup + 5 * solve, setup, solve, st[0][1]
+
+
+def tune(out_path: str = TABLE, quick: bool = False) -> dict:
+    import within_b200 as W
+    entries = []
+    for name, codes, weights in _designs(quick):
+        y = np.random.default_rng(7).standard_normal(codes.shape[0])
+        key = design_key(codes.shape[0], [int(codes[:, t].max()) + 1 for t in range(codes.shape[1])], False,
+                         weights is not None)
+        rec = W.default_tuning()
+        best = _cost(W, codes, weights, rec, y)
+        trail = [{"tuning": dict(rec), "cost_s": best[0], "setup_s": best[1], "solve_s": best[2],
+                  "iterations": best[3]}]
+        for knob, values in CANDIDATES.items():
+            for v in values:
+                if rec[knob] == v:
+                    continue
+                cand = dict(rec)
+                cand[knob] = v
+                c = _cost(W, codes, weights, cand, y)
+                trail.append({"tuning": cand, "cost_s": c[0], "setup_s": c[1], "solve_s": c[2],
+                              "iterations": c[3]})
+                if c[0] < 0.98 * best[0]:   # a 2 % margin against timing noise
+                    rec, best = cand, c
+        entries.append({"design": name, "key": key, "tuning": rec,
+                        "measured": {"cost_s": best[0], "setup_s": best[1], "solve_s": best[2],
+                                     "iterations": best[3]},
+                        "candidates": trail})
+        print(json.dumps({"design": name, "tuning": rec, "measured": entries[-1]["measured"]}), flush=True)
+    table = {"objective": "set-up + 5 x FP64 1-RHS solve at tol 1e-8 (device time), one coordinate-descent pass",
+             "entries": entries}
+    with open(out_path, "w") as f:
+        json.dump(table, f, indent=1)
+    return table
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=TABLE)
+    ap.add_argument("--quick", action="store_true", help="skip the 10M-row panel")
+    a = ap.parse_args()
+    tune(a.out, a.quick)

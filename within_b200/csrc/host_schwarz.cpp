@@ -398,11 +398,16 @@ Lap lap_from_edges(std::vector<Edge>& edges, uint32_t n) {
         std::vector<uint32_t> pos(start.begin(), start.end() - 1);
         for (const Edge& e : edges) srt[pos[e.lo]++] = e;
     }
-    for (uint32_t i = 0; i < n; ++i)
-        std::sort(srt.begin() + start[i], srt.begin() + start[i + 1], [](const Edge& a, const Edge& b) {
-            if (a.hi != b.hi) return a.hi < b.hi;
-            return a.w < b.w;
-        });
+    // each lo group sorts on its own (blocks of groups on host threads)
+    const uint32_t gblk = 4096;
+    par_for_each(((size_t)n + gblk - 1) / gblk, [&](size_t b) {
+        const uint32_t i1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)gblk);
+        for (uint32_t i = (uint32_t)(b * gblk); i < i1; ++i)
+            std::sort(srt.begin() + start[i], srt.begin() + start[i + 1], [](const Edge& a, const Edge& b2) {
+                if (a.hi != b2.hi) return a.hi < b2.hi;
+                return a.w < b2.w;
+            });
+    });
     std::vector<Edge> dd;
     dd.reserve(srt.size());
     for (auto& e : srt) {
@@ -428,33 +433,54 @@ Lap lap_from_edges(std::vector<Edge>& edges, uint32_t n) {
     }
     Lap L;
     L.n = n;
-    L.col.reserve(rp[n]);
-    L.val.reserve(rp[n]);
-    L.ptr.reserve((size_t)n + 1);
-    for (uint32_t i = 0; i < n; ++i) {
-        ent[fill[i]] = {i, diag[i]};
-        std::sort(ent.begin() + rp[i], ent.begin() + rp[i + 1]);
-        for (uint32_t q = rp[i]; q < rp[i + 1]; ++q) {
-            L.col.push_back(ent[q].first);
-            L.val.push_back(ent[q].second);
+    L.col.resize(rp[n]);
+    L.val.resize(rp[n]);
+    L.ptr.assign(rp.begin(), rp.end());
+    par_for_each(((size_t)n + gblk - 1) / gblk, [&](size_t b) {
+        const uint32_t i1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)gblk);
+        for (uint32_t i = (uint32_t)(b * gblk); i < i1; ++i) {
+            ent[fill[i]] = {i, diag[i]};
+            std::sort(ent.begin() + rp[i], ent.begin() + rp[i + 1]);
+            for (uint32_t q = rp[i]; q < rp[i + 1]; ++q) {
+                L.col[q] = ent[q].first;
+                L.val[q] = ent[q].second;
+            }
         }
-        L.ptr.push_back((uint32_t)L.col.size());
-    }
+    });
     return L;
 }
 
 Lap sampled_reduced(const Comp& c, uint64_t seed, uint32_t split) {
     const uint32_t ne = c.m.nr(), nk = c.m.nc();
+    // every eliminated vertex draws from its own seeded stream, so blocks of
+    // vertices sample on host threads and their edges concatenate in vertex
+    // order: the same edge list as one sequential pass
+    const uint32_t block = 16384;
+    const size_t nblk = ((size_t)ne + block - 1) / block;
+    std::vector<std::vector<Edge>> part(nblk);
+    par_for_each(nblk, [&](size_t b) {
+        std::vector<std::pair<uint32_t, double>> ent;
+        std::vector<Edge>& out = part[b];
+        const uint32_t k1 = (uint32_t)std::min<size_t>(ne, (b + 1) * (size_t)block);
+        for (uint32_t k = (uint32_t)(b * block); k < k1; ++k) {
+            ent.clear();
+            for (uint32_t a = c.m.c.ptr[k]; a < c.m.c.ptr[k + 1]; ++a) ent.push_back({c.m.c.col[a], c.m.c.val[a]});
+            if (ent.empty()) continue;
+            if (c.grounded && c.ground[k] > 0.0) ent.push_back({nk, c.ground[k]});
+            if (ent.size() <= 1) continue;
+            Rng r{mix64(seed * 0x100000001B3ull + k)};
+            sample_star(ent, split, r, out);
+        }
+    });
     std::vector<Edge> edges;
-    std::vector<std::pair<uint32_t, double>> ent;
-    for (uint32_t k = 0; k < ne; ++k) {
-        ent.clear();
-        for (uint32_t a = c.m.c.ptr[k]; a < c.m.c.ptr[k + 1]; ++a) ent.push_back({c.m.c.col[a], c.m.c.val[a]});
-        if (ent.empty()) continue;
-        if (c.grounded && c.ground[k] > 0.0) ent.push_back({nk, c.ground[k]});
-        if (ent.size() <= 1) continue;
-        Rng r{mix64(seed * 0x100000001B3ull + k)};
-        sample_star(ent, split, r, edges);
+    {
+        size_t tot = 0;
+        for (auto& v : part) tot += v.size();
+        edges.reserve(tot + (c.grounded ? nk : 0));
+        for (auto& v : part) {
+            edges.insert(edges.end(), v.begin(), v.end());
+            std::vector<Edge>().swap(v);
+        }
     }
     if (c.grounded)
         for (uint32_t i = 0; i < nk; ++i)

@@ -42,7 +42,8 @@ template <int K>
 constexpr int sr_items_wide() { return K == 1 ? 16 : (K == 2 ? 8 : sr_items<K>()); }
 template <int K>
 constexpr int sr_tile_wide() { return SR_THREADS * sr_items_wide<K>(); }
-// a problem takes wide tiles when its segments average at least this many positions
+// the mean segment length from which a plan may take wide tiles (a tuning
+// choice, within_tuning.wide_mean_len; off unless chosen)
 constexpr uint32_t SR_WIDE_MEAN_LEN = 64;
 // resident CTAs per SM the register budget is sized for (no spills at K = 8)
 // (the register footprint scales with K x the accumulator width)
@@ -282,6 +283,39 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
     }
 }
 
+// Sum of positions [a, b) of one segment by one thread, in position order.
+// Four positions' values are requested before any is added, so four load
+// chains (index, value, gathered operand) are in flight at once; the adds
+// still run in position order, so the sum has the bits of a plain loop.
+template <class F, int K>
+__device__ __forceinline__ void seg_sum(const F& f, const typename F::Prob& pr, uint32_t a, uint32_t b,
+                                        typename F::Acc (&acc)[K]) {
+    using A = typename F::Acc;
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = (A)0;
+    uint32_t q = a;
+    for (; q + 4 <= b; q += 4) {
+        A v0[K], v1[K], v2[K], v3[K];
+        f.value(pr, q, v0);
+        f.value(pr, q + 1, v1);
+        f.value(pr, q + 2, v2);
+        f.value(pr, q + 3, v3);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            acc[k] += v0[k];
+            acc[k] += v1[k];
+            acc[k] += v2[k];
+            acc[k] += v3[k];
+        }
+    }
+    for (; q < b; ++q) {
+        A v[K];
+        f.value(pr, q, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += v[k];
+    }
+}
+
 // One thread per segment, for a problem whose segments are all short (at
 // most SEGT_MAX_LEN positions, as the rows of C, the DOFs' slot lists and the
 // factor rows of most elimination rounds are): each thread sums its
@@ -301,14 +335,7 @@ segthread_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ ski
     const uint32_t* ptr = f.seg_ptr(pr);
     const uint32_t a = __ldg(ptr + sg), b = __ldg(ptr + sg + 1);
     A acc[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] = (A)0;
-    for (uint32_t q = a; q < b; ++q) {
-        A v[K];
-        f.value(pr, q, v);
-#pragma unroll
-        for (int k = 0; k < K; ++k) acc[k] += v[k];
-    }
+    seg_sum<F, K>(f, pr, a, b, acc);
     f.emit(pr, sg, acc);
 }
 
@@ -337,14 +364,7 @@ rounds_fused_kernel(F f, const uint32_t* __restrict__ round_rows, uint32_t r_lo,
         for (uint32_t sg = threadIdx.x; sg < n_seg; sg += RF_THREADS) {
             const uint32_t a = __ldg(ptr + sg), b = __ldg(ptr + sg + 1);
             A acc[K];
-#pragma unroll
-            for (int k = 0; k < K; ++k) acc[k] = (A)0;
-            for (uint32_t q = a; q < b; ++q) {
-                A v[K];
-                f.value(pr, q, v);
-#pragma unroll
-                for (int k = 0; k < K; ++k) acc[k] += v[k];
-            }
+            seg_sum<F, K>(f, pr, a, b, acc);
             f.emit(pr, sg, acc);
         }
         __syncthreads();   // the next round reads this round's results

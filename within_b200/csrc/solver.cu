@@ -20,6 +20,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -48,6 +49,26 @@ thread_local uint64_t g_launches = 0;
         if (e_ != cudaSuccess)                                                         \
             throw WError(ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));   \
     } while (0)
+
+// WITHIN_TRACE=1: host-side phase times of the set-up and of the lazy first
+// use of each column bucket, one line each on stderr (a diagnostic; no effect
+// on results)
+bool trace_on() {
+    static const bool on = [] {
+        const char* e = getenv("WITHIN_TRACE");
+        return e && atoi(e) != 0;
+    }();
+    return on;
+}
+double now_s();
+struct PhaseTrace {
+    const char* what;
+    double t0;
+    explicit PhaseTrace(const char* w) : what(w), t0(trace_on() ? now_s() : 0.0) {}
+    ~PhaseTrace() {
+        if (trace_on()) fprintf(stderr, "[within trace] %s %.3f ms\n", what, (now_s() - t0) * 1e3);
+    }
+};
 
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -94,14 +115,44 @@ struct DevPlan {
     std::vector<uint32_t> range_lo, range_hi;   // tile ranges (per round, for round plans)
 };
 
-// Tile size of a plan: wide tiles when K <= 2 and its segments average
-// SR_WIDE_MEAN_LEN positions or more.  Fixed by the design, so the summation
-// order is too.  WITHIN_WIDE_TILES=0: never.
-bool plan_wide(int K, uint64_t positions, uint64_t segments) {
-    if (K > 2) return false;
+// The per-solver choices of kernel variants and factor stop rules
+// (within_tuning of the C ABI), resolved once when the solver is built:
+// explicit fields of the caller's record, else the WITHIN_* environment
+// overrides, else the defaults.  Every choice is a function of the design and
+// this record only, so summation orders -- and results -- are reproducible.
+struct Tuning {
+    bool staged = true;          // staged (TMA) row sweep and gather where they apply
+    // plans whose segments average this many positions take wide tiles; off by
+    // default (on the 10M-row panel wide tiles made C^T, restrict, means and
+    // kept sums 1.5-2x slower: two blocks per SM hide less latency)
+    uint32_t wide_mean_len = UINT32_MAX;
+    bool fuse_rounds = true;     // the small tail of elimination rounds in one block
+    bool segthread = true;       // one thread per segment where every segment is short
+};
+
+Tuning resolve_tuning(const within_tuning* t) {
+    Tuning r;
+    if (t) {
+        r.staged = t->staged_sweep != 0;
+        r.wide_mean_len = t->wide_mean_len;
+        r.fuse_rounds = t->fuse_rounds != 0;
+        r.segthread = t->thread_per_segment != 0;
+        return r;
+    }
+    if (const char* e = getenv("WITHIN_TSWEEP")) r.staged = atoi(e) != 0;
     if (const char* e = getenv("WITHIN_WIDE_TILES"))
-        if (atoi(e) == 0) return false;
-    return segments > 0 && positions >= (uint64_t)SR_WIDE_MEAN_LEN * segments;
+        if (atoi(e) == 0) r.wide_mean_len = UINT32_MAX;
+    if (const char* e = getenv("WITHIN_FUSE_ROUNDS")) r.fuse_rounds = atoi(e) != 0;
+    if (const char* e = getenv("WITHIN_SEGTHREAD")) r.segthread = atoi(e) != 0;
+    return r;
+}
+
+// Tile size of a plan: wide tiles when K <= 2 and its segments average
+// wide_mean_len positions or more.  Fixed by the design and the tuning, so
+// the summation order is too.
+bool plan_wide(int K, uint64_t positions, uint64_t segments, uint32_t wide_mean_len) {
+    if (K > 2 || wide_mean_len == UINT32_MAX) return false;
+    return segments > 0 && positions >= (uint64_t)wide_mean_len * segments;
 }
 int plan_tile(int K, bool wide) {
     if (wide) return K == 1 ? sr_tile_wide<1>() : sr_tile_wide<2>();
@@ -350,6 +401,7 @@ struct KPlans {
 struct SchwarzUser {
     Arena arena;
     KPlans kp[4];
+    Tuning tuning;
 };
 
 within_preconditioner::~within_preconditioner() { delete standalone; }
@@ -365,7 +417,7 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     auto one = [&](const std::vector<uint32_t>& ptr) {
         HostPlan hp;
         const uint32_t n_seg = (uint32_t)ptr.size() - 1;
-        const bool wide = plan_wide(K, n_seg ? ptr[n_seg] - ptr[0] : 0, n_seg);
+        const bool wide = plan_wide(K, n_seg ? ptr[n_seg] - ptr[0] : 0, n_seg, U.tuning.wide_mean_len);
         hp.add(0, ptr.data(), n_seg, plan_tile(K, wide));
         DevPlan d = make_plan(A, hp, K);
         d.wide = wide;
@@ -379,8 +431,7 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     kp.dense = one(H.dense_rows_ptr);
     kp.c = one(H.c_ptr);
     kp.prolong = one(H.dof_ptr);
-    const char* segt = getenv("WITHIN_SEGTHREAD");
-    const bool segt_on = !(segt && atoi(segt) == 0);
+    const bool segt_on = U.tuning.segthread;
     if (segt_on && H.c_ptr.size() > 1 && seg_max_len(H.c_ptr.data(), H.c_ptr.size() - 1) <= SEGT_MAX_LEN)
         kp.c_thread = (uint32_t)(H.c_ptr.size() - 1);
     if (segt_on && H.dof_ptr.size() > 1 && seg_max_len(H.dof_ptr.data(), H.dof_ptr.size() - 1) <= SEGT_MAX_LEN)
@@ -414,8 +465,7 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     // the fused tail: the longest suffix of rounds that are one-thread rounds
     // in both directions with at most RF_MAX_ROWS rows (WITHIN_FUSE_ROUNDS=0: none)
     {
-        const char* fz = getenv("WITHIN_FUSE_ROUNDS");
-        const bool fuse_on = segt_on && !(fz && atoi(fz) == 0);
+        const bool fuse_on = segt_on && U.tuning.fuse_rounds;
         const uint32_t nr = H.n_rounds;
         uint32_t lo = nr;
         auto ok = [&](uint32_t r) {
@@ -714,8 +764,7 @@ size_t tg_smem(int nq, bool wtd, bool demean) {
 }
 // whether the staged gather applies to this solver's design (WITHIN_TSWEEP=0: never)
 bool tg_applies(const within_solver& s) {
-    if (const char* e = getenv("WITHIN_TSWEEP"))
-        if (atoi(e) == 0) return false;
+    if (!s.schwarz.tuning.staged) return false;
     if (s.design.terms.size() > (size_t)TS_MAXQ || s.design.terms.empty()) return false;
     for (const Term& T : s.design.terms)
         if (T.cols.size() != 1 || T.cols[0] >= 0) return false;
@@ -796,9 +845,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
             nhist += cls[t] == CLS_HIST;
             if (cls[t] == CLS_HIST) nbk += (int)D.terms[t].n_levels;
         }
-        bool ok = K == 1 && simple && Q <= TS_MAXQ && nrun >= 1;
-        if (const char* e = getenv("WITHIN_TSWEEP"))
-            if (atoi(e) == 0) ok = false;
+        const bool ok = K == 1 && simple && Q <= TS_MAXQ && nrun >= 1 && s.schwarz.tuning.staged;
         const size_t sm = ts_smem_bytes<K>(nbk, nhist, Q, s.op.sqrt_w != nullptr);
         if (ok && sm <= TS_SMEM_CAP) {
             rk.ts = true;
@@ -921,7 +968,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
             pos += lp.back() - lp.front();
             segs += lp.size() - 1;
         }
-        const bool wide = plan_wide(K, pos, segs);
+        const bool wide = plan_wide(K, pos, segs, s.schwarz.tuning.wide_mean_len);
         const int Ttile = plan_tile(K, wide);
         HostPlan hp;
         for (size_t i = 0; i < rk.rest_host.size(); ++i)
@@ -1048,6 +1095,7 @@ int env_path(int dflt) {
 within_solver::Work& ensure_work(within_solver& s, int K) {
     auto& w = s.work[kidx(K)];
     if (w.ready) return w;
+    PhaseTrace pt("first use of a column bucket: workspaces and plans");
     Arena& A = s.arena;
     w.u = A.alloc<double>(s.n_obs * K);
     w.b = A.alloc<double>(s.n_obs * K);
@@ -1152,6 +1200,7 @@ template <int K>
 bool build_loop_graph(within_solver& s, within_solver::Work& w) {
     if (w.loop_graph) return true;
     if (w.loop_failed) return false;
+    PhaseTrace pt("LSMR loop graph capture and instantiation");
     if (const char* e = getenv("WITHIN_GRAPH_LOOP"))
         if (atoi(e) == 0) {
             w.loop_failed = true;
@@ -1732,7 +1781,7 @@ int guarded(F f) {
 }
 
 within_solver* make_solver(const within_design* d, const double* weights, const within_precond_config* cfg,
-                           const within_preconditioner* prebuilt, int device) {
+                           const within_preconditioner* prebuilt, int device, const within_tuning* tuning = nullptr) {
     if (!d) throw WError(ERR_INVALID, "design is NULL");
     if (device < 0) CK(cudaGetDevice(&device));
     set_device(device);
@@ -1740,6 +1789,7 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
     s->device = device;
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     s->sweep_err = s->arena.alloc<int>(1);
+    s->schwarz.tuning = resolve_tuning(tuning);
     std::vector<EffectIn> effs;
     for (size_t e = 0; e < d->levels.size(); ++e) {
         EffectIn ef;
@@ -1748,7 +1798,11 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         for (size_t j : d->slope_of[e]) ef.slopes.push_back(d->slopes[j].data());
         effs.push_back(ef);
     }
-    s->design = make_design(d->n_obs, effs);
+    PhaseTrace pt_all("Solver::new total");
+    {
+        PhaseTrace pt("design build (locality sort)");
+        s->design = make_design(d->n_obs, effs);
+    }
     HostDesign& D = s->design;
     s->n_obs = D.n_obs;
     s->n_dofs = D.n_dofs;
@@ -1787,13 +1841,27 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
             pc.scaling_error = cfg->scaling_error != 0;
             if (pc.kind < 0 || pc.kind > 2) throw WError(ERR_INVALID, "unknown preconditioner kind");
         }
-        // tuning of the round-parallel factor (see PrecondCfg)
-        if (const char* e = getenv("WITHIN_CORE_DENSE_MAX")) pc.core_dense_max = (uint32_t)atol(e);
-        if (const char* e = getenv("WITHIN_CORE_MIN_FRAC")) pc.core_min_frac = atof(e);
-        if (const char* e = getenv("WITHIN_MAX_ROUNDS")) pc.max_rounds = (uint32_t)atol(e);
-        if (const char* e = getenv("WITHIN_CORE_SMALL")) pc.core_small = (uint32_t)atol(e);
-        if (const char* e = getenv("WITHIN_CORE_DENSE_LATE")) pc.core_dense_late = (uint32_t)atol(e);
-        BuildResult br = build_preconditioner(D, weights ? w.data() : nullptr, pc);
+        // stop rules of the round-parallel factor (see PrecondCfg): the
+        // caller's tuning record, else the environment overrides
+        if (tuning) {
+            pc.core_dense_max = tuning->core_dense_max;
+            pc.core_min_frac = tuning->core_min_frac;
+            pc.max_rounds = tuning->max_rounds;
+            pc.core_small = tuning->core_small;
+            pc.core_dense_late = tuning->core_dense_late;
+        } else {
+            if (const char* e = getenv("WITHIN_CORE_DENSE_MAX")) pc.core_dense_max = (uint32_t)atol(e);
+            if (const char* e = getenv("WITHIN_CORE_MIN_FRAC")) pc.core_min_frac = atof(e);
+            if (const char* e = getenv("WITHIN_MAX_ROUNDS")) pc.max_rounds = (uint32_t)atol(e);
+            if (const char* e = getenv("WITHIN_CORE_SMALL")) pc.core_small = (uint32_t)atol(e);
+            if (const char* e = getenv("WITHIN_CORE_DENSE_LATE")) pc.core_dense_late = (uint32_t)atol(e);
+        }
+        BuildResult br;
+        {
+            PhaseTrace pt("preconditioner host build");
+            br = build_preconditioner(D, weights ? w.data() : nullptr, pc);
+        }
+        PhaseTrace pt_up("preconditioner upload");
         s->n_warnings = br.n_warnings;
         if (br.kind != 0) {
             auto* P = new within_preconditioner();
@@ -1814,6 +1882,7 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         }
     }
     // design operator on the device
+    PhaseTrace pt_op("design upload and scatter orders");
     Arena& A = s->arena;
     OpParams& op = s->op;
     op.n = (uint32_t)D.n_obs;
@@ -1906,6 +1975,9 @@ struct Staging {
     within_solver& s;
     cudaStream_t st;
     static constexpr size_t CHUNK = (size_t)16 << 20;   // bytes per slot
+    // copies up to this size skip the slots (allocating them costs more than
+    // the overlap gains)
+    static constexpr size_t SMALL = (size_t)32 << 20;
     char* slot[2] = {nullptr, nullptr};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     Staging(within_solver& s_, cudaStream_t st_) : s(s_), st(st_) {}
@@ -1925,7 +1997,7 @@ struct Staging {
     }
     void h2d(void* dst, const void* src, size_t bytes) {
         if (!bytes) return;
-        if (is_pinned(src)) {
+        if (is_pinned(src) || bytes <= SMALL) {   // small pageable copies: the driver's own staging
             CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
             return;
         }
@@ -1942,7 +2014,7 @@ struct Staging {
     // device -> host; returns after the data is in dst
     void d2h(void* dst, const void* src, size_t bytes) {
         if (!bytes) return;
-        if (is_pinned(dst)) {
+        if (is_pinned(dst) || bytes <= SMALL) {
             CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             return;
@@ -1991,8 +2063,12 @@ void host_solve(within_solver& s, const double* Y, uint64_t k, const within_lsmr
         }
     } fr{s.stream, dY, dX, dD};
     Staging io(s, s.stream);
-    io.h2d(dY, Y, k * n * sizeof(double));
+    {
+        PhaseTrace pt("host -> device copy of the right-hand sides");
+        io.h2d(dY, Y, k * n * sizeof(double));
+    }
     dispatch_solve(s, dY, k, tol, maxiter, X ? dX : nullptr, Dm ? dD : nullptr, stats, s.stream, ls);
+    PhaseTrace pt_out("device -> host copy of the results");
     if (Dm) io.d2h(Dm, dD, k * n * sizeof(double));
     if (X) {
         io.d2h(X, dX, k * nd * sizeof(double));
@@ -2128,6 +2204,31 @@ int within_solver_new(const within_design* design, const double* weights, const 
                       const within_preconditioner* prebuilt, int32_t device, within_solver** out) {
     *out = nullptr;
     return guarded([&] { *out = make_solver(design, weights, cfg, prebuilt, device); });
+}
+
+void within_tuning_default(within_tuning* t) {
+    if (!t) return;
+    t->staged_sweep = 1;
+    t->wide_mean_len = UINT32_MAX;
+    t->fuse_rounds = 1;
+    t->thread_per_segment = 1;
+    PrecondCfg pc;
+    t->core_dense_max = pc.core_dense_max;
+    t->core_min_frac = pc.core_min_frac;
+    t->max_rounds = pc.max_rounds;
+    t->core_small = pc.core_small;
+    t->core_dense_late = pc.core_dense_late;
+}
+
+int within_solver_new_tuned(const within_design* design, const double* weights, const within_precond_config* cfg,
+                            const within_preconditioner* prebuilt, int32_t device, const within_tuning* tuning,
+                            within_solver** out) {
+    *out = nullptr;
+    return guarded([&] {
+        if (tuning && !(tuning->core_min_frac >= 0.0 && tuning->core_min_frac <= 1.0))
+            throw WError(ERR_INVALID, "tuning: core_min_frac must lie in [0, 1]");
+        *out = make_solver(design, weights, cfg, prebuilt, device, tuning);
+    });
 }
 
 int within_solvers_new(uint64_t n, const within_design* const* designs, const double* const* weights,
@@ -2552,7 +2653,10 @@ int within_preconditioner_apply(const within_preconditioner* pc, const double* x
             ++g_launches;
         } else {
             std::lock_guard<std::mutex> g(p->mu);
-            if (!p->standalone) p->standalone = new SchwarzUser();
+            if (!p->standalone) {
+                p->standalone = new SchwarzUser();
+                p->standalone->tuning = resolve_tuning(nullptr);
+            }
             schwarz_apply<1>(*p, *p->standalone, x_dev, y_dev, nullptr, st);
         }
         CK(cudaGetLastError());
