@@ -399,7 +399,7 @@ Lap lap_from_edges(std::vector<Edge>& edges, uint32_t n) {
         for (const Edge& e : edges) srt[pos[e.lo]++] = e;
     }
     // each lo group sorts on its own (blocks of groups on host threads)
-    const uint32_t gblk = 4096;
+    const uint32_t gblk = 256;
     par_for_each(((size_t)n + gblk - 1) / gblk, [&](size_t b) {
         const uint32_t i1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)gblk);
         for (uint32_t i = (uint32_t)(b * gblk); i < i1; ++i)
@@ -414,39 +414,39 @@ Lap lap_from_edges(std::vector<Edge>& edges, uint32_t n) {
         if (!dd.empty() && dd.back().lo == e.lo && dd.back().hi == e.hi) dd.back().w += e.w;
         else dd.push_back(e);
     }
-    // rows in one flat array: every edge at both ends, then the diagonal,
-    // each row sorted by (column, value)
-    std::vector<uint32_t> rp(n + 1, 0);
+    // rows in one flat array sorted by column without a sort: dd is ordered
+    // by (lo, hi), so the edges reaching row i from below (hi == i) arrive in
+    // ascending lo and those leaving it upwards (lo == i) in ascending hi;
+    // row i is [lower neighbours, i, upper neighbours]
+    std::vector<uint32_t> rp(n + 1, 0), nlow(n, 0);
     for (auto& e : dd) {
         ++rp[e.lo + 1];
         ++rp[e.hi + 1];
+        ++nlow[e.hi];
     }
     for (uint32_t i = 0; i < n; ++i) rp[i + 1] += rp[i] + 1;
-    std::vector<std::pair<uint32_t, double>> ent(rp[n]);
-    std::vector<uint32_t> fill(rp.begin(), rp.end() - 1);
-    std::vector<double> diag(n, 0.0);
-    for (auto& e : dd) {
-        ent[fill[e.lo]++] = {e.hi, -e.w};
-        ent[fill[e.hi]++] = {e.lo, -e.w};
-        diag[e.lo] += e.w;
-        diag[e.hi] += e.w;
-    }
     Lap L;
     L.n = n;
     L.col.resize(rp[n]);
     L.val.resize(rp[n]);
     L.ptr.assign(rp.begin(), rp.end());
-    par_for_each(((size_t)n + gblk - 1) / gblk, [&](size_t b) {
-        const uint32_t i1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)gblk);
-        for (uint32_t i = (uint32_t)(b * gblk); i < i1; ++i) {
-            ent[fill[i]] = {i, diag[i]};
-            std::sort(ent.begin() + rp[i], ent.begin() + rp[i + 1]);
-            for (uint32_t q = rp[i]; q < rp[i + 1]; ++q) {
-                L.col[q] = ent[q].first;
-                L.val[q] = ent[q].second;
-            }
-        }
-    });
+    std::vector<uint32_t> lo_fill(rp.begin(), rp.end() - 1), up_fill(n);
+    for (uint32_t i = 0; i < n; ++i) up_fill[i] = rp[i] + nlow[i] + 1;
+    std::vector<double> diag(n, 0.0);
+    for (auto& e : dd) {
+        const uint32_t a = up_fill[e.lo]++, b = lo_fill[e.hi]++;
+        L.col[a] = e.hi;
+        L.val[a] = -e.w;
+        L.col[b] = e.lo;
+        L.val[b] = -e.w;
+        diag[e.lo] += e.w;
+        diag[e.hi] += e.w;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t q = rp[i] + nlow[i];
+        L.col[q] = i;
+        L.val[q] = diag[i];
+    }
     return L;
 }
 
@@ -607,6 +607,7 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
     std::vector<std::pair<uint32_t, double>> ent;
     uint32_t r = 0;
     double last_frac = 1.0;
+    bool dense_graph = false;   // see the stop rules below
     while (!live.empty()) {
         // compact adjacency: drop dead neighbours, merge parallel edges
         for (uint32_t v : live) {
@@ -637,15 +638,24 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
         // core_min_frac of the vertices eliminated) or at max_rounds, keeps
         // only its diagonal -- its intra-core edges are dropped, which leaves
         // an SDD (positive semi-definite) approximation of the core.
-        // A graph of at most core_small vertices (a few thousand kept levels
+        // A graph whose rounds stall while nearly all of it is still alive
+        // (more than DENSE_ALIVE of the vertices: a few thousand kept levels
         // with a dense or banded Schur complement, where every round removes
-        // only a few per cent) keeps eliminating until core_dense_late remain:
-        // its diagonal alone would leave the preconditioner far from exact.
-        const bool tiny_graph = live.size() <= cfg.core_small;
-        const uint32_t dense_at = r == 0 ? cfg.core_dense_max : std::min(cfg.core_dense_max, cfg.core_dense_late);
+        // only a few per cent) and that has at most core_small vertices keeps
+        // eliminating until core_dense_late remain: its diagonal alone would
+        // leave almost the whole reduced system approximated by its diagonal.
+        // A graph that stalls after its rounds removed a good part of it (the
+        // worker/firm panels) stops as before.
+        constexpr double DENSE_ALIVE = 0.8;
+        const bool plain_stall = last_frac < cfg.core_min_frac || r >= cfg.max_rounds;
+        if (!dense_graph && plain_stall && r > 0 && live.size() <= cfg.core_small &&
+            (double)live.size() > DENSE_ALIVE * (double)n)
+            dense_graph = true;
+        const uint32_t dense_at =
+            dense_graph ? std::min(cfg.core_dense_max, cfg.core_dense_late) : cfg.core_dense_max;
         const bool small = live.size() <= dense_at && live.size() > 1;
-        const bool stalled = (tiny_graph ? last_frac < cfg.core_min_frac_small : last_frac < cfg.core_min_frac) ||
-                             r >= (tiny_graph ? 4 * cfg.max_rounds : cfg.max_rounds);
+        const bool stalled = dense_graph ? (last_frac < cfg.core_min_frac_small || r >= 4 * cfg.max_rounds)
+                                         : plain_stall;
         if (small || (stalled && live.size() > 1)) {
             f.core = live;
             std::sort(f.core.begin(), f.core.end());

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -1818,6 +1819,16 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
     }
     s->reparam = build_reparam(D, weights ? w.data() : nullptr);
     // preconditioner (operator/schwarz.rs:231-270)
+    BuildResult pre;
+    PrecondCfg pre_cfg;
+    std::exception_ptr pre_err;
+    std::thread pre_thread;
+    struct Joiner {   // the host build never outlives this frame, whatever throws
+        std::thread& t;
+        ~Joiner() {
+            if (t.joinable()) t.join();
+        }
+    } pre_join{pre_thread};
     if (prebuilt) {
         if (prebuilt->n != D.n_dofs)
             throw WError(ERR_DIMENSION, "prebuilt preconditioner shape (" + std::to_string(prebuilt->n) + "x" +
@@ -1856,30 +1867,18 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
             if (const char* e = getenv("WITHIN_CORE_SMALL")) pc.core_small = (uint32_t)atol(e);
             if (const char* e = getenv("WITHIN_CORE_DENSE_LATE")) pc.core_dense_late = (uint32_t)atol(e);
         }
-        BuildResult br;
-        {
-            PhaseTrace pt("preconditioner host build");
-            br = build_preconditioner(D, weights ? w.data() : nullptr, pc);
-        }
-        PhaseTrace pt_up("preconditioner upload");
-        s->n_warnings = br.n_warnings;
-        if (br.kind != 0) {
-            auto* P = new within_preconditioner();
-            P->device = device;
-            P->kind = br.kind;
-            P->n = (uint32_t)D.n_dofs;
+        // the host build runs on its own thread while this one uploads the
+        // design and builds its scatter orders and sweep plans (both only read
+        // the host design)
+        pre_cfg = pc;
+        pre_thread = std::thread([&] {
             try {
-                if (br.kind == 2) {
-                    P->inv_diag = P->arena.upload(br.inv_diag);
-                    P->host_inv_diag = br.inv_diag;
-                }
-                else upload_schwarz(*P, std::move(br.schwarz));
+                PhaseTrace pt("preconditioner host build");
+                pre = build_preconditioner(D, weights ? w.data() : nullptr, pre_cfg);
             } catch (...) {
-                delete P;
-                throw;
+                pre_err = std::current_exception();
             }
-            s->precond = P;
-        }
+        });
     }
     // design operator on the device
     PhaseTrace pt_op("design upload and scatter orders");
@@ -1928,6 +1927,34 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         }
     }
     s->scatter_probs = A.upload(s->scatter_host);
+    if (pre_thread.joinable()) {
+        {   // single-column plans of the sweep need only the design: built before the join
+            PhaseTrace pt("single-column sweep plans");
+            ensure_scatter(*s, 1);
+            if (env_path(2) == 2) ensure_rowsweep<1>(*s);
+        }
+        pre_thread.join();
+        if (pre_err) std::rethrow_exception(pre_err);
+        PhaseTrace pt_up("preconditioner upload");
+        s->n_warnings = pre.n_warnings;
+        if (pre.kind != 0) {
+            auto* P = new within_preconditioner();
+            P->device = device;
+            P->kind = pre.kind;
+            P->n = (uint32_t)D.n_dofs;
+            try {
+                if (pre.kind == 2) {
+                    P->inv_diag = P->arena.upload(pre.inv_diag);
+                    P->host_inv_diag = pre.inv_diag;
+                }
+                else upload_schwarz(*P, std::move(pre.schwarz));
+            } catch (...) {
+                delete P;
+                throw;
+            }
+            s->precond = P;
+        }
+    }
     CK(cudaDeviceSynchronize());
     return s.release();
 }
