@@ -249,9 +249,8 @@ int within_solver_operator_apply_adjoint(within_solver* s, const double* u_dev, 
  * the reduction's scratch (per-tile partial sums, per-split completion
  * counters) lives in one 8 MiB static device array of the library instead of
  * solver-owned memory, and the call allocates nothing.
- *  - The solver's single-column tile plan must already exist: the solver's
- *    first single-RHS solve or within_solver_operator_apply_adjoint builds
- *    it; before that the call returns WITHIN_ERR_INVALID_INPUT.
+ *  - It uses the solver's single-column tile plan, which the solver builds at
+ *    construction, so the call works on a fresh solver.
  *  - A design whose reduction needs more than 8 MiB of scratch (about
  *    700,000 tiles of 2,048 observations, i.e. more than 10^9 observation x
  *    term pairs) is rejected with WITHIN_ERR_UNSUPPORTED and a message giving

@@ -43,10 +43,10 @@ def test_noalloc_adjoint_matches_existing_two_calls(wb):
         np.testing.assert_allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=1e-12, atol=1e-12)
 
 
-def test_noalloc_adjoint_on_callers_stream_and_before_any_plan(wb):
-    """On the caller's own stream (torch's current stream, no wait inside the
-    call) it matches the existing entry point; on a fresh solver, before the
-    single-column plan exists, it refuses with WITHIN_ERR_INVALID_INPUT."""
+def test_noalloc_adjoint_on_callers_stream_and_on_a_fresh_solver(wb):
+    """On a fresh solver (no solve or adjoint call yet: the single-column plan
+    is built at construction) and on the caller's own stream (torch's current
+    stream, no wait inside the call) it matches the existing entry point."""
     import torch
     from within_b200 import _ffi
     L = _ffi.lib()
@@ -54,23 +54,24 @@ def test_noalloc_adjoint_on_callers_stream_and_before_any_plan(wb):
     n = 50_000
     cats = np.asfortranarray(np.column_stack([rng.integers(0, 4_000, n), rng.integers(0, 300, n)])
                              .astype(np.uint32))
-    fresh = wb.Solver(cats, preconditioner=wb.PreconditionerConfig.Diagonal)
-    u = torch.tensor(rng.standard_normal(n), device="cuda")
-    out = torch.zeros(fresh.n_dofs, dtype=torch.float64, device="cuda")
-    torch.cuda.synchronize()
-    rc = L.within_solver_operator_apply_adjoint_noalloc(fresh.handle, C.c_void_p(u.data_ptr()),
-                                                        C.c_void_p(out.data_ptr()), None)
-    assert rc == 1, rc   # WITHIN_ERR_INVALID_INPUT
-    assert b"plan" in L.within_last_error()
-    ref = torch.empty_like(out)
-    fresh.operator_apply_adjoint_device(u, ref)
-    torch.cuda.synchronize()
-    stream = torch.cuda.Stream()
-    with torch.cuda.stream(stream):
-        for _ in range(2):
-            out.fill_(float("nan"))
-            _ffi.check(L.within_solver_operator_apply_adjoint_noalloc(
-                fresh.handle, C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()),
-                C.c_void_p(stream.cuda_stream)))
-            stream.synchronize()
-            np.testing.assert_allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=1e-12, atol=1e-12)
+    for pc in (wb.PreconditionerConfig.Diagonal, wb.PreconditionerConfig.Off):
+        fresh = wb.Solver(cats, preconditioner=pc)
+        u = torch.tensor(rng.standard_normal(n), device="cuda")
+        out = torch.full((fresh.n_dofs,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        _ffi.check(L.within_solver_operator_apply_adjoint_noalloc(fresh.handle, C.c_void_p(u.data_ptr()),
+                                                                  C.c_void_p(out.data_ptr()), None))
+        first = out.cpu().numpy()
+        ref = torch.empty_like(out)
+        fresh.operator_apply_adjoint_device(u, ref)
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(first, ref.cpu().numpy(), rtol=1e-12, atol=1e-12)
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                out.fill_(float("nan"))
+                _ffi.check(L.within_solver_operator_apply_adjoint_noalloc(
+                    fresh.handle, C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()),
+                    C.c_void_p(stream.cuda_stream)))
+                stream.synchronize()
+                np.testing.assert_allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=1e-12, atol=1e-12)

@@ -1927,12 +1927,13 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         }
     }
     s->scatter_probs = A.upload(s->scatter_host);
+    {   // single-column plans of the sweep need only the design: built at construction
+        // (while the preconditioner's host build, if any, runs on its thread)
+        PhaseTrace pt("single-column sweep plans");
+        ensure_scatter(*s, 1);
+        if (env_path(2) == 2) ensure_rowsweep<1>(*s);
+    }
     if (pre_thread.joinable()) {
-        {   // single-column plans of the sweep need only the design: built before the join
-            PhaseTrace pt("single-column sweep plans");
-            ensure_scatter(*s, 1);
-            if (env_path(2) == 2) ensure_rowsweep<1>(*s);
-        }
         pre_thread.join();
         if (pre_err) std::rethrow_exception(pre_err);
         PhaseTrace pt_up("preconditioner upload");
@@ -2768,8 +2769,7 @@ extern "C" int within_solver_operator_apply_adjoint_noalloc(within_solver* s, co
         if (!s->scatter_ready[0])
             throw WError(ERR_INVALID,
                          "within_solver_operator_apply_adjoint_noalloc: the solver's single-column tile plan "
-                         "does not exist yet; it is built by the solver's first single-RHS solve or "
-                         "within_solver_operator_apply_adjoint call");
+                         "is missing (it is built at construction)");
         const DevPlan& pl = s->scatter_plan[0];
         const size_t head_b = align256((size_t)pl.n_tiles * sizeof(double));
         const size_t tail_b = align256((size_t)std::max<uint32_t>(1, pl.n_splits) * sizeof(double));
