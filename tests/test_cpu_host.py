@@ -55,6 +55,20 @@ def test_tile_planner_properties(tmp_path):
     assert "plan ok" in out
 
 
+def test_segsweep_planner_and_warp_algorithm(tmp_path):
+    """The warp-range segmented sweep (segsweep.cuh) executed lane by lane on
+    the host over random multi-problem layouts planned by SSHostPlan::add:
+    every segment emitted once with its exact sum, every position read once,
+    every table index in range (tests/cpp/segsweep_test.cpp)."""
+    exe = tmp_path / "segsweep_test"
+    csrc = os.path.join(ROOT, "within_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", csrc, "-o", str(exe),
+                    os.path.join(ROOT, "tests", "cpp", "segsweep_test.cpp"),
+                    os.path.join(csrc, "host_design.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert "segsweep ok" in out
+
+
 def test_schwarz_round_schedule_and_index_ranges(tmp_path):
     """The round-parallel approximate-Cholesky schedule (no row of a round
     reads a row of the same round, forward or backward) and the index range of

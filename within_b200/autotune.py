@@ -13,7 +13,7 @@ choice made at run time would not be.
 The search is one pass of coordinate descent per design from the defaults:
 each knob in turn over its candidate values, keeping the best by a margin of
 2 %.  The kernel knobs (staged sweep, wide tiles, fused rounds, one thread per
-segment) change only the solve, so they are judged by the solve's device
+segment, warp ranges) change only the solve, so they are judged by the solve's device
 time (median of 5 solves of one FP64 right-hand side at tol 1e-8); the stop
 rules of the round-parallel factor change the set-up too, so they are judged
 by the set-up time plus five solves (a preconditioner reused five times).
@@ -42,11 +42,12 @@ CANDIDATES = {
     "wide_mean_len": [U32_MAX, 64, 256],
     "fuse_rounds": [1, 0],
     "thread_per_segment": [1, 0],
+    "warp_ranges": [0, 1],
     "core_min_frac": [0.3, 0.1, 0.5],
     "core_dense_late": [512, 256, 1024],
     "core_small": [16384, 0],
 }
-KERNEL_KNOBS = {"staged_sweep", "wide_mean_len", "fuse_rounds", "thread_per_segment"}
+KERNEL_KNOBS = {"staged_sweep", "wide_mean_len", "fuse_rounds", "thread_per_segment", "warp_ranges"}
 
 
 def design_key(n_obs: int, levels: list[int], slopes: bool, weighted: bool) -> list[float]:

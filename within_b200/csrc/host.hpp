@@ -166,6 +166,22 @@ struct HostPlan {
     void add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, int tile);
 };
 
+// Range plan of the warp-range segmented sweep (segsweep.cuh): ranges of
+// `range_len` positions (a multiple of SS_ALIGN), the segment-start bitmap,
+// the ids of non-empty segments of problems that have empty ones, the empty
+// segments (emitted as zeros by the range holding their position) and the
+// split segments (positions in more than one range).
+struct SSHostPlan {
+    std::vector<SSRange> ranges;
+    std::vector<SSSplit> splits;
+    std::vector<uint32_t> bits;
+    std::vector<uint32_t> nz_ids;
+    std::vector<uint32_t> empties;
+    void add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, uint32_t range_len);
+};
+// range length for `positions` positions spread over about `warps` warps
+uint32_t ss_range_len(uint64_t positions, uint32_t warps);
+
 // dense generalised inverse of a symmetric PSD matrix (the preconditioner's dense route)
 std::vector<double> dense_pseudo_inverse(uint32_t n, const std::vector<double>& a);
 

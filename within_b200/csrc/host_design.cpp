@@ -304,4 +304,85 @@ void HostPlan::add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, int T)
     (void)base;
 }
 
+uint32_t ss_range_len(uint64_t positions, uint32_t warps) {
+    const uint64_t per = (positions + std::max<uint32_t>(1, warps) - 1) / std::max<uint32_t>(1, warps);
+    const uint64_t len = (per + SS_ALIGN - 1) / SS_ALIGN * SS_ALIGN;
+    return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(len, SS_ALIGN), 1u << 16);
+}
+
+void SSHostPlan::add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, uint32_t L) {
+    if (n_seg == 0) return;
+    const uint32_t ptr0 = ptr[0], pend = ptr[n_seg];
+    const uint32_t P = pend - ptr0;
+    // segment-start bitmap: bit (p - ptr0) is set where a non-empty segment
+    // starts; words past the last position cover the reads of a full last
+    // chunk (up to 3 words beyond it at 4 positions per lane)
+    const uint32_t word0 = (uint32_t)bits.size();
+    bits.resize((size_t)word0 + (P + 31) / 32 + 4, 0u);
+    std::vector<uint32_t> nz;   // non-empty segment ids in order
+    nz.reserve(n_seg);
+    bool has_empty = false;
+    for (uint32_t g = 0; g < n_seg; ++g) {
+        if (ptr[g + 1] > ptr[g]) {
+            nz.push_back(g);
+            const uint32_t b = ptr[g] - ptr0;
+            bits[(size_t)word0 + b / 32] |= 1u << (b % 32);
+        } else {
+            has_empty = true;
+        }
+    }
+    uint32_t nz_off = SS_IDENTITY;
+    if (has_empty) {
+        nz_off = (uint32_t)nz_ids.size();
+        nz_ids.insert(nz_ids.end(), nz.begin(), nz.end());
+    }
+    const uint32_t nr = P == 0 ? 1u : (P + L - 1) / L;
+    const uint32_t r_first = (uint32_t)ranges.size();
+    size_t q = 0;   // nz[q] is the non-empty segment holding the range's first position
+    for (uint32_t j = 0; j < nr; ++j) {
+        SSRange r{};
+        r.problem = problem;
+        r.p0 = ptr0 + j * L;
+        r.p1 = (uint32_t)std::min<uint64_t>((uint64_t)r.p0 + L, pend);
+        r.word0 = word0 + (j * L) / 32;
+        while (q + 1 < nz.size() && ptr[nz[q + 1]] <= r.p0) ++q;
+        r.o0 = (uint32_t)q;
+        r.head_split = -1;
+        r.tail_split = -1;
+        r.nz_off = nz_off;
+        ranges.push_back(r);
+    }
+    // split segments: positions in more than one range
+    for (size_t o = 0; o < nz.size(); ++o) {
+        const uint32_t g = nz[o], a = ptr[g] - ptr0, b = ptr[g + 1] - ptr0;
+        const uint32_t r0 = a / L, r1 = (b - 1) / L;
+        if (r1 == r0) continue;
+        const int id = (int)splits.size();
+        splits.push_back(SSSplit{problem, g, r_first + r0, r_first + r1});
+        ranges[r_first + r0].tail_split = id;
+        for (uint32_t t = r0 + 1; t <= r1; ++t) ranges[r_first + t].head_split = id;
+    }
+    // empty segments go to the range holding their position (the last range
+    // for those at the problem's end); the list is in range order
+    std::vector<uint32_t> cnt(nr, 0);
+    for (uint32_t g = 0; g < n_seg; ++g)
+        if (ptr[g + 1] == ptr[g]) {
+            const uint32_t rel = ptr[g] - ptr0;
+            ++cnt[std::min(nr - 1, rel / L)];
+        }
+    uint32_t e = (uint32_t)empties.size();
+    for (uint32_t j = 0; j < nr; ++j) {
+        ranges[r_first + j].e_lo = e;
+        e += cnt[j];
+        ranges[r_first + j].e_hi = ranges[r_first + j].e_lo;
+    }
+    empties.resize(e);
+    for (uint32_t g = 0; g < n_seg; ++g)
+        if (ptr[g + 1] == ptr[g]) {
+            const uint32_t rel = ptr[g] - ptr0;
+            SSRange& r = ranges[r_first + std::min(nr - 1, rel / L)];
+            empties[r.e_hi++] = g;
+        }
+}
+
 }  // namespace wgpu

@@ -12,6 +12,7 @@
 #include <cstdint>
 
 #include "segreduce.cuh"
+#include "segsweep.cuh"
 
 namespace wgpu {
 

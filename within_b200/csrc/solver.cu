@@ -114,6 +114,14 @@ struct DevPlan {
     uint32_t n_splits = 0;
     bool wide = false;   // tiles of sr_tile_wide<K>() positions (else sr_tile<K>())
     std::vector<uint32_t> range_lo, range_hi;   // tile ranges (per round, for round plans)
+    // warp-range plan (segsweep.cuh): n_tiles counts ranges, head holds one
+    // partial per range, tail / counters one per split segment
+    bool ss = false;
+    SSRange* ranges = nullptr;
+    SSSplit* ss_splits = nullptr;
+    uint32_t* bits = nullptr;
+    uint32_t* nz_ids = nullptr;
+    uint32_t* empties = nullptr;
 };
 
 // The per-solver choices of kernel variants and factor stop rules
@@ -129,6 +137,7 @@ struct Tuning {
     uint32_t wide_mean_len = UINT32_MAX;
     bool fuse_rounds = true;     // the small tail of elimination rounds in one block
     bool segthread = true;       // one thread per segment where every segment is short
+    bool warp_ranges = false;    // segmented reductions by warp ranges (segsweep.cuh), else block tiles
 };
 
 Tuning resolve_tuning(const within_tuning* t) {
@@ -138,6 +147,7 @@ Tuning resolve_tuning(const within_tuning* t) {
         r.wide_mean_len = t->wide_mean_len;
         r.fuse_rounds = t->fuse_rounds != 0;
         r.segthread = t->thread_per_segment != 0;
+        r.warp_ranges = t->warp_ranges != 0;
         return r;
     }
     if (const char* e = getenv("WITHIN_TSWEEP")) r.staged = atoi(e) != 0;
@@ -145,6 +155,7 @@ Tuning resolve_tuning(const within_tuning* t) {
         if (atoi(e) == 0) r.wide_mean_len = UINT32_MAX;
     if (const char* e = getenv("WITHIN_FUSE_ROUNDS")) r.fuse_rounds = atoi(e) != 0;
     if (const char* e = getenv("WITHIN_SEGTHREAD")) r.segthread = atoi(e) != 0;
+    if (const char* e = getenv("WITHIN_WARP_RANGES")) r.warp_ranges = atoi(e) != 0;
     return r;
 }
 
@@ -172,6 +183,34 @@ DevPlan make_plan(Arena& A, const HostPlan& hp, int K) {
     return d;
 }
 
+DevPlan make_ss_plan(Arena& A, const SSHostPlan& hp, int K) {
+    DevPlan d;
+    d.ss = true;
+    d.n_tiles = (uint32_t)hp.ranges.size();
+    d.n_splits = (uint32_t)hp.splits.size();
+    d.ranges = A.upload(hp.ranges);
+    d.ss_splits = A.upload(hp.splits);
+    d.bits = A.upload(hp.bits);
+    d.nz_ids = hp.nz_ids.empty() ? nullptr : A.upload(hp.nz_ids);
+    d.empties = hp.empties.empty() ? nullptr : A.upload(hp.empties);
+    d.head = A.alloc<double>(std::max<size_t>(1, hp.ranges.size()) * K);
+    d.tail = A.alloc<double>(std::max<size_t>(1, hp.splits.size()) * K);
+    d.counters = A.alloc<unsigned>(std::max<size_t>(1, hp.splits.size()));
+    return d;
+}
+
+// Warps a warp-range plan is cut for: one wave of the kernel's resident warps.
+uint32_t ss_target_warps(int K) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int blocks = K >= 8 ? 2 : (K >= 4 ? 3 : 4);
+    return (uint32_t)(sms * blocks * (SS_THREADS / 32));
+}
+
 template <class F, int K>
 void launch_segthread(const F& f, uint32_t prob, uint32_t n_seg, const int* skip, cudaStream_t st) {
     if (!n_seg) return;
@@ -183,6 +222,13 @@ void launch_segthread(const F& f, uint32_t prob, uint32_t n_seg, const int* skip
 template <class F, int K>
 void launch_sr(const F& f, const DevPlan& p, uint32_t lo, uint32_t hi, const int* skip, cudaStream_t st) {
     if (hi <= lo) return;
+    if (p.ss) {
+        constexpr uint32_t WPB = SS_THREADS / 32;
+        segsweep_kernel<F, K><<<(hi - lo + WPB - 1) / WPB, SS_THREADS, 0, st>>>(
+            f, p.ranges, lo, hi, p.bits, p.nz_ids, p.empties, p.ss_splits, p.head, p.tail, p.counters, skip);
+        ++g_launches;
+        return;
+    }
     if constexpr (K <= 2) {
         if (p.wide) {
             segreduce_kernel<F, K, sr_items_wide<K>()><<<hi - lo, SR_THREADS, 0, st>>>(
@@ -415,9 +461,18 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     const SchwarzHost& H = P.host;
     Arena& A = U.arena;
     const int T = plan_tile(K, false);
+    const bool ss = U.tuning.warp_ranges;
     auto one = [&](const std::vector<uint32_t>& ptr) {
-        HostPlan hp;
         const uint32_t n_seg = (uint32_t)ptr.size() - 1;
+        if (ss) {
+            SSHostPlan sp;
+            sp.add(0, ptr.data(), n_seg, ss_range_len(n_seg ? ptr[n_seg] - ptr[0] : 0, ss_target_warps(K)));
+            DevPlan d = make_ss_plan(A, sp, K);
+            d.range_lo = {0};
+            d.range_hi = {d.n_tiles};
+            return d;
+        }
+        HostPlan hp;
         const bool wide = plan_wide(K, n_seg ? ptr[n_seg] - ptr[0] : 0, n_seg, U.tuning.wide_mean_len);
         hp.add(0, ptr.data(), n_seg, plan_tile(K, wide));
         DevPlan d = make_plan(A, hp, K);
@@ -439,6 +494,21 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
         kp.prolong_thread = (uint32_t)(H.dof_ptr.size() - 1);
     kp.core = one(H.core_rows_ptr);
     auto rounds = [&](const std::vector<uint32_t>& rptr, const std::vector<uint32_t>& ptr) {
+        if (ss) {
+            SSHostPlan sp;
+            std::vector<uint32_t> lo, hi;
+            for (uint32_t r = 0; r + 1 < rptr.size(); ++r) {
+                const uint32_t* rp = ptr.data() + rptr[r];
+                const uint32_t m = rptr[r + 1] - rptr[r];
+                lo.push_back((uint32_t)sp.ranges.size());
+                sp.add(r, rp, m, ss_range_len(m ? rp[m] - rp[0] : 0, ss_target_warps(K)));
+                hi.push_back((uint32_t)sp.ranges.size());
+            }
+            DevPlan d = make_ss_plan(A, sp, K);
+            d.range_lo = lo;
+            d.range_hi = hi;
+            return d;
+        }
         HostPlan hp;
         std::vector<uint32_t> lo, hi;
         for (uint32_t r = 0; r + 1 < rptr.size(); ++r) {
@@ -969,13 +1039,21 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
             pos += lp.back() - lp.front();
             segs += lp.size() - 1;
         }
-        const bool wide = plan_wide(K, pos, segs, s.schwarz.tuning.wide_mean_len);
-        const int Ttile = plan_tile(K, wide);
-        HostPlan hp;
-        for (size_t i = 0; i < rk.rest_host.size(); ++i)
-            hp.add((uint32_t)i, rk.rest_ptrs[i].data(), (uint32_t)rk.rest_ptrs[i].size() - 1, Ttile);
-        rk.rest = make_plan(A, hp, K);
-        rk.rest.wide = wide;
+        if (s.schwarz.tuning.warp_ranges) {
+            SSHostPlan sp;
+            const uint32_t L = ss_range_len(pos, ss_target_warps(K));
+            for (size_t i = 0; i < rk.rest_host.size(); ++i)
+                sp.add((uint32_t)i, rk.rest_ptrs[i].data(), (uint32_t)rk.rest_ptrs[i].size() - 1, L);
+            rk.rest = make_ss_plan(A, sp, K);
+        } else {
+            const bool wide = plan_wide(K, pos, segs, s.schwarz.tuning.wide_mean_len);
+            const int Ttile = plan_tile(K, wide);
+            HostPlan hp;
+            for (size_t i = 0; i < rk.rest_host.size(); ++i)
+                hp.add((uint32_t)i, rk.rest_ptrs[i].data(), (uint32_t)rk.rest_ptrs[i].size() - 1, Ttile);
+            rk.rest = make_plan(A, hp, K);
+            rk.rest.wide = wide;
+        }
         rk.rest_probs = A.upload(rk.rest_host);
     }
     // dynamic shared memory above the default needs the opt-in (set outside any capture)
@@ -2246,6 +2324,7 @@ void within_tuning_default(within_tuning* t) {
     t->max_rounds = pc.max_rounds;
     t->core_small = pc.core_small;
     t->core_dense_late = pc.core_dense_late;
+    t->warp_ranges = 0;
 }
 
 int within_solver_new_tuned(const within_design* design, const double* weights, const within_precond_config* cfg,
