@@ -151,8 +151,9 @@ typedef struct {
     uint32_t max_rounds;        /* round budget (4x for graphs of at most core_small vertices) */
     uint32_t core_small;        /* graphs this small keep eliminating ... */
     uint32_t core_dense_late;   /* ... until this many vertices remain (then a dense core) */
-    int32_t warp_ranges;        /* 1: segmented reductions (Schwarz steps, adjoint combines) by warp ranges
-                                   over a segment-start bitmap; 0: by block tiles */
+    int32_t warp_ranges;        /* segmented reductions by warp ranges over a segment-start bitmap instead
+                                   of block tiles: 1 (default) C^T and the adjoint's combines, 2 every
+                                   tile plan, 0 none */
 } within_tuning;
 void within_tuning_default(within_tuning* t);
 int within_solver_new_tuned(const within_design* design, const double* weights,

@@ -1,5 +1,6 @@
-"""The warp-range segmented reductions (within_tuning.warp_ranges = 1,
-segsweep.cuh) against the oracle and against the block-tile engine: every
+"""The warp-range segmented reductions (within_tuning.warp_ranges = 1 for
+C^T and the adjoint's combines, 2 for every tile plan; segsweep.cuh)
+against the oracle and against the block-tile engine: every
 column bucket (K = 1, 2, 4, 8), FP64 and mixed precision, designs with empty
 levels (empty segments in the adjoint and Schwarz plans), a slope term, a
 deep round-scheduled factor, and run-to-run bitwise reproducibility."""
@@ -20,8 +21,8 @@ def rel_inf(a, b, y):
     assert e["inf_over_inf"] <= 1e-6, e
     return e["inf_over_l2"]
 
-WR = {"warp_ranges": 1}
-WR_ALL = {"warp_ranges": 1, "thread_per_segment": 0}   # also C, prolongation and every round
+WR = {"warp_ranges": 2}
+WR_ALL = {"warp_ranges": 2, "thread_per_segment": 0}   # also C, prolongation and every round
 
 
 def _panel(n=300_000, seed=31):
@@ -29,7 +30,7 @@ def _panel(n=300_000, seed=31):
     return WL.akm_panel(n=n, n_workers=n // 10, n_firms=n // 100, seed=seed)
 
 
-@pytest.mark.parametrize("tuning", [WR, WR_ALL, {"warp_ranges": 1, "staged_sweep": 0}])
+@pytest.mark.parametrize("tuning", [{"warp_ranges": 1}, WR, WR_ALL, {"warp_ranges": 1, "staged_sweep": 0}])
 def test_warp_ranges_match_oracle_panel(wb, oracle, tuning):
     codes = _panel()
     y = np.random.default_rng(32).standard_normal(codes.shape[0])
@@ -105,7 +106,7 @@ def test_warp_ranges_deep_factor(wb, oracle):
     n = 150_000
     cats = as_solver_categories([rng.integers(0, 20_000, n), rng.integers(0, 3_000, n), rng.integers(0, 12, n)])
     y = rng.standard_normal(n)
-    for tuning in (WR, WR_ALL, {"warp_ranges": 1, "fuse_rounds": 0}):
+    for tuning in (WR, WR_ALL, {"warp_ranges": 2, "fuse_rounds": 0}):
         r = wb.Solver(cats, tuning=tuning).solve(y, wb.LsmrOptions(tol=1e-10, maxiter=3000))
         o = oracle.OracleSolver(cats).solve(y, tol=1e-10, maxiter=3000)
         assert r.converged

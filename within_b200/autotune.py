@@ -42,7 +42,7 @@ CANDIDATES = {
     "wide_mean_len": [U32_MAX, 64, 256],
     "fuse_rounds": [1, 0],
     "thread_per_segment": [1, 0],
-    "warp_ranges": [0, 1],
+    "warp_ranges": [1, 0, 2],
     "core_min_frac": [0.3, 0.1, 0.5],
     "core_dense_late": [512, 256, 1024],
     "core_small": [16384, 0],

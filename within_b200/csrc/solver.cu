@@ -137,7 +137,11 @@ struct Tuning {
     uint32_t wide_mean_len = UINT32_MAX;
     bool fuse_rounds = true;     // the small tail of elimination rounds in one block
     bool segthread = true;       // one thread per segment where every segment is short
-    bool warp_ranges = false;    // segmented reductions by warp ranges (segsweep.cuh), else block tiles
+    // segmented reductions by warp ranges (segsweep.cuh) instead of block
+    // tiles: 1 = C^T and the adjoint's combines (rows of ~10-1000 positions,
+    // measured faster on the 10M-row panel), 2 = every tile plan (restrict,
+    // means, kept sums, rounds, ... measured slower there), 0 = none
+    int warp_ranges = 1;
 };
 
 Tuning resolve_tuning(const within_tuning* t) {
@@ -147,7 +151,7 @@ Tuning resolve_tuning(const within_tuning* t) {
         r.wide_mean_len = t->wide_mean_len;
         r.fuse_rounds = t->fuse_rounds != 0;
         r.segthread = t->thread_per_segment != 0;
-        r.warp_ranges = t->warp_ranges != 0;
+        r.warp_ranges = t->warp_ranges;
         return r;
     }
     if (const char* e = getenv("WITHIN_TSWEEP")) r.staged = atoi(e) != 0;
@@ -155,7 +159,7 @@ Tuning resolve_tuning(const within_tuning* t) {
         if (atoi(e) == 0) r.wide_mean_len = UINT32_MAX;
     if (const char* e = getenv("WITHIN_FUSE_ROUNDS")) r.fuse_rounds = atoi(e) != 0;
     if (const char* e = getenv("WITHIN_SEGTHREAD")) r.segthread = atoi(e) != 0;
-    if (const char* e = getenv("WITHIN_WARP_RANGES")) r.warp_ranges = atoi(e) != 0;
+    if (const char* e = getenv("WITHIN_WARP_RANGES")) r.warp_ranges = atoi(e);
     return r;
 }
 
@@ -461,10 +465,10 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     const SchwarzHost& H = P.host;
     Arena& A = U.arena;
     const int T = plan_tile(K, false);
-    const bool ss = U.tuning.warp_ranges;
-    auto one = [&](const std::vector<uint32_t>& ptr) {
+    const bool ss = U.tuning.warp_ranges >= 2;
+    auto one = [&](const std::vector<uint32_t>& ptr, bool ss_plan) {
         const uint32_t n_seg = (uint32_t)ptr.size() - 1;
-        if (ss) {
+        if (ss_plan) {
             SSHostPlan sp;
             sp.add(0, ptr.data(), n_seg, ss_range_len(n_seg ? ptr[n_seg] - ptr[0] : 0, ss_target_warps(K)));
             DevPlan d = make_ss_plan(A, sp, K);
@@ -481,18 +485,18 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
         d.range_hi = {d.n_tiles};
         return d;
     };
-    kp.restrict_ = one(H.loc_ptr);
-    kp.ct = one(H.ct_ptr);
-    kp.kept = one(H.kept_ptr);
-    kp.dense = one(H.dense_rows_ptr);
-    kp.c = one(H.c_ptr);
-    kp.prolong = one(H.dof_ptr);
+    kp.restrict_ = one(H.loc_ptr, ss);
+    kp.ct = one(H.ct_ptr, U.tuning.warp_ranges >= 1);
+    kp.kept = one(H.kept_ptr, ss);
+    kp.dense = one(H.dense_rows_ptr, ss);
+    kp.c = one(H.c_ptr, ss);
+    kp.prolong = one(H.dof_ptr, ss);
     const bool segt_on = U.tuning.segthread;
     if (segt_on && H.c_ptr.size() > 1 && seg_max_len(H.c_ptr.data(), H.c_ptr.size() - 1) <= SEGT_MAX_LEN)
         kp.c_thread = (uint32_t)(H.c_ptr.size() - 1);
     if (segt_on && H.dof_ptr.size() > 1 && seg_max_len(H.dof_ptr.data(), H.dof_ptr.size() - 1) <= SEGT_MAX_LEN)
         kp.prolong_thread = (uint32_t)(H.dof_ptr.size() - 1);
-    kp.core = one(H.core_rows_ptr);
+    kp.core = one(H.core_rows_ptr, ss);
     auto rounds = [&](const std::vector<uint32_t>& rptr, const std::vector<uint32_t>& ptr) {
         if (ss) {
             SSHostPlan sp;
@@ -1039,7 +1043,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
             pos += lp.back() - lp.front();
             segs += lp.size() - 1;
         }
-        if (s.schwarz.tuning.warp_ranges) {
+        if (s.schwarz.tuning.warp_ranges >= 1) {
             SSHostPlan sp;
             const uint32_t L = ss_range_len(pos, ss_target_warps(K));
             for (size_t i = 0; i < rk.rest_host.size(); ++i)
@@ -2324,7 +2328,7 @@ void within_tuning_default(within_tuning* t) {
     t->max_rounds = pc.max_rounds;
     t->core_small = pc.core_small;
     t->core_dense_late = pc.core_dense_late;
-    t->warp_ranges = 0;
+    t->warp_ranges = 1;
 }
 
 int within_solver_new_tuned(const within_design* design, const double* weights, const within_precond_config* cfg,
