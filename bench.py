@@ -54,11 +54,50 @@ def parse():
     ap.add_argument("--kernel-timeline", choices=["fp64", "mixed"], default=None,
                     help="instead of the bench line: per-kernel device times of one solve (torch.profiler "
                          "/ CUPTI timestamps); 'mixed' = weighted panel, k = 4, mixed precision")
+    ap.add_argument("--tuning", default="auto",
+                    help="tuning record of the headline solver: 'auto' (the autotuner's table), 'none' (the "
+                         "defaults and WITHIN_* overrides) or a JSON dict of within_tuning fields")
     ap.add_argument("--cpu-sample-iters", type=int, default=3)
     ap.add_argument("--ref-budget-s", type=float, default=150.0,
                     help="host seconds the reference arm's warm-up and timed steps may take before each "
                          "step becomes a bounded run of iterations")
     return ap.parse_args()
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# design-operator pair's kernels, from one ncu capture (--clock-control none)
+# of the 4,000,000-row panel: the staged gather k_tgather<3,0,0> (D x) and the
+# staged adjoint sweep k_tsweep<1,0,3,2,1,0> with its crossing-run fix-up
+# k_rw_fix<1,0> and the warp-range run combine segsweep_kernel<ScatterF<1,0>>
+# (D^T u).  Every stream of the pair grows with the row count on this panel
+# generator (workers n/10, firms n/100), so a 10,000,000-row launch moves 2.5x.
+PAIR_TRAFFIC_4M = {"gather": 51_800_064, "adjoint": 90_200_832}
+PAIR_TRAFFIC_KERNELS = "k_tgather<3,0,0> + k_tsweep<1,0,3,2,1,0> + k_rw_fix<1,0> + segsweep_kernel<ScatterF<1,0>>"
+
+
+def pair_traffic(n, q, solver):
+    """The pair's DRAM bytes per launch (gather + adjoint) scaled from the 4M-row
+    capture, or None when the workload or the kernels differ from the capture's."""
+    t = solver.tuning
+    if t is None:
+        staged = os.environ.get("WITHIN_TSWEEP", "1") != "0" and os.environ.get("WITHIN_SWEEP", "2") != "0"
+        ranges = int(os.environ.get("WITHIN_WARP_RANGES", "1"))
+    else:
+        staged, ranges = t.get("staged_sweep", 1) == 1, t.get("warp_ranges", 1)
+    if q != 3 or not staged or ranges < 1:
+        return None, None
+    f = n / 4_000_000
+    return (f * (PAIR_TRAFFIC_4M["gather"] + PAIR_TRAFFIC_4M["adjoint"]),
+            f"ncu capture of the 4,000,000-row panel x {f:g}: {PAIR_TRAFFIC_KERNELS}")
+
+
+def tuning_arg(args):
+    t = getattr(args, "tuning", "auto")
+    if t == "auto":
+        return "auto"
+    if t == "none":
+        return None
+    return json.loads(t)
 
 
 def workload(rows):
@@ -475,7 +514,7 @@ def run_ours(args):
     from within_b200 import _ffi
     codes, y = workload(args.rows)
     t0 = time.perf_counter()
-    solver = W.Solver(codes, device=local)
+    solver = W.Solver(codes, device=local, tuning=tuning_arg(args))
     t_setup = time.perf_counter() - t0
     n, nd = solver.n_obs, solver.n_dofs
     opts = W.LsmrOptions(tol=args.tol)
@@ -592,10 +631,7 @@ def run_ours(args):
     bytes_scatter = 4 * Q * n + 8 * n + 8 * nd         # codes/permutation, u, out
     achieved = (bytes_gather + bytes_scatter) / (t_gather + t_scatter) / 1e9
     peak, peak_kind = peaks()
-    # DRAM bytes per launch of the pair, ncu on the 10M-row panel (dram__bytes_read.sum +
-    # dram__bytes_write.sum of k_apply and of the adjoint row sweep; the small run-combine
-    # launch is not included): profiles/operator_traffic_akm10m.md
-    traffic = (128803072 + 45006848 + 201513472 + 15891200) if n == 10_000_000 else None
+    traffic, traffic_src = pair_traffic(n, Q, solver)
     pc = solver.preconditioner
     ps = pc.stats() if pc is not None else None
     ib = iteration_bytes(n, nd, Q, k=1, ps=ps)
@@ -607,9 +643,11 @@ def run_ours(args):
                      "kernels included in the time, not in the bytes)"}
     whole["frac_survey"] = whole["gbs_survey"] / peaks()[0]
     whole["frac_fused"] = whole["gbs_fused"] / peaks()[0]
-    roof = {"bound": "hbm", "kernel": "design operator pair (gather k_apply D v + row-sweep D^T u and its run combine)",
+    roof = {"bound": "hbm",
+            "kernel": "design operator pair: within_solver_operator_apply (D v) + "
+                      "within_solver_operator_apply_adjoint (D^T u), the kernels the solver selects for the design",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_kind": peak_kind, "traffic": traffic,
+            "peak_kind": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
             "gather_gbs": bytes_gather / t_gather / 1e9, "scatter_gbs": bytes_scatter / t_scatter / 1e9,
             "algorithmic_bytes_per_launch": {"gather": bytes_gather, "scatter": bytes_scatter}}
     line = {
@@ -736,11 +774,11 @@ def kernel_timeline(args):
     if args.kernel_timeline == "mixed":
         rng = np.random.default_rng(4)
         w = rng.lognormal(0.0, 1.0, codes.shape[0])
-        s = W.Solver(codes, weights=w, precision="mixed")
+        s = W.Solver(codes, weights=w, precision="mixed", tuning=tuning_arg(args))
         Y = torch.tensor(np.asfortranarray(rng.standard_normal((codes.shape[0], 4))), device=dev)
         Y = Y.t().contiguous().t()
     else:
-        s = W.Solver(codes)
+        s = W.Solver(codes, tuning=tuning_arg(args))
         Y = torch.tensor(y, device=dev)
     opts = W.LsmrOptions(tol=args.tol)
     for _ in range(2):

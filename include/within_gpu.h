@@ -154,6 +154,9 @@ typedef struct {
     int32_t warp_ranges;        /* segmented reductions by warp ranges over a segment-start bitmap instead
                                    of block tiles: 1 (default) C^T and the adjoint's combines, 2 every
                                    tile plan, 0 none */
+    int32_t gpu_cross_tab;      /* the additive-Schwarz set-up's cross-tabs on the GPU (sort and segment;
+                                   the same bits as on the host): 1 (default) for designs of at least
+                                   2^18 observations, 2 always, 0 never */
 } within_tuning;
 void within_tuning_default(within_tuning* t);
 int within_solver_new_tuned(const within_design* design, const double* weights,

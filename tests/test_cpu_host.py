@@ -69,6 +69,21 @@ def test_segsweep_planner_and_warp_algorithm(tmp_path):
     assert "segsweep ok" in out
 
 
+def test_schwarz_build_from_gpu_form_cross_tabs(tmp_path):
+    """The additive-Schwarz build from cross-tabs in the GPU cross-tab's form
+    (sorted keys, per-cell sums in observation order, CSR + CSC over raw level
+    ids) gives the host-accumulated build's image bit for bit: unweighted,
+    weighted with zero weights, slopes, unused levels, round factors
+    (tests/cpp/xtab_test.cpp)."""
+    exe = tmp_path / "xtab_test"
+    csrc = os.path.join(ROOT, "within_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-I", csrc, "-o", str(exe),
+                    os.path.join(ROOT, "tests", "cpp", "xtab_test.cpp"),
+                    os.path.join(csrc, "host_design.cpp"), os.path.join(csrc, "host_schwarz.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert "xtab ok 24" in out
+
+
 def test_schwarz_round_schedule_and_index_ranges(tmp_path):
     """The round-parallel approximate-Cholesky schedule (no row of a round
     reads a row of the same round, forward or backward) and the index range of

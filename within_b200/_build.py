@@ -15,7 +15,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libwithin_gpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["solver.cu", "host_design.cpp", "host_schwarz.cpp"]
+SOURCES = ["solver.cu", "xtab.cu", "host_design.cpp", "host_schwarz.cpp"]
 HEADERS = ["host.hpp", "kernels.cuh", "segreduce.cuh", "segplan.hpp", "refine.cuh", "rowsweep.cuh",
            "bulk.cuh", "tsweep.cuh", "segsweep.cuh"]
 

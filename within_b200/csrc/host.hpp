@@ -156,8 +156,30 @@ struct BuildResult {
     SchwarzHost schwarz;
     uint64_t n_warnings = 0;
 };
+// Weighted cross-tab of one channel pair (term a column ca, term b column cb)
+// over raw level ids, as computed on the GPU (xtab.cu): every cell
+// (level of a, level of b) with a non-zero sum of w_i * load_a_i * load_b_i
+// over its observations, each sum taken in observation order; CSR by a
+// (cells of a row in ascending b) and the same cells CSC by b.
+struct CrossTab {
+    std::vector<uint32_t> row_ptr, col;   // L_a + 1, nnz
+    std::vector<double> val;
+    std::vector<uint32_t> col_ptr, row;   // L_b + 1, nnz
+    std::vector<double> tval;
+};
+// The channel pairs of a design's additive-Schwarz build, in build order:
+// (term, column) of the first and second channel; columns are -1 for the
+// intercept, else the slope index into HostDesign::loads.
+struct ChannelPair {
+    uint32_t term_a, term_b;
+    int load_a, load_b;
+};
+std::vector<ChannelPair> schwarz_channel_pairs(const HostDesign& d);
+
+// cross_tabs: the GPU cross-tab of every channel pair (schwarz_channel_pairs
+// order), or nullptr to accumulate them on the host; both give the same bits.
 BuildResult build_preconditioner(const HostDesign& d, const double* weights_internal,
-                                 const PrecondCfg& cfg);
+                                 const PrecondCfg& cfg, const std::vector<CrossTab>* cross_tabs = nullptr);
 
 // ---- segmented-reduction plans ----
 struct HostPlan {

@@ -27,12 +27,39 @@
 #include <numeric>
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 #include <thread>
 
 #include "host.hpp"
 
 namespace wgpu {
 namespace {
+
+// WITHIN_TRACE=1: phase times of the build, one line each on stderr (a
+// diagnostic; no effect on results)
+struct BuildTrace {
+    const char* what;
+    long idx;
+    double t0;
+    static bool on() {
+        static const bool v = [] {
+            const char* e = std::getenv("WITHIN_TRACE");
+            return e && std::atoi(e) != 0;
+        }();
+        return v;
+    }
+    static double now() {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+    }
+    explicit BuildTrace(const char* w, long i = -1) : what(w), idx(i), t0(on() ? now() : 0.0) {}
+    void done() {
+        if (!on() || !what) return;
+        if (idx >= 0) fprintf(stderr, "[within trace]   %s %ld %.3f ms\n", what, idx, (now() - t0) * 1e3);
+        else fprintf(stderr, "[within trace]   %s %.3f ms\n", what, (now() - t0) * 1e3);
+        what = nullptr;
+    }
+    ~BuildTrace() { done(); }
+};
 
 // f(i) for i in [0, n) on up to 16 of the host's hardware threads (a build may
 // itself run on one of many threads building designs side by side;
@@ -815,7 +842,19 @@ struct Domain {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-BuildResult build_preconditioner(const HostDesign& d, const double* w, const PrecondCfg& cfg) {
+std::vector<ChannelPair> schwarz_channel_pairs(const HostDesign& d) {
+    std::vector<std::pair<uint32_t, int>> ch;   // (term, load index or -1)
+    for (uint32_t t = 0; t < d.terms.size(); ++t)
+        for (int c : d.terms[t].cols) ch.push_back({t, c});
+    std::vector<ChannelPair> out;
+    for (size_t a = 0; a < ch.size(); ++a)
+        for (size_t b = a + 1; b < ch.size(); ++b)
+            if (ch[a].first != ch[b].first) out.push_back({ch[a].first, ch[b].first, ch[a].second, ch[b].second});
+    return out;
+}
+
+BuildResult build_preconditioner(const HostDesign& d, const double* w, const PrecondCfg& cfg,
+                                 const std::vector<CrossTab>* cross_tabs) {
     BuildResult out;
     if (cfg.kind == 0) return out;
     if (cfg.kind == 2) {  // operator/schwarz.rs:185-229
@@ -863,7 +902,9 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             if (ch[a].term != ch[b].term) pairs.push_back({a, b});
     std::vector<std::vector<Domain>> pair_doms(pairs.size());
     std::vector<uint64_t> pair_warnings(pairs.size(), 0);
+    BuildTrace tr_pairs("channel pairs: cross-tabs, components, SDDM forms");
     par_for_each(pairs.size(), [&](size_t pi) {
+            BuildTrace tr_pair("pair", (long)pi);
             std::vector<Domain>& doms = pair_doms[pi];
             uint64_t& n_warnings = pair_warnings[pi];
             Ch R = ch[pairs[pi].first], Cc = ch[pairs[pi].second];
@@ -881,6 +922,52 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             const uint32_t* cl = d.codes[Cc.term].data();
             int kr = TR.cols[R.col], kc = TC.cols[Cc.col];
             std::vector<double> rdiag(nr, 0.0), cdiag(nc, 0.0);
+            Bip full;
+            full.c.nr = nr;
+            full.c.nc = nc;
+            if (cross_tabs) {
+                // the GPU cross-tab over raw level ids: keep the active levels
+                // (every cell's levels are active) and renumber them
+                const CrossTab& X = (*cross_tabs)[pi];
+                full.c.col.reserve(X.col.size());
+                full.c.val.reserve(X.col.size());
+                for (uint32_t j = 0; j < TR.n_levels; ++j) {
+                    if (!active[R.term][j]) continue;
+                    for (uint32_t p = X.row_ptr[j]; p < X.row_ptr[j + 1]; ++p) {
+                        full.c.col.push_back(cmap[X.col[p]]);
+                        full.c.val.push_back(X.val[p]);
+                    }
+                    full.c.ptr.push_back((uint32_t)full.c.col.size());
+                }
+                full.ct.nr = nc;
+                full.ct.nc = nr;
+                full.ct.col.reserve(X.row.size());
+                full.ct.val.reserve(X.row.size());
+                for (uint32_t k = 0; k < TC.n_levels; ++k) {
+                    if (!active[Cc.term][k]) continue;
+                    for (uint32_t p = X.col_ptr[k]; p < X.col_ptr[k + 1]; ++p) {
+                        full.ct.col.push_back(rmap[X.row[p]]);
+                        full.ct.val.push_back(X.tval[p]);
+                    }
+                    full.ct.ptr.push_back((uint32_t)full.ct.col.size());
+                }
+                if (!w && kr < 0 && kc < 0) {
+                    // unweighted intercepts: the diagonals are observation counts,
+                    // integer sums of the cells (exact in any order)
+                    for (uint32_t r = 0; r < nr; ++r)
+                        for (uint32_t p = full.c.ptr[r]; p < full.c.ptr[r + 1]; ++p) rdiag[r] += full.c.val[p];
+                    for (uint32_t c = 0; c < nc; ++c)
+                        for (uint32_t p = full.ct.ptr[c]; p < full.ct.ptr[c + 1]; ++p) cdiag[c] += full.ct.val[p];
+                } else {
+                    for (uint64_t i = 0; i < d.n_obs; ++i) {
+                        double wi = w ? w[i] : 1.0;
+                        double lr = kr < 0 ? 1.0 : d.loads[kr][i];
+                        double lc = kc < 0 ? 1.0 : d.loads[kc][i];
+                        rdiag[rmap[rl[i]]] += wi * lr * lr;
+                        cdiag[cmap[cl[i]]] += wi * lc * lc;
+                    }
+                }
+            } else {
             std::vector<uint32_t> cnt(nr + 1, 0);
             for (uint64_t i = 0; i < d.n_obs; ++i) ++cnt[rmap[rl[i]] + 1];
             for (uint32_t i = 0; i < nr; ++i) cnt[i + 1] += cnt[i];
@@ -897,9 +984,6 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 bc[p] = ck;
                 bv[p] = wi * lr * lc;
             }
-            Bip full;
-            full.c.nr = nr;
-            full.c.nc = nc;
             {
                 std::vector<double> work(nc, 0.0);
                 std::vector<uint32_t> touched;
@@ -922,6 +1006,10 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             std::vector<uint32_t>().swap(bc);
             std::vector<double>().swap(bv);
             full.ct = transpose(full.c);
+            }
+            if (BuildTrace::on())
+                fprintf(stderr, "[within trace]     pair %zu cross-tab %u x %u, %u cells%s\n", pi, nr, nc,
+                        full.c.nnz(), cross_tabs ? " (GPU)" : "");
             const bool known = kr < 0 && kc < 0;
             // components (cross_tab.rs:175-211): label by DFS, then group
             const uint32_t nl = nr + nc;
@@ -1003,6 +1091,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 doms.push_back(std::move(dm));
             }
         });
+    tr_pairs.done();
     std::vector<Domain> doms;
     for (size_t pi = 0; pi < pairs.size(); ++pi) {
         for (auto& dm : pair_doms[pi]) doms.push_back(std::move(dm));
@@ -1024,8 +1113,10 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
     }
 
     // ---- local solvers: reduced systems and their factors (one domain per host thread) ----
+    BuildTrace tr_local("local solvers: reduced systems and factors");
     par_for_each(doms.size(), [&](size_t di) {
         Domain& dm = doms[di];
+        const double t_dom = BuildTrace::on() ? BuildTrace::now() : 0.0;
         dm.inv_e = inv_elim(dm.comp);
         if (dm.comp.laplacian) {
             Lap L = reduced_for(dm.comp, dm.inv_e, cfg);
@@ -1038,8 +1129,13 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             factor_lap(L, cfg, dm.fac);
             dm.mode = 2;
         }
+        if (BuildTrace::on() && BuildTrace::now() - t_dom > 0.01)
+            fprintf(stderr, "[within trace]     domain %zu (%u + %u vertices, %u cells) %.3f ms\n", di,
+                    dm.comp.m.nr(), dm.comp.m.nc(), dm.comp.m.c.nnz(), (BuildTrace::now() - t_dom) * 1e3);
     });
 
+    tr_local.done();
+    BuildTrace tr_pack("pack");
     // ---- pack (layout documented on SchwarzHost) ----
     out.kind = 1;
     SchwarzHost& S = out.schwarz;

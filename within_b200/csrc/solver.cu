@@ -39,6 +39,11 @@
 
 using namespace wgpu;
 
+namespace wgpu {
+void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32_t* b_dev, uint32_t L_b,
+                   const double* w, const double* la, const double* lb, CrossTab& out, cudaStream_t st);
+}
+
 namespace {
 
 thread_local std::string g_err;
@@ -142,7 +147,11 @@ struct Tuning {
     // measured faster on the 10M-row panel), 2 = every tile plan (restrict,
     // means, kept sums, rounds, ... measured slower there), 0 = none
     int warp_ranges = 1;
+    // cross-tabs of the additive-Schwarz set-up on the GPU (xtab.cu): 1 for
+    // designs of at least XTAB_MIN_OBS observations, 2 always, 0 never
+    int gpu_cross_tab = 1;
 };
+constexpr uint64_t XTAB_MIN_OBS = 1ull << 18;
 
 Tuning resolve_tuning(const within_tuning* t) {
     Tuning r;
@@ -152,6 +161,7 @@ Tuning resolve_tuning(const within_tuning* t) {
         r.fuse_rounds = t->fuse_rounds != 0;
         r.segthread = t->thread_per_segment != 0;
         r.warp_ranges = t->warp_ranges;
+        r.gpu_cross_tab = t->gpu_cross_tab;
         return r;
     }
     if (const char* e = getenv("WITHIN_TSWEEP")) r.staged = atoi(e) != 0;
@@ -160,6 +170,7 @@ Tuning resolve_tuning(const within_tuning* t) {
     if (const char* e = getenv("WITHIN_FUSE_ROUNDS")) r.fuse_rounds = atoi(e) != 0;
     if (const char* e = getenv("WITHIN_SEGTHREAD")) r.segthread = atoi(e) != 0;
     if (const char* e = getenv("WITHIN_WARP_RANGES")) r.warp_ranges = atoi(e);
+    if (const char* e = getenv("WITHIN_GPU_XTAB")) r.gpu_cross_tab = atoi(e);
     return r;
 }
 
@@ -1900,9 +1911,28 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         for (uint64_t i = 0; i < D.n_obs; ++i) w[i] = D.obs_perm.empty() ? weights[i] : weights[D.obs_perm[i]];
     }
     s->reparam = build_reparam(D, weights ? w.data() : nullptr);
+    // codes and loads of the design operator on the device (the GPU cross-tabs
+    // of the preconditioner's set-up read them)
+    Arena& A = s->arena;
+    OpParams& op = s->op;
+    {
+        PhaseTrace pt("design codes upload");
+        op.n = (uint32_t)D.n_obs;
+        op.Q = (int)D.terms.size();
+        for (size_t k = 0; k < D.loads.size(); ++k) op.loads[k] = A.upload(D.loads[k]);
+        for (int t = 0; t < op.Q; ++t) {
+            const Term& T = D.terms[t];
+            op.codes[t] = A.upload(D.codes[t]);
+            op.off[t] = T.offset;
+            op.L[t] = T.n_levels;
+            op.ncol[t] = (int)T.cols.size();
+            for (size_t c = 0; c < T.cols.size(); ++c) op.load[t][c] = T.cols[c];
+        }
+    }
     // preconditioner (operator/schwarz.rs:231-270)
     BuildResult pre;
     PrecondCfg pre_cfg;
+    std::vector<CrossTab> pre_xtabs;
     std::exception_ptr pre_err;
     std::thread pre_thread;
     struct Joiner {   // the host build never outlives this frame, whatever throws
@@ -1953,30 +1983,38 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         // design and builds its scatter orders and sweep plans (both only read
         // the host design)
         pre_cfg = pc;
-        pre_thread = std::thread([&] {
+        // the cross-tabs of the additive-Schwarz set-up on the GPU
+        const int gx = s->schwarz.tuning.gpu_cross_tab;
+        const bool use_xtab = pc.kind == 1 && (gx >= 2 || (gx == 1 && D.n_obs >= XTAB_MIN_OBS));
+        if (use_xtab) {
+            PhaseTrace pt("GPU cross-tabs");
+            double* w_dev = nullptr;
+            std::unique_ptr<Arena> tmp(new Arena());
+            if (weights) w_dev = tmp->upload(w);
+            const std::vector<ChannelPair> cps = schwarz_channel_pairs(D);
+            pre_xtabs.resize(cps.size());
+            for (size_t i = 0; i < cps.size(); ++i) {
+                const ChannelPair& cp = cps[i];
+                try {
+                    gpu_cross_tab(D.n_obs, op.codes[cp.term_a], D.terms[cp.term_a].n_levels, op.codes[cp.term_b],
+                                  D.terms[cp.term_b].n_levels, w_dev, cp.load_a < 0 ? nullptr : op.loads[cp.load_a],
+                                  cp.load_b < 0 ? nullptr : op.loads[cp.load_b], pre_xtabs[i], s->stream);
+                } catch (const std::runtime_error& e) {
+                    throw WError(ERR_CUDA, e.what());
+                }
+            }
+        }
+        pre_thread = std::thread([&, use_xtab] {
             try {
                 PhaseTrace pt("preconditioner host build");
-                pre = build_preconditioner(D, weights ? w.data() : nullptr, pre_cfg);
+                pre = build_preconditioner(D, weights ? w.data() : nullptr, pre_cfg, use_xtab ? &pre_xtabs : nullptr);
             } catch (...) {
                 pre_err = std::current_exception();
             }
         });
     }
-    // design operator on the device
+    // the rest of the design operator on the device
     PhaseTrace pt_op("design upload and scatter orders");
-    Arena& A = s->arena;
-    OpParams& op = s->op;
-    op.n = (uint32_t)D.n_obs;
-    op.Q = (int)D.terms.size();
-    for (size_t k = 0; k < D.loads.size(); ++k) op.loads[k] = A.upload(D.loads[k]);
-    for (int t = 0; t < op.Q; ++t) {
-        const Term& T = D.terms[t];
-        op.codes[t] = A.upload(D.codes[t]);
-        op.off[t] = T.offset;
-        op.L[t] = T.n_levels;
-        op.ncol[t] = (int)T.cols.size();
-        for (size_t c = 0; c < T.cols.size(); ++c) op.load[t][c] = T.cols[c];
-    }
     if (weights) {
         std::vector<double> sw(w);
         for (double& x : sw) x = std::sqrt(x);
@@ -2329,6 +2367,7 @@ void within_tuning_default(within_tuning* t) {
     t->core_small = pc.core_small;
     t->core_dense_late = pc.core_dense_late;
     t->warp_ranges = 1;
+    t->gpu_cross_tab = 1;
 }
 
 int within_solver_new_tuned(const within_design* design, const double* weights, const within_precond_config* cfg,
