@@ -10,7 +10,7 @@
 // Random worker/firm/year-like designs (every fourth with a slope on the second
 // factor and observation weights, which takes the signed / cover routes of the
 // set-up), with the round stop rules relaxed so that several rounds are
-// scheduled.
+// scheduled; two large ones run the threaded rounds.
 #include "host.hpp"
 
 #include <cstdio>
@@ -46,10 +46,13 @@ static int fail(const char* what, int trial) {
 int main() {
     std::mt19937_64 rng(11);
     uint64_t rounds_seen = 0, rows_checked = 0, not_laplacian = 0;
-    for (int trial = 0; trial < 24; ++trial) {
-        const uint32_t n = 4000 + (uint32_t)(rng() % 20000);
-        const uint32_t L0 = 300 + (uint32_t)(rng() % 2000), L1 = 80 + (uint32_t)(rng() % 400),
-                       L2 = 3 + (uint32_t)(rng() % 30);
+    for (int trial = 0; trial < 26; ++trial) {
+        // the last two: a reduced system of ~20,000 vertices, whose rounds run on host threads
+        const bool big = trial >= 24;
+        const uint32_t n = big ? 160000 : 4000 + (uint32_t)(rng() % 20000);
+        const uint32_t L0 = big ? 60000 : 300 + (uint32_t)(rng() % 2000);
+        const uint32_t L1 = big ? 20000 : 80 + (uint32_t)(rng() % 400);
+        const uint32_t L2 = 3 + (uint32_t)(rng() % 30);
         std::vector<uint32_t> a(n), b(n), c(n);
         std::vector<double> z(n), w(n);
         // clustered first factor (panel-like runs), random others
@@ -79,7 +82,7 @@ int main() {
         BuildResult br = build_preconditioner(d, wp, cfg);
         if (br.kind != 1) return fail("additive Schwarz expected", trial);
         const SchwarzHost& S = br.schwarz;
-        if (trial % 6 == 0) {
+        if (trial % 6 == 0 || big) {
             setenv("WITHIN_HOST_THREADS", "1", 1);
             BuildResult one = build_preconditioner(d, wp, cfg);
             unsetenv("WITHIN_HOST_THREADS");

@@ -16,7 +16,8 @@ each knob in turn over its candidate values, keeping the best by a margin of
 segment, warp ranges) change only the solve, so they are judged by the solve's device
 time (median of 5 solves of one FP64 right-hand side at tol 1e-8); the stop
 rules of the round-parallel factor change the set-up too, so they are judged
-by the set-up time plus five solves (a preconditioner reused five times).
+by the set-up time plus five solves (a preconditioner reused five times), with the
+set-up taken as the fastest measured for the same factor rules.
 One untimed build and solve run before the search, so the first candidate
 pays no process warm-up.
 
@@ -126,9 +127,20 @@ def _measure(W, codes, weights, rec, y, reps=5):
     return setup, float(np.median(ts)), st[0][1]
 
 
-def _cost(knob, m):
+FACTOR_FIELDS = ("core_dense_max", "core_min_frac", "max_rounds", "core_small", "core_dense_late")
+
+
+def _factor_key(rec):
+    return tuple(rec.get(f) for f in FACTOR_FIELDS)
+
+
+def _cost(knob, m, setup_floor):
+    """Kernel knobs: the solve time.  Factor rules: set-up + 5 solves, the
+    set-up taken as the fastest seen for the record's factor rules (the
+    kernel knobs barely change it, so every measurement of those rules
+    counts; one slow set-up must not decide)."""
     setup, solve, _ = m
-    return solve if knob in KERNEL_KNOBS else setup + 5 * solve
+    return solve if knob in KERNEL_KNOBS else setup_floor + 5 * solve
 
 
 def tune(out_path: str = TABLE, quick: bool = False) -> dict:
@@ -141,6 +153,7 @@ def tune(out_path: str = TABLE, quick: bool = False) -> dict:
         rec = W.default_tuning()
         _measure(W, codes, weights, rec, y, reps=1)   # warm-up: the process's first build and solve
         best = _measure(W, codes, weights, rec, y)
+        floor = {_factor_key(rec): best[0]}
         trail = [{"tuning": dict(rec), "setup_s": best[0], "solve_s": best[1], "iterations": best[2]}]
         for knob, values in CANDIDATES.items():
             for v in values:
@@ -149,8 +162,11 @@ def tune(out_path: str = TABLE, quick: bool = False) -> dict:
                 cand = dict(rec)
                 cand[knob] = v
                 m = _measure(W, codes, weights, cand, y)
+                fk = _factor_key(cand)
+                floor[fk] = min(floor.get(fk, m[0]), m[0])
                 trail.append({"tuning": cand, "setup_s": m[0], "solve_s": m[1], "iterations": m[2]})
-                if _cost(knob, m) < 0.98 * _cost(knob, best):   # a 2 % margin against timing noise
+                # a 2 % margin against timing noise
+                if _cost(knob, m, floor[fk]) < 0.98 * _cost(knob, best, floor[_factor_key(rec)]):
                     rec, best = cand, m
         entries.append({"design": name, "key": key, "tuning": rec,
                         "measured": {"setup_s": best[0], "solve_s": best[1], "iterations": best[2]},

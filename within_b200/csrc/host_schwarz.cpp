@@ -316,45 +316,68 @@ Lap exact_reduced(const Comp& c, const std::vector<double>& inv_e) {
     }
     Lap L;
     L.n = nk + (c.grounded ? 1 : 0);
-    std::vector<double> work(nk, 0.0);
-    std::vector<uint32_t> touched;
-    for (uint32_t i = 0; i < nk; ++i) {
-        work[i] = c.diag[ne + i];
-        touched.push_back(i);
-        for (uint32_t a = c.m.ct.ptr[i]; a < c.m.ct.ptr[i + 1]; ++a) {
-            uint32_t k = c.m.ct.col[a];
-            double w = c.m.ct.val[a], inv = inv_e[k];
-            for (uint32_t b = c.m.c.ptr[k]; b < c.m.c.ptr[k + 1]; ++b) {
-                uint32_t j = c.m.c.col[b];
-                if (work[j] == 0.0 && j != i) touched.push_back(j);
-                work[j] -= (w * c.m.c.val[b]) * inv;
+    // row i of the reduced matrix depends only on the rows of C through the
+    // neighbours of kept vertex i, so blocks of rows are formed on host
+    // threads (each row by the same sequential loop) and joined in row order
+    struct RowOut {
+        std::vector<uint32_t> col;
+        std::vector<double> val;
+    };
+    constexpr uint32_t RBLK = 4;
+    const uint32_t nblk = (nk + RBLK - 1) / RBLK;
+    std::vector<std::vector<RowOut>> rows(nblk);
+    auto row_block = [&](size_t bi) {
+        std::vector<double> work(nk, 0.0);
+        std::vector<uint32_t> touched;
+        const uint32_t i0 = (uint32_t)bi * RBLK, i1 = std::min(nk, i0 + RBLK);
+        rows[bi].resize(i1 - i0);
+        for (uint32_t i = i0; i < i1; ++i) {
+            RowOut& R = rows[bi][i - i0];
+            work[i] = c.diag[ne + i];
+            touched.push_back(i);
+            for (uint32_t a = c.m.ct.ptr[i]; a < c.m.ct.ptr[i + 1]; ++a) {
+                uint32_t k = c.m.ct.col[a];
+                double w = c.m.ct.val[a], inv = inv_e[k];
+                for (uint32_t b = c.m.c.ptr[k]; b < c.m.c.ptr[k + 1]; ++b) {
+                    uint32_t j = c.m.c.col[b];
+                    if (work[j] == 0.0 && j != i) touched.push_back(j);
+                    work[j] -= (w * c.m.c.val[b]) * inv;
+                }
             }
-        }
-        std::sort(touched.begin(), touched.end());
-        touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
-        double adjacency = 0;
-        size_t dpos = 0;
-        for (uint32_t j : touched) {
-            double v = work[j];
-            work[j] = 0.0;
-            if (j == i) {
-                dpos = L.col.size();
-                L.col.push_back(j);
-                L.val.push_back(0.0);
-            } else if (v != 0.0) {
-                adjacency -= v;
-                L.col.push_back(j);
-                L.val.push_back(v);
+            std::sort(touched.begin(), touched.end());
+            touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+            double adjacency = 0;
+            size_t dpos = 0;
+            for (uint32_t j : touched) {
+                double v = work[j];
+                work[j] = 0.0;
+                if (j == i) {
+                    dpos = R.col.size();
+                    R.col.push_back(j);
+                    R.val.push_back(0.0);
+                } else if (v != 0.0) {
+                    adjacency -= v;
+                    R.col.push_back(j);
+                    R.val.push_back(v);
+                }
             }
+            R.val[dpos] = adjacency + surplus[i];
+            if (c.grounded && surplus[i] > 0.0) {
+                R.col.push_back(nk);
+                R.val.push_back(-surplus[i]);
+            }
+            touched.clear();
         }
-        L.val[dpos] = adjacency + surplus[i];
-        if (c.grounded && surplus[i] > 0.0) {
-            L.col.push_back(nk);
-            L.val.push_back(-surplus[i]);
+    };
+    // worth threads only when the rows reach many eliminated neighbours
+    if (c.m.c.nnz() >= (1u << 20)) par_for_each(nblk, row_block);
+    else for (size_t bi = 0; bi < nblk; ++bi) row_block(bi);
+    for (auto& blk : rows)
+        for (RowOut& R : blk) {
+            L.col.insert(L.col.end(), R.col.begin(), R.col.end());
+            L.val.insert(L.val.end(), R.val.begin(), R.val.end());
+            L.ptr.push_back((uint32_t)L.col.size());
         }
-        L.ptr.push_back((uint32_t)L.col.size());
-        touched.clear();
-    }
     if (c.grounded) {
         for (uint32_t i = 0; i < nk; ++i)
             if (surplus[i] > 0.0) {
@@ -627,38 +650,59 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
     std::vector<uint32_t> live(n);
     std::iota(live.begin(), live.end(), 0u);
     std::vector<uint64_t> key(n);
-    std::vector<double> acc(n, 0.0);
-    std::vector<char> seen(n, 0);
     std::vector<uint32_t> sel;
     std::vector<Edge> fill;
-    std::vector<std::pair<uint32_t, double>> ent;
     uint32_t r = 0;
     double last_frac = 1.0;
     bool dense_graph = false;   // see the stop rules below
+    // Every vertex's compaction, key, selection test and elimination reads
+    // only its own adjacency (and its neighbours' keys), and every eliminated
+    // vertex samples from its own seeded stream, so these run over blocks of
+    // vertices on host threads; selections and fill edges are joined in
+    // vertex order, which gives the sequential loop's lists exactly.
+    constexpr size_t VBLK = 4096;
+    auto blocks = [](size_t m) { return (m + VBLK - 1) / VBLK; };
+    const bool threaded = n >= 4 * VBLK;
+    auto par = [&](size_t nb, auto&& fn) {
+        if (threaded) par_for_each(nb, fn);
+        else for (size_t b = 0; b < nb; ++b) fn(b);
+    };
+    struct Scratch {
+        std::vector<double> acc;
+        std::vector<char> seen;
+        std::vector<uint32_t> order;
+    };
     while (!live.empty()) {
         // compact adjacency: drop dead neighbours, merge parallel edges
-        for (uint32_t v : live) {
-            auto& a = adj[v];
-            size_t w = 0;
-            std::vector<uint32_t> order;
-            for (auto& e : a) {
-                if (!alive[e.first] || e.first == v) continue;
-                if (!seen[e.first]) {
-                    seen[e.first] = 1;
-                    order.push_back(e.first);
+        par(blocks(live.size()), [&](size_t b) {
+            Scratch sc;
+            sc.acc.assign(n, 0.0);
+            sc.seen.assign(n, 0);
+            const size_t j1 = std::min(live.size(), (b + 1) * VBLK);
+            for (size_t j = b * VBLK; j < j1; ++j) {
+                const uint32_t v = live[j];
+                auto& a = adj[v];
+                size_t w = 0;
+                sc.order.clear();
+                for (auto& e : a) {
+                    if (!alive[e.first] || e.first == v) continue;
+                    if (!sc.seen[e.first]) {
+                        sc.seen[e.first] = 1;
+                        sc.order.push_back(e.first);
+                    }
+                    sc.acc[e.first] += e.second;
                 }
-                acc[e.first] += e.second;
+                std::sort(sc.order.begin(), sc.order.end());
+                a.resize(sc.order.size());
+                for (uint32_t u : sc.order) {
+                    a[w++] = {u, sc.acc[u]};
+                    sc.acc[u] = 0.0;
+                    sc.seen[u] = 0;
+                }
+                uint64_t deg = std::min<uint64_t>(a.size(), 255);
+                key[v] = (deg << 56) | (mix64(seed ^ ((uint64_t)v << 20) ^ r) & 0x00FFFFFFFF000000ull) | 0;
             }
-            std::sort(order.begin(), order.end());
-            a.resize(order.size());
-            for (uint32_t u : order) {
-                a[w++] = {u, acc[u]};
-                acc[u] = 0.0;
-                seen[u] = 0;
-            }
-            uint64_t deg = std::min<uint64_t>(a.size(), 255);
-            key[v] = (deg << 56) | (mix64(seed ^ ((uint64_t)v << 20) ^ r) & 0x00FFFFFFFF000000ull) | 0;
-        }
+        });
         // Stop the rounds once the remaining graph is a small or dense core:
         // a dense core (<= core_dense_max vertices) is inverted exactly; a
         // larger one, reached when rounds stop paying (fewer than
@@ -723,34 +767,49 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
             ++r;
             break;
         }
-        sel.clear();
-        for (uint32_t v : live) {
-            bool best = true;
-            for (auto& e : adj[v]) {
-                uint32_t u = e.first;
-                if (key[u] < key[v] || (key[u] == key[v] && u < v)) {
-                    best = false;
-                    break;
+        // the round: every live vertex that is the minimum of (key, id) over its neighbours
+        std::vector<std::vector<uint32_t>> sel_part(blocks(live.size()));
+        par(sel_part.size(), [&](size_t b) {
+            const size_t j1 = std::min(live.size(), (b + 1) * VBLK);
+            for (size_t j = b * VBLK; j < j1; ++j) {
+                const uint32_t v = live[j];
+                bool best = true;
+                for (auto& e : adj[v]) {
+                    uint32_t u = e.first;
+                    if (key[u] < key[v] || (key[u] == key[v] && u < v)) {
+                        best = false;
+                        break;
+                    }
                 }
+                if (best) sel_part[b].push_back(v);
             }
-            if (best) sel.push_back(v);
-        }
+        });
+        sel.clear();
+        for (auto& p : sel_part) sel.insert(sel.end(), p.begin(), p.end());
+        // eliminate the round: columns of L, pivots and sampled fill edges
+        std::vector<std::vector<Edge>> fill_part(blocks(sel.size()));
+        par(fill_part.size(), [&](size_t b) {
+            std::vector<std::pair<uint32_t, double>> ent;
+            const size_t j1 = std::min(sel.size(), (b + 1) * VBLK);
+            for (size_t j = b * VBLK; j < j1; ++j) {
+                const uint32_t v = sel[j];
+                f.round[v] = r;
+                double d = 0;
+                for (auto& e : adj[v]) d += e.second;
+                if (!(d > 0.0)) {
+                    f.dinv[v] = 0.0;
+                    continue;
+                }
+                f.dinv[v] = 1.0 / d;
+                auto& cv = f.colv[v];
+                for (auto& e : adj[v]) cv.push_back({e.first, -e.second / d});
+                ent = adj[v];
+                Rng rng{mix64(seed * 0x9E3779B97F4A7C15ull + v + 1)};
+                sample_star(ent, split, rng, fill_part[b]);
+            }
+        });
         fill.clear();
-        for (uint32_t v : sel) {
-            f.round[v] = r;
-            double d = 0;
-            for (auto& e : adj[v]) d += e.second;
-            if (!(d > 0.0)) {
-                f.dinv[v] = 0.0;
-                continue;
-            }
-            f.dinv[v] = 1.0 / d;
-            auto& cv = f.colv[v];
-            for (auto& e : adj[v]) cv.push_back({e.first, -e.second / d});
-            ent = adj[v];
-            Rng rng{mix64(seed * 0x9E3779B97F4A7C15ull + v + 1)};
-            sample_star(ent, split, rng, fill);
-        }
+        for (auto& p : fill_part) fill.insert(fill.end(), p.begin(), p.end());
         for (uint32_t v : sel) {
             alive[v] = 0;
             adj[v].clear();
@@ -1120,7 +1179,11 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         dm.inv_e = inv_elim(dm.comp);
         if (dm.comp.laplacian) {
             Lap L = reduced_for(dm.comp, dm.inv_e, cfg);
+            const double t_red = BuildTrace::on() ? BuildTrace::now() : 0.0;
             factor_lap(L, cfg, dm.fac);
+            if (BuildTrace::on() && BuildTrace::now() - t_dom > 0.01)
+                fprintf(stderr, "[within trace]     domain %zu reduced system %.3f ms, factor %.3f ms\n", di,
+                        (t_red - t_dom) * 1e3, (BuildTrace::now() - t_red) * 1e3);
             dm.mode = dm.comp.grounded ? 1 : 0;
         } else {
             Comp cov = cover_of(dm.comp);
@@ -1183,51 +1246,71 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
     S.c_col.resize(o_c[nsub]);
     S.c_val.resize(o_c[nsub]);
     S.red_sub.resize(red);
+    // f(lo, hi) over [0, m) in blocks on host threads when m is large (every
+    // block writes its own entries, so the result is the sequential loop's)
+    auto blocked = [](uint32_t m, auto&& f) {
+        constexpr uint32_t BLK = 1u << 16;
+        if (m < 4 * BLK) {
+            f(0u, m);
+            return;
+        }
+        par_for_each((m + BLK - 1) / BLK, [&](size_t b) {
+            const uint32_t lo = (uint32_t)b * BLK;
+            f(lo, std::min(m, lo + BLK));
+        });
+    };
     par_for_each(nsub, [&](size_t si) {
         const uint32_t s = (uint32_t)si;
         const Domain& dm = doms[s];
         const uint32_t ne = dm.comp.m.nr(), nk = dm.comp.m.nc(), nloc = ne + nk;
         const uint32_t lo = (uint32_t)o_loc[s], rd = (uint32_t)o_red[s];
-        for (uint32_t j = 0; j < nloc; ++j) {
-            double f = dm.comp.factors.empty() ? (j < ne ? 1.0 : -1.0) : dm.comp.factors[j];
-            double pw = dm.pw.empty() ? 1.0 : dm.pw[j];
-            S.glob[lo + j] = dm.globals[j];
-            S.scale[lo + j] = pw * f;
-            S.slot_sub[lo + j] = s;
-            S.inv_e[lo + j] = j < ne ? dm.inv_e[j] : 0.0;
-        }
+        blocked(nloc, [&](uint32_t j0, uint32_t j1) {
+            for (uint32_t j = j0; j < j1; ++j) {
+                double f = dm.comp.factors.empty() ? (j < ne ? 1.0 : -1.0) : dm.comp.factors[j];
+                double pw = dm.pw.empty() ? 1.0 : dm.pw[j];
+                S.glob[lo + j] = dm.globals[j];
+                S.scale[lo + j] = pw * f;
+                S.slot_sub[lo + j] = s;
+                S.inv_e[lo + j] = j < ne ? dm.inv_e[j] : 0.0;
+            }
+        });
         // C^T rows (kept), columns = local slots of eliminated entries, values
         // pre-divided by D_e (solver.rs:360-371 scales rhs_e by 1/D_e first)
         const Csr& ct = dm.comp.m.ct;
-        for (uint32_t k = 0; k < nk; ++k) {
-            double rs = 0.0;
-            for (uint32_t a = ct.ptr[k]; a < ct.ptr[k + 1]; ++a) {
-                const double v = ct.val[a] * dm.inv_e[ct.col[a]];
-                S.ct_col[o_ct[s] + a] = lo + ct.col[a];
-                S.ct_val[o_ct[s] + a] = v;
-                rs += v;
+        blocked(nk, [&](uint32_t k0, uint32_t k1) {
+            for (uint32_t k = k0; k < k1; ++k) {
+                double rs = 0.0;
+                for (uint32_t a = ct.ptr[k]; a < ct.ptr[k + 1]; ++a) {
+                    const double v = ct.val[a] * dm.inv_e[ct.col[a]];
+                    S.ct_col[o_ct[s] + a] = lo + ct.col[a];
+                    S.ct_val[o_ct[s] + a] = v;
+                    rs += v;
+                }
+                S.ct_ptr[o_kp[s] + k + 1] = (uint32_t)(o_ct[s] + ct.ptr[k + 1]);
+                S.ct_rowsum[o_kp[s] + k] = rs;
+                S.ct_row_slot[o_kp[s] + k] = lo + ne + k;
+                S.ct_row_red[o_kp[s] + k] = rd + k;
             }
-            S.ct_ptr[o_kp[s] + k + 1] = (uint32_t)(o_ct[s] + ct.ptr[k + 1]);
-            S.ct_rowsum[o_kp[s] + k] = rs;
-            S.ct_row_slot[o_kp[s] + k] = lo + ne + k;
-            S.ct_row_red[o_kp[s] + k] = rd + k;
-        }
+        });
         // C rows (eliminated), columns = reduced slot of the kept entry (bit 31:
         // gauge/cover read-back needed), values pre-divided by D_e (solver.rs:41-77)
         const uint32_t flag = dm.mode == 0 ? 0u : 0x80000000u;
         const Csr& c = dm.comp.m.c;
-        for (uint32_t e = 0; e < ne; ++e) {
-            for (uint32_t a = c.ptr[e]; a < c.ptr[e + 1]; ++a) {
-                S.c_col[o_c[s] + a] = (rd + c.col[a]) | flag;
-                S.c_val[o_c[s] + a] = c.val[a] * dm.inv_e[e];
+        blocked(ne, [&](uint32_t e0, uint32_t e1) {
+            for (uint32_t e = e0; e < e1; ++e) {
+                for (uint32_t a = c.ptr[e]; a < c.ptr[e + 1]; ++a) {
+                    S.c_col[o_c[s] + a] = (rd + c.col[a]) | flag;
+                    S.c_val[o_c[s] + a] = c.val[a] * dm.inv_e[e];
+                }
+                S.c_ptr[o_el[s] + e + 1] = (uint32_t)(o_c[s] + c.ptr[e + 1]);
+                S.elim_slot[o_el[s] + e] = lo + e;
             }
-            S.c_ptr[o_el[s] + e + 1] = (uint32_t)(o_c[s] + c.ptr[e + 1]);
-            S.elim_slot[o_el[s] + e] = lo + e;
-        }
+        });
         for (uint32_t i = 0; i < dm.fac.n; ++i) S.red_sub[rd + i] = s;
     });
     S.n_red = red;
     S.dinv.assign(red, 0.0);
+    if (BuildTrace::on()) fprintf(stderr, "[within trace]     pack: slots and C / C^T %.3f ms\n", (BuildTrace::now() - tr_pack.t0) * 1e3);
     // dense blocks
     S.dense_rows_ptr.push_back(0);
     for (uint32_t s = 0; s < S.n_sub; ++s) {
@@ -1303,6 +1386,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         S.fwd_round_ptr.push_back((uint32_t)S.fwd_row.size());
         S.bwd_round_ptr.push_back((uint32_t)S.bwd_row.size());
     }
+    if (BuildTrace::on()) fprintf(stderr, "[within trace]     pack: dense blocks and rounds %.3f ms\n", (BuildTrace::now() - tr_pack.t0) * 1e3);
     // prolongation: DOF -> local slots, in subdomain order
     S.dof_ptr.assign(S.n_dofs + 1, 0);
     for (uint32_t g : S.glob) ++S.dof_ptr[g + 1];
