@@ -59,6 +59,19 @@ static CrossTab cross_tab_like_gpu(const HostDesign& d, const double* w, const C
         ++X.col_ptr[X.col[k] + 1];
     }
     for (uint32_t c = 0; c < Lb; ++c) X.col_ptr[c + 1] += X.col_ptr[c];
+    // components: the smallest vertex (levels of a, then L_a + levels of b) of each
+    std::vector<uint32_t> par(La + Lb);
+    std::iota(par.begin(), par.end(), 0u);
+    auto find = [&](uint32_t v) {
+        while (par[v] != v) v = par[v] = par[par[v]];
+        return v;
+    };
+    for (size_t k = 0; k < ra.size(); ++k) {
+        uint32_t x = find(ra[k]), y = find(La + X.col[k]);
+        if (x != y) par[std::max(x, y)] = std::min(x, y);
+    }
+    X.comp.resize(La + Lb);
+    for (uint32_t v = 0; v < La + Lb; ++v) X.comp[v] = find(v);
     return X;
 }
 

@@ -166,6 +166,10 @@ struct CrossTab {
     std::vector<double> val;
     std::vector<uint32_t> col_ptr, row;   // L_b + 1, nnz
     std::vector<double> tval;
+    // connected components of the bipartite cell graph (vertices: levels of a
+    // as 0 .. L_a - 1, then levels of b as L_a .. L_a + L_b - 1): the smallest
+    // vertex of each vertex's component; empty = not computed
+    std::vector<uint32_t> comp;
 };
 // The channel pairs of a design's additive-Schwarz build, in build order:
 // (term, column) of the first and second channel; columns are -1 for the
@@ -177,9 +181,10 @@ struct ChannelPair {
 std::vector<ChannelPair> schwarz_channel_pairs(const HostDesign& d);
 
 // cross_tabs: the GPU cross-tab of every channel pair (schwarz_channel_pairs
-// order), or nullptr to accumulate them on the host; both give the same bits.
+// order; the build may move their arrays out), or nullptr to accumulate them
+// on the host; both give the same bits.
 BuildResult build_preconditioner(const HostDesign& d, const double* weights_internal,
-                                 const PrecondCfg& cfg, const std::vector<CrossTab>* cross_tabs = nullptr);
+                                 const PrecondCfg& cfg, std::vector<CrossTab>* cross_tabs = nullptr);
 
 // ---- segmented-reduction plans ----
 struct HostPlan {

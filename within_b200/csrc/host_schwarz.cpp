@@ -24,6 +24,7 @@
 #include <cfloat>
 #include <cmath>
 #include <exception>
+#include <functional>
 #include <numeric>
 #include <cstdio>
 #include <cstdlib>
@@ -913,7 +914,7 @@ std::vector<ChannelPair> schwarz_channel_pairs(const HostDesign& d) {
 }
 
 BuildResult build_preconditioner(const HostDesign& d, const double* w, const PrecondCfg& cfg,
-                                 const std::vector<CrossTab>* cross_tabs) {
+                                 std::vector<CrossTab>* cross_tabs) {
     BuildResult out;
     if (cfg.kind == 0) return out;
     if (cfg.kind == 2) {  // operator/schwarz.rs:185-229
@@ -987,28 +988,40 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             if (cross_tabs) {
                 // the GPU cross-tab over raw level ids: keep the active levels
                 // (every cell's levels are active) and renumber them
-                const CrossTab& X = (*cross_tabs)[pi];
-                full.c.col.reserve(X.col.size());
-                full.c.val.reserve(X.col.size());
-                for (uint32_t j = 0; j < TR.n_levels; ++j) {
-                    if (!active[R.term][j]) continue;
-                    for (uint32_t p = X.row_ptr[j]; p < X.row_ptr[j + 1]; ++p) {
-                        full.c.col.push_back(cmap[X.col[p]]);
-                        full.c.val.push_back(X.val[p]);
+                CrossTab& X = (*cross_tabs)[pi];
+                if (nr == TR.n_levels && nc == TC.n_levels) {
+                    // every level is active: the renumbering is the identity
+                    full.c.ptr = std::move(X.row_ptr);
+                    full.c.col = std::move(X.col);
+                    full.c.val = std::move(X.val);
+                    full.ct.nr = nc;
+                    full.ct.nc = nr;
+                    full.ct.ptr = std::move(X.col_ptr);
+                    full.ct.col = std::move(X.row);
+                    full.ct.val = std::move(X.tval);
+                } else {
+                    full.c.col.reserve(X.col.size());
+                    full.c.val.reserve(X.col.size());
+                    for (uint32_t j = 0; j < TR.n_levels; ++j) {
+                        if (!active[R.term][j]) continue;
+                        for (uint32_t p = X.row_ptr[j]; p < X.row_ptr[j + 1]; ++p) {
+                            full.c.col.push_back(cmap[X.col[p]]);
+                            full.c.val.push_back(X.val[p]);
+                        }
+                        full.c.ptr.push_back((uint32_t)full.c.col.size());
                     }
-                    full.c.ptr.push_back((uint32_t)full.c.col.size());
-                }
-                full.ct.nr = nc;
-                full.ct.nc = nr;
-                full.ct.col.reserve(X.row.size());
-                full.ct.val.reserve(X.row.size());
-                for (uint32_t k = 0; k < TC.n_levels; ++k) {
-                    if (!active[Cc.term][k]) continue;
-                    for (uint32_t p = X.col_ptr[k]; p < X.col_ptr[k + 1]; ++p) {
-                        full.ct.col.push_back(rmap[X.row[p]]);
-                        full.ct.val.push_back(X.tval[p]);
+                    full.ct.nr = nc;
+                    full.ct.nc = nr;
+                    full.ct.col.reserve(X.row.size());
+                    full.ct.val.reserve(X.row.size());
+                    for (uint32_t k = 0; k < TC.n_levels; ++k) {
+                        if (!active[Cc.term][k]) continue;
+                        for (uint32_t p = X.col_ptr[k]; p < X.col_ptr[k + 1]; ++p) {
+                            full.ct.col.push_back(rmap[X.row[p]]);
+                            full.ct.val.push_back(X.tval[p]);
+                        }
+                        full.ct.ptr.push_back((uint32_t)full.ct.col.size());
                     }
-                    full.ct.ptr.push_back((uint32_t)full.ct.col.size());
                 }
                 if (!w && kr < 0 && kc < 0) {
                     // unweighted intercepts: the diagonals are observation counts,
@@ -1070,10 +1083,31 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 fprintf(stderr, "[within trace]     pair %zu cross-tab %u x %u, %u cells%s\n", pi, nr, nc,
                         full.c.nnz(), cross_tabs ? " (GPU)" : "");
             const bool known = kr < 0 && kc < 0;
-            // components (cross_tab.rs:175-211): label by DFS, then group
+            // components (cross_tab.rs:175-211): label by DFS, then group;
+            // numbered in the order of their smallest vertex
             const uint32_t nl = nr + nc;
             std::vector<uint32_t> lab(nl, UINT32_MAX), stk;
             uint32_t ncomp = 0;
+            if (cross_tabs && !(*cross_tabs)[pi].comp.empty()) {
+                // the GPU's labels (smallest raw vertex of each component; the
+                // renumbering of active levels keeps their order, rows before
+                // columns), numbered in the same order as the DFS below
+                const std::vector<uint32_t>& cm = (*cross_tabs)[pi].comp;
+                std::vector<uint32_t> id(cm.size(), UINT32_MAX);
+                uint32_t v = 0;
+                for (uint32_t j = 0; j < TR.n_levels; ++j)
+                    if (active[R.term][j]) {
+                        uint32_t& c = id[cm[j]];
+                        if (c == UINT32_MAX) c = ncomp++;
+                        lab[v++] = c;
+                    }
+                for (uint32_t k = 0; k < TC.n_levels; ++k)
+                    if (active[Cc.term][k]) {
+                        uint32_t& c = id[cm[TR.n_levels + k]];
+                        if (c == UINT32_MAX) c = ncomp++;
+                        lab[v++] = c;
+                    }
+            }
             for (uint32_t s0 = 0; s0 < nl; ++s0) {
                 if (lab[s0] != UINT32_MAX) continue;
                 lab[s0] = ncomp;
@@ -1087,6 +1121,9 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 }
                 ++ncomp;
             }
+            if (BuildTrace::on())
+                fprintf(stderr, "[within trace]     pair %zu: %u components after %.3f ms\n", pi, ncomp,
+                        (BuildTrace::now() - tr_pair.t0) * 1e3);
             std::vector<std::vector<uint32_t>> crow(ncomp), ccol(ncomp);
             for (uint32_t i = 0; i < nr; ++i) crow[lab[i]].push_back(i);
             for (uint32_t k = 0; k < nc; ++k) ccol[lab[nr + k]].push_back(k);
@@ -1231,21 +1268,22 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         if (!dm.fac.dense) rounds = std::max(rounds, dm.fac.n_rounds);
     }
     const uint32_t red = (uint32_t)o_red[nsub];
-    S.glob.resize(o_loc[nsub]);
-    S.scale.resize(o_loc[nsub]);
-    S.slot_sub.resize(o_loc[nsub]);
-    S.inv_e.resize(o_loc[nsub]);
-    S.ct_ptr.resize(o_kp[nsub] + 1);
-    S.ct_rowsum.resize(o_kp[nsub]);
-    S.ct_row_slot.resize(o_kp[nsub]);
-    S.ct_row_red.resize(o_kp[nsub]);
-    S.ct_col.resize(o_ct[nsub]);
-    S.ct_val.resize(o_ct[nsub]);
-    S.c_ptr.resize(o_el[nsub] + 1);
-    S.elim_slot.resize(o_el[nsub]);
-    S.c_col.resize(o_c[nsub]);
-    S.c_val.resize(o_c[nsub]);
-    S.red_sub.resize(red);
+    // the arrays (hundreds of MB on large designs) are allocated side by side
+    // on host threads: their first-touch page faults and zero fill dominate
+    // a sequential allocation
+    {
+        std::vector<std::function<void()>> allocs = {
+            [&] { S.glob.resize(o_loc[nsub]); },       [&] { S.scale.resize(o_loc[nsub]); },
+            [&] { S.slot_sub.resize(o_loc[nsub]); },   [&] { S.inv_e.resize(o_loc[nsub]); },
+            [&] { S.ct_ptr.resize(o_kp[nsub] + 1); },  [&] { S.ct_rowsum.resize(o_kp[nsub]); },
+            [&] { S.ct_row_slot.resize(o_kp[nsub]); }, [&] { S.ct_row_red.resize(o_kp[nsub]); },
+            [&] { S.ct_col.resize(o_ct[nsub]); },      [&] { S.ct_val.resize(o_ct[nsub]); },
+            [&] { S.c_ptr.resize(o_el[nsub] + 1); },   [&] { S.elim_slot.resize(o_el[nsub]); },
+            [&] { S.c_col.resize(o_c[nsub]); },        [&] { S.c_val.resize(o_c[nsub]); },
+            [&] { S.red_sub.resize(red); }};
+        par_for_each(allocs.size(), [&](size_t i) { allocs[i](); });
+    }
+    if (BuildTrace::on()) fprintf(stderr, "[within trace]     pack: allocation %.3f ms\n", (BuildTrace::now() - tr_pack.t0) * 1e3);
     // f(lo, hi) over [0, m) in blocks on host threads when m is large (every
     // block writes its own entries, so the result is the sequential loop's)
     auto blocked = [](uint32_t m, auto&& f) {

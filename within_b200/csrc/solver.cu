@@ -71,9 +71,11 @@ struct PhaseTrace {
     const char* what;
     double t0;
     explicit PhaseTrace(const char* w) : what(w), t0(trace_on() ? now_s() : 0.0) {}
-    ~PhaseTrace() {
-        if (trace_on()) fprintf(stderr, "[within trace] %s %.3f ms\n", what, (now_s() - t0) * 1e3);
+    void done() {
+        if (trace_on() && what) fprintf(stderr, "[within trace] %s %.3f ms\n", what, (now_s() - t0) * 1e3);
+        what = nullptr;
     }
+    ~PhaseTrace() { done(); }
 };
 
 double now_s() {
@@ -2053,8 +2055,11 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         ensure_scatter(*s, 1);
         if (env_path(2) == 2) ensure_rowsweep<1>(*s);
     }
+    pt_op.done();
     if (pre_thread.joinable()) {
+        PhaseTrace pt_wait("wait for the preconditioner host build");
         pre_thread.join();
+        pt_wait.done();
         if (pre_err) std::rethrow_exception(pre_err);
         PhaseTrace pt_up("preconditioner upload");
         s->n_warnings = pre.n_warnings;

@@ -128,6 +128,40 @@ __global__ void k_xt_transpose(uint32_t nnz, const uint64_t* __restrict__ tkey, 
     tval[k] = val[tidx[k]];
 }
 
+// connected components of the cell graph by label propagation with pointer
+// jumping: every vertex starts as its own label, every edge hooks the larger
+// of its two labels' representatives onto the smaller (atomicMin), then every
+// label jumps to its representative's label until both settle; repeated
+// until an edge pass sees no two different labels.  Labels only decrease and
+// the smallest vertex of a component keeps its own, so the fixed point -- the
+// smallest vertex of each component -- is the same whatever the schedule.
+__global__ void k_cc_init(uint32_t nv, uint32_t* __restrict__ lab) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < nv) lab[v] = v;
+}
+
+__global__ void k_cc_hook(uint32_t nnz, const uint32_t* __restrict__ ra, const uint32_t* __restrict__ cb,
+                          uint32_t L_a, uint32_t* lab, int* __restrict__ changed) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    const uint32_t a = lab[ra[k]], b = lab[L_a + cb[k]];
+    if (a == b) return;
+    atomicMin(&lab[a > b ? a : b], a < b ? a : b);
+    *changed = 1;
+}
+
+__global__ void k_cc_jump(uint32_t nv, uint32_t* lab) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    uint32_t l = lab[v];
+    for (uint32_t t = 0; t < 64; ++t) {   // at most 64 hops a pass; the passes repeat until labels settle
+        const uint32_t m = lab[l];
+        if (m == l) break;
+        l = m;
+    }
+    lab[v] = l;
+}
+
 struct DevBuf {
     std::vector<void*> p;
     template <class T>
@@ -163,6 +197,7 @@ void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32
     out.val.clear();
     out.row.clear();
     out.tval.clear();
+    out.comp.clear();
     if (n == 0) return;
     DevBuf B;
     uint64_t* key = B.get<uint64_t>(n);
@@ -233,12 +268,33 @@ void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32
     }
     k_xt_ptr<<<pg, XT_THREADS, 0, st>>>(nnz, tcol, L_b, cptr);
     XT_CK(cudaGetLastError());
+    // connected components over the kept cells
+    const uint32_t nv = L_a + L_b;
+    uint32_t* lab = B.get<uint32_t>(nv);
+    int* changed = B.get<int>(1);
+    k_cc_init<<<(nv + XT_THREADS - 1) / XT_THREADS, XT_THREADS, 0, st>>>(nv, lab);
+    XT_CK(cudaGetLastError());
+    for (uint32_t it = 0;; ++it) {
+        if (it > nv) throw std::runtime_error("gpu_cross_tab: components did not settle");
+        int h_changed = 0;
+        XT_CK(cudaMemsetAsync(changed, 0, sizeof(int), st));
+        if (nnz)
+            k_cc_hook<<<(nnz + XT_THREADS - 1) / XT_THREADS, XT_THREADS, 0, st>>>(nnz, ra, cb, L_a, lab, changed);
+        XT_CK(cudaGetLastError());
+        k_cc_jump<<<(nv + XT_THREADS - 1) / XT_THREADS, XT_THREADS, 0, st>>>(nv, lab);
+        XT_CK(cudaGetLastError());
+        XT_CK(cudaMemcpyAsync(&h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, st));
+        XT_CK(cudaStreamSynchronize(st));
+        if (!h_changed) break;
+    }
+    out.comp.resize(nv);
     out.col.resize(nnz);
     out.val.resize(nnz);
     out.row.resize(nnz);
     out.tval.resize(nnz);
     XT_CK(cudaMemcpyAsync(out.row_ptr.data(), rptr, ((size_t)L_a + 1) * 4, cudaMemcpyDeviceToHost, st));
     XT_CK(cudaMemcpyAsync(out.col_ptr.data(), cptr, ((size_t)L_b + 1) * 4, cudaMemcpyDeviceToHost, st));
+    XT_CK(cudaMemcpyAsync(out.comp.data(), lab, (size_t)nv * 4, cudaMemcpyDeviceToHost, st));
     if (nnz) {
         XT_CK(cudaMemcpyAsync(out.col.data(), cb, (size_t)nnz * 4, cudaMemcpyDeviceToHost, st));
         XT_CK(cudaMemcpyAsync(out.val.data(), val, (size_t)nnz * 8, cudaMemcpyDeviceToHost, st));
