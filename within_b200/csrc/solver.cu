@@ -1995,16 +1995,29 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
             if (weights) w_dev = tmp->upload(w);
             const std::vector<ChannelPair> cps = schwarz_channel_pairs(D);
             pre_xtabs.resize(cps.size());
-            for (size_t i = 0; i < cps.size(); ++i) {
-                const ChannelPair& cp = cps[i];
-                try {
-                    gpu_cross_tab(D.n_obs, op.codes[cp.term_a], D.terms[cp.term_a].n_levels, op.codes[cp.term_b],
-                                  D.terms[cp.term_b].n_levels, w_dev, cp.load_a < 0 ? nullptr : op.loads[cp.load_a],
-                                  cp.load_b < 0 ? nullptr : op.loads[cp.load_b], pre_xtabs[i], s->stream);
-                } catch (const std::runtime_error& e) {
-                    throw WError(ERR_CUDA, e.what());
-                }
-            }
+            // one host thread and stream per pair: the pairs' device work and
+            // their copies back (page faults of fresh host memory included) overlap
+            std::vector<std::string> errs(cps.size());
+            std::vector<std::thread> th;
+            for (size_t i = 0; i < cps.size(); ++i)
+                th.emplace_back([&, i] {
+                    const ChannelPair& cp = cps[i];
+                    cudaStream_t st = nullptr;
+                    try {
+                        set_device(device);
+                        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                        gpu_cross_tab(D.n_obs, op.codes[cp.term_a], D.terms[cp.term_a].n_levels,
+                                      op.codes[cp.term_b], D.terms[cp.term_b].n_levels, w_dev,
+                                      cp.load_a < 0 ? nullptr : op.loads[cp.load_a],
+                                      cp.load_b < 0 ? nullptr : op.loads[cp.load_b], pre_xtabs[i], st);
+                    } catch (const std::exception& e) {
+                        errs[i] = e.what();
+                    }
+                    if (st) cudaStreamDestroy(st);
+                });
+            for (auto& t : th) t.join();
+            for (const std::string& e : errs)
+                if (!e.empty()) throw WError(ERR_CUDA, e);
         }
         pre_thread = std::thread([&, use_xtab] {
             try {

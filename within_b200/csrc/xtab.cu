@@ -18,8 +18,12 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -35,6 +39,18 @@ namespace {
     } while (0)
 
 constexpr int XT_THREADS = 256;
+
+// WITHIN_TRACE=1: device and copy times of each cross-tab on stderr
+bool xt_trace() {
+    static const bool on = [] {
+        const char* e = std::getenv("WITHIN_TRACE");
+        return e && std::atoi(e) != 0;
+    }();
+    return on;
+}
+double xt_now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 int bits_for(uint32_t levels) {
     int b = 1;
@@ -188,6 +204,7 @@ int grid_of(uint64_t n) {
 // weights or nullptr.  Synchronous on `st`.
 void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32_t* b_dev, uint32_t L_b,
                    const double* w, const double* la, const double* lb, CrossTab& out, cudaStream_t st) {
+    const double t0 = xt_trace() ? xt_now() : 0.0;
     const int bits_a = bits_for(L_a), bits_b = bits_for(L_b);
     if (bits_a + bits_b > 64) throw std::runtime_error("gpu_cross_tab: level ids need more than 64 key bits");
     if (n >= 0xFFFFFFFFull) throw std::runtime_error("gpu_cross_tab: more than 2^32 - 1 observations");
@@ -288,10 +305,16 @@ void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32
         if (!h_changed) break;
     }
     out.comp.resize(nv);
-    out.col.resize(nnz);
-    out.val.resize(nnz);
-    out.row.resize(nnz);
-    out.tval.resize(nnz);
+    if (xt_trace()) XT_CK(cudaStreamSynchronize(st));   // so the trace splits device and copy time
+    const double t_dev = xt_trace() ? xt_now() : 0.0;
+    {   // fresh host arrays side by side (their first-touch page faults dominate one thread's resize)
+        std::thread a([&] { out.col.resize(nnz); }), b([&] { out.val.resize(nnz); }),
+            c([&] { out.row.resize(nnz); });
+        out.tval.resize(nnz);
+        a.join();
+        b.join();
+        c.join();
+    }
     XT_CK(cudaMemcpyAsync(out.row_ptr.data(), rptr, ((size_t)L_a + 1) * 4, cudaMemcpyDeviceToHost, st));
     XT_CK(cudaMemcpyAsync(out.col_ptr.data(), cptr, ((size_t)L_b + 1) * 4, cudaMemcpyDeviceToHost, st));
     XT_CK(cudaMemcpyAsync(out.comp.data(), lab, (size_t)nv * 4, cudaMemcpyDeviceToHost, st));
@@ -302,6 +325,9 @@ void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32
         XT_CK(cudaMemcpyAsync(out.tval.data(), tval, (size_t)nnz * 8, cudaMemcpyDeviceToHost, st));
     }
     XT_CK(cudaStreamSynchronize(st));
+    if (xt_trace())
+        fprintf(stderr, "[within trace]   GPU cross-tab %u x %u, %u cells: device %.3f ms, host copies %.3f ms\n", L_a,
+                L_b, nnz, (t_dev - t0) * 1e3, (xt_now() - t_dev) * 1e3);
 }
 
 }  // namespace wgpu
