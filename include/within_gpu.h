@@ -157,6 +157,8 @@ typedef struct {
     int32_t gpu_cross_tab;      /* the additive-Schwarz set-up's cross-tabs on the GPU (sort and segment;
                                    the same bits as on the host): 1 (default) for designs of at least
                                    2^18 observations, 2 always, 0 never */
+    int32_t vector_rows;        /* 1: the C back-substitution's short rows by groups of lanes (coalesced
+                                   reads, a fixed tree per row) instead of one thread per row; 0 (default) */
 } within_tuning;
 void within_tuning_default(within_tuning* t);
 int within_solver_new_tuned(const within_design* design, const double* weights,

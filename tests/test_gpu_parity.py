@@ -383,6 +383,7 @@ def test_windowed_reorthogonalisation_matches_restatement(wb, oracle, local_size
     {"core_small": 0, "core_min_frac": 0.1},
     {"core_dense_late": 256, "core_dense_max": 256},
     {"warp_ranges": 0},
+    {"vector_rows": 1},
 ])
 def test_tuning_records_match_oracle(wb, oracle, tuning):
     """Every kernel variant and factor rule a tuning record can select gives

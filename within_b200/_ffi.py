@@ -75,7 +75,8 @@ class TuningC(C.Structure):
     _fields_ = [("staged_sweep", C.c_int32), ("wide_mean_len", C.c_uint32), ("fuse_rounds", C.c_int32),
                 ("thread_per_segment", C.c_int32), ("core_dense_max", C.c_uint32), ("core_min_frac", C.c_double),
                 ("max_rounds", C.c_uint32), ("core_small", C.c_uint32), ("core_dense_late", C.c_uint32),
-                ("warp_ranges", C.c_int32), ("gpu_cross_tab", C.c_int32)]
+                ("warp_ranges", C.c_int32), ("gpu_cross_tab", C.c_int32),
+                ("vector_rows", C.c_int32)]
 
 
 class PrecondStatsC(C.Structure):

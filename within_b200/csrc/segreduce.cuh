@@ -339,6 +339,68 @@ segthread_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ ski
     f.emit(pr, sg, acc);
 }
 
+// G lanes per segment, for a problem whose segments are all short (at most
+// SEGT_MAX_LEN positions, as the rows of C are): the G lanes of a group read
+// consecutive positions of their segment (coalesced across the warp), lane j
+// summing positions j, j + G, ... in order (up to four values requested
+// before any is added), then a fixed xor tree adds the G lane sums and the
+// group's first lane emits.  Every sum has one fixed order, so results are
+// bitwise reproducible (they differ in the last bits from segthread_kernel's
+// sequential sums).
+template <class F, int K, int G>
+__global__ void __launch_bounds__(SEGT_THREADS)
+segvec_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ skip) {
+    static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "lanes per segment: a power of two up to 32");
+    using A = typename F::Acc;
+    if (skip && *skip) return;
+    const unsigned FULL = 0xffffffffu;
+    const uint32_t t = blockIdx.x * SEGT_THREADS + threadIdx.x;
+    const uint32_t sg = t / G, j = t % G;
+    const bool valid = sg < n_seg;   // every lane of the warp reaches the shuffles
+    const typename F::Prob pr = f.probs[prob];
+    A acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = (A)0;
+    if (valid) {
+        const uint32_t* ptr = f.seg_ptr(pr);
+        const uint32_t a = __ldg(ptr + sg), b = __ldg(ptr + sg + 1);
+        uint32_t q = a + j;
+        for (; q + 3 * G < b; q += 4 * G) {
+            A v0[K], v1[K], v2[K], v3[K];
+            f.value(pr, q, v0);
+            f.value(pr, q + G, v1);
+            f.value(pr, q + 2 * G, v2);
+            f.value(pr, q + 3 * G, v3);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                acc[k] += v0[k];
+                acc[k] += v1[k];
+                acc[k] += v2[k];
+                acc[k] += v3[k];
+            }
+        }
+        for (; q < b; q += G) {
+            A v[K];
+            f.value(pr, q, v);
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] += v[k];
+        }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += __shfl_xor_sync(FULL, acc[k], o);
+    if (valid && j == 0) f.emit(pr, sg, acc);
+}
+
+// lanes per segment for a plan of mean segment length `mean` (segvec_kernel):
+// about two positions per lane, 0 = one thread per segment
+inline int segvec_lanes(double mean) {
+    int g = 1;
+    while (g < 32 && 2.0 * g < mean) g *= 2;
+    return g >= 4 ? g : 0;
+}
+
 // A run of consecutive elimination rounds whose segments are all short and
 // few (the small tail of a round-scheduled factor: rounds of a few hundred
 // rows each): one block walks the rounds in order (forward) or in reverse

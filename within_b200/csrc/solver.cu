@@ -152,6 +152,8 @@ struct Tuning {
     // cross-tabs of the additive-Schwarz set-up on the GPU (xtab.cu): 1 for
     // designs of at least XTAB_MIN_OBS observations, 2 always, 0 never
     int gpu_cross_tab = 1;
+    // C's rows (all short) by groups of lanes (segvec_kernel) instead of one thread each
+    bool vector_rows = false;
 };
 constexpr uint64_t XTAB_MIN_OBS = 1ull << 18;
 
@@ -164,6 +166,7 @@ Tuning resolve_tuning(const within_tuning* t) {
         r.segthread = t->thread_per_segment != 0;
         r.warp_ranges = t->warp_ranges;
         r.gpu_cross_tab = t->gpu_cross_tab;
+        r.vector_rows = t->vector_rows != 0;
         return r;
     }
     if (const char* e = getenv("WITHIN_TSWEEP")) r.staged = atoi(e) != 0;
@@ -173,6 +176,7 @@ Tuning resolve_tuning(const within_tuning* t) {
     if (const char* e = getenv("WITHIN_SEGTHREAD")) r.segthread = atoi(e) != 0;
     if (const char* e = getenv("WITHIN_WARP_RANGES")) r.warp_ranges = atoi(e);
     if (const char* e = getenv("WITHIN_GPU_XTAB")) r.gpu_cross_tab = atoi(e);
+    if (const char* e = getenv("WITHIN_VECTOR_ROWS")) r.vector_rows = atoi(e) != 0;
     return r;
 }
 
@@ -233,6 +237,20 @@ void launch_segthread(const F& f, uint32_t prob, uint32_t n_seg, const int* skip
     if (!n_seg) return;
     segthread_kernel<F, K><<<(n_seg + SEGT_THREADS - 1) / SEGT_THREADS, SEGT_THREADS, 0, st>>>(f, prob, n_seg,
                                                                                                 skip);
+    ++g_launches;
+}
+
+template <class F, int K>
+void launch_segvec(const F& f, uint32_t prob, uint32_t n_seg, int lanes, const int* skip, cudaStream_t st) {
+    if (!n_seg) return;
+    const uint64_t threads = (uint64_t)n_seg * lanes;
+    const unsigned grid = (unsigned)((threads + SEGT_THREADS - 1) / SEGT_THREADS);
+    switch (lanes) {
+        case 4: segvec_kernel<F, K, 4><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
+        case 8: segvec_kernel<F, K, 8><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
+        case 16: segvec_kernel<F, K, 16><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
+        default: segvec_kernel<F, K, 32><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
+    }
     ++g_launches;
 }
 
@@ -449,6 +467,7 @@ struct KPlans {
     // C, the prolongation and each elimination round on one thread per segment
     // when every segment is short: segment counts (0: segmented reduction)
     uint32_t c_thread = 0, prolong_thread = 0;
+    int c_lanes = 0;   // C's rows by groups of this many lanes (segvec_kernel), 0 = one thread each
     std::vector<uint32_t> fwd_thread, bwd_thread;
     // rounds [fuse_lo, n_rounds) run as one single-block launch per direction
     // (rounds_fused_kernel) when each has at most RF_MAX_ROWS short rows
@@ -507,6 +526,8 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     const bool segt_on = U.tuning.segthread;
     if (segt_on && H.c_ptr.size() > 1 && seg_max_len(H.c_ptr.data(), H.c_ptr.size() - 1) <= SEGT_MAX_LEN)
         kp.c_thread = (uint32_t)(H.c_ptr.size() - 1);
+    if (kp.c_thread && U.tuning.vector_rows)
+        kp.c_lanes = segvec_lanes((double)(H.c_ptr.back() - H.c_ptr.front()) / (double)kp.c_thread);
     if (segt_on && H.dof_ptr.size() > 1 && seg_max_len(H.dof_ptr.data(), H.dof_ptr.size() - 1) <= SEGT_MAX_LEN)
         kp.prolong_thread = (uint32_t)(H.dof_ptr.size() - 1);
     kp.core = one(H.core_rows_ptr, ss);
@@ -662,7 +683,8 @@ void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const T* r, T* z, c
         if (kp.bwd_thread[r]) launch_segthread<BF, K>(BF{P.p_bwd, S}, r, kp.bwd_thread[r], skip, st);
         else launch_sr<BF, K>(BF{P.p_bwd, S}, kp.bwd, kp.bwd.range_lo[r], kp.bwd.range_hi[r], skip, st);
     }
-    if (kp.c_thread) launch_segthread<CFT, K>(CFT{P.p_c, S}, 0, kp.c_thread, skip, st);
+    if (kp.c_thread && kp.c_lanes) launch_segvec<CFT, K>(CFT{P.p_c, S}, 0, kp.c_thread, kp.c_lanes, skip, st);
+    else if (kp.c_thread) launch_segthread<CFT, K>(CFT{P.p_c, S}, 0, kp.c_thread, skip, st);
     else launch_sr<CFT, K>(CFT{P.p_c, S}, kp.c, 0, kp.c.n_tiles, skip, st);
     launch_sr<MF, K>(MF{P.p_restrict, S}, kp.restrict_, 0, kp.restrict_.n_tiles, skip, st);
     if (kp.prolong_thread) launch_segthread<PF, K>(PF{P.p_prolong, S, z}, 0, kp.prolong_thread, skip, st);
@@ -2386,6 +2408,7 @@ void within_tuning_default(within_tuning* t) {
     t->core_dense_late = pc.core_dense_late;
     t->warp_ranges = 1;
     t->gpu_cross_tab = 1;
+    t->vector_rows = 0;
 }
 
 int within_solver_new_tuned(const within_design* design, const double* weights, const within_precond_config* cfg,

@@ -178,17 +178,21 @@ __global__ void k_cc_jump(uint32_t nv, uint32_t* lab) {
     lab[v] = l;
 }
 
+// temporaries from the device's stream-ordered pool: no device-wide
+// synchronisation per allocation or free (the pairs run side by side)
 struct DevBuf {
+    cudaStream_t st;
     std::vector<void*> p;
+    explicit DevBuf(cudaStream_t s) : st(s) {}
     template <class T>
     T* get(size_t n) {
         void* q = nullptr;
-        XT_CK(cudaMalloc(&q, std::max<size_t>(1, n) * sizeof(T)));
+        XT_CK(cudaMallocAsync(&q, std::max<size_t>(1, n) * sizeof(T), st));
         p.push_back(q);
         return (T*)q;
     }
     ~DevBuf() {
-        for (void* q : p) cudaFree(q);
+        for (void* q : p) cudaFreeAsync(q, st);
     }
 };
 
@@ -216,7 +220,7 @@ void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32
     out.tval.clear();
     out.comp.clear();
     if (n == 0) return;
-    DevBuf B;
+    DevBuf B(st);
     uint64_t* key = B.get<uint64_t>(n);
     uint64_t* skey = B.get<uint64_t>(n);
     uint32_t* idx = B.get<uint32_t>(n);
