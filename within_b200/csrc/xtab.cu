@@ -178,22 +178,22 @@ __global__ void k_cc_jump(uint32_t nv, uint32_t* lab) {
     lab[v] = l;
 }
 
-// temporaries from the device's stream-ordered pool: no device-wide
-// synchronisation per allocation or free (the pairs run side by side)
+// all temporaries of one cross-tab carved from a single allocation sized for
+// the worst case (cells and kept cells bounded by the observations), so a
+// pair pays one allocation and one free
 struct DevBuf {
-    cudaStream_t st;
-    std::vector<void*> p;
-    explicit DevBuf(cudaStream_t s) : st(s) {}
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+    explicit DevBuf(size_t bytes) : cap(bytes) { XT_CK(cudaMalloc((void**)&base, cap)); }
     template <class T>
     T* get(size_t n) {
-        void* q = nullptr;
-        XT_CK(cudaMallocAsync(&q, std::max<size_t>(1, n) * sizeof(T), st));
-        p.push_back(q);
-        return (T*)q;
+        const size_t b = (std::max<size_t>(1, n) * sizeof(T) + 255) / 256 * 256;
+        if (used + b > cap) throw std::runtime_error("gpu_cross_tab: scratch plan exceeded");
+        T* q = reinterpret_cast<T*>(base + used);
+        used += b;
+        return q;
     }
-    ~DevBuf() {
-        for (void* q : p) cudaFreeAsync(q, st);
-    }
+    ~DevBuf() { cudaFree(base); }
 };
 
 int grid_of(uint64_t n) {
@@ -220,23 +220,25 @@ void gpu_cross_tab(uint64_t n, const uint32_t* a_dev, uint32_t L_a, const uint32
     out.tval.clear();
     out.comp.clear();
     if (n == 0) return;
-    DevBuf B(st);
+    // scratch of every step below, with the library's temporary sizes queried for n items
+    size_t tb = 0, sb = 0;
+    XT_CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)nullptr, (uint64_t*)nullptr, (uint32_t*)nullptr,
+                                          (uint32_t*)nullptr, (int64_t)n, 0, bits_a + bits_b, st));
+    XT_CK(cub::DeviceScan::InclusiveSum(nullptr, sb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)n, st));
+    const size_t pad = 32 * 256;
+    DevBuf B(116 * n + 2 * (tb + sb) + 8 * ((size_t)L_a + L_b + 2) + pad);
     uint64_t* key = B.get<uint64_t>(n);
     uint64_t* skey = B.get<uint64_t>(n);
     uint32_t* idx = B.get<uint32_t>(n);
     uint32_t* sidx = B.get<uint32_t>(n);
     k_xt_keys<<<grid_of(n), XT_THREADS, 0, st>>>(n, a_dev, b_dev, bits_b, key, idx);
     XT_CK(cudaGetLastError());
-    size_t tb = 0;
-    XT_CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, skey, idx, sidx, (int64_t)n, 0, bits_a + bits_b, st));
     void* tmp = B.get<char>(tb);
     XT_CK(cub::DeviceRadixSort::SortPairs(tmp, tb, key, skey, idx, sidx, (int64_t)n, 0, bits_a + bits_b, st));
     uint32_t* head = B.get<uint32_t>(n);
     uint32_t* cell_of = B.get<uint32_t>(n);
     k_xt_heads<<<grid_of(n), XT_THREADS, 0, st>>>(n, skey, head);
     XT_CK(cudaGetLastError());
-    size_t sb = 0;
-    XT_CK(cub::DeviceScan::InclusiveSum(nullptr, sb, head, cell_of, (int64_t)n, st));
     void* stmp = B.get<char>(sb);
     XT_CK(cub::DeviceScan::InclusiveSum(stmp, sb, head, cell_of, (int64_t)n, st));
     uint32_t n_cells = 0;
