@@ -17,7 +17,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["solver.cu", "xtab.cu", "host_design.cpp", "host_schwarz.cpp"]
 HEADERS = ["host.hpp", "kernels.cuh", "segreduce.cuh", "segplan.hpp", "refine.cuh", "rowsweep.cuh",
-           "bulk.cuh", "tsweep.cuh", "segsweep.cuh"]
+           "bulk.cuh", "tsweep.cuh", "segsweep.cuh", "pdl.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

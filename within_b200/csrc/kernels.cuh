@@ -7,6 +7,7 @@
 // strided partials, a fixed shuffle tree, per-block partials summed by the last
 // block in block order), so every result is bitwise reproducible.
 #pragma once
+#include "pdl.cuh"
 #include <cfloat>
 #include <climits>
 #include <cstdint>
@@ -288,6 +289,8 @@ __device__ __forceinline__ void rows4_dx(const OpParamsT<T>& p, uint32_t base, i
 // y = W^{1/2} D x  (Operator::apply; internal order)
 template <int K, class T = double>
 __global__ void k_apply(OpParamsT<T> p, const T* __restrict__ x, T* __restrict__ y, const int* skip = nullptr) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (skip && *skip) return;
     const uint32_t stride = gridDim.x * blockDim.x * 4;
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * 4; base < p.n; base += stride) {
@@ -308,6 +311,8 @@ __global__ void k_apply(OpParamsT<T> p, const T* __restrict__ x, T* __restrict__
 template <int K>
 __global__ void k_demean(OpParams p, const double* __restrict__ x, const double* __restrict__ yint,
                          double* __restrict__ out) {
+    pdl_wait();
+    pdl_launch_dependents();
     const uint32_t stride = gridDim.x * blockDim.x * 4;
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * 4; base < p.n; base += stride) {
         const int nr = (int)min(4u, p.n - base);
@@ -331,6 +336,8 @@ template <int K>
 __global__ void __launch_bounds__(RED_THREADS)
 k_gather_update(OpParams p, const double* __restrict__ v, double* __restrict__ u, ColState* cur,
                 Ctl* ctl, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) {
         // nothing left to update this iteration either (k_alpha_step also returns)
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->k5_skip = 1;
@@ -838,6 +845,8 @@ struct ProlongF {
 template <int K, class T = double>
 __global__ void k_diag_apply(uint32_t n, const T* __restrict__ d, const T* __restrict__ p,
                              T* __restrict__ v, const Ctl* ctl) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl && ctl->all_done) return;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const double dj = d ? (double)d[j] : 1.0;
@@ -864,6 +873,8 @@ template <int K>
 __global__ void __launch_bounds__(RED_THREADS)
 k_alpha_step(uint32_t n, const double* __restrict__ v, const double* __restrict__ p,
              const ColState* cur, ColState* nxt, Ctl* ctl, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     double acc[3 * K];
 #pragma unroll
@@ -985,6 +996,8 @@ __global__ void k_solution_update(uint32_t n, double* __restrict__ v, double* __
                                   double* __restrict__ hb, double* __restrict__ x,
                                   const ColState* nxt, const Ctl* ctl, Ring ring = Ring{nullptr, nullptr, 0},
                                   const double* __restrict__ p = nullptr) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->k5_skip) return;
     double vs[K], tx[K], thb[K], th[K];
     bool up[K];
@@ -1031,6 +1044,8 @@ template <int K>
 __global__ void __launch_bounds__(RED_THREADS)
 k_reorth_dot(uint32_t n, int j, Ring ring, const double* __restrict__ v, const ColState* cur, const Ctl* ctl,
              double* coef, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     size_t slot[K];
     bool ok[K];
@@ -1058,6 +1073,8 @@ k_reorth_dot(uint32_t n, int j, Ring ring, const double* __restrict__ v, const C
 template <int K>
 __global__ void k_reorth_axpy(uint32_t n, int j, Ring ring, double* __restrict__ v, double* __restrict__ p,
                               const ColState* cur, const Ctl* ctl, const double* coef) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     size_t slot[K];
     double c[K];
@@ -1090,6 +1107,8 @@ __global__ void __launch_bounds__(RED_THREADS)
 k_load_rhs(uint32_t n, uint32_t k_used, const double* __restrict__ Y, const uint32_t* __restrict__ perm,
            const double* __restrict__ sqrt_w, double* __restrict__ yint, double* __restrict__ b,
            double* partials, unsigned* counter, double* out_max, int* nonfinite) {
+    pdl_wait();
+    pdl_launch_dependents();
     double mx[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) mx[k] = 0.0;
@@ -1151,6 +1170,8 @@ __global__ void __launch_bounds__(RED_THREADS)
 k_norm_b(uint32_t n, const double* __restrict__ b, const double* bmax, ColState* st, double tol,
          long long maxiter, uint32_t k_used, Ctl* ctl, double* partials, unsigned* counter, int warm = 0,
          int stale_window = 0, double stale_thr = 0.0) {
+    pdl_wait();
+    pdl_launch_dependents();
     double acc[K];
     double sc[K];
 #pragma unroll
@@ -1210,6 +1231,8 @@ k_norm_b(uint32_t n, const double* __restrict__ b, const double* bmax, ColState*
 template <int K>
 __global__ void k_load_x0(uint32_t nd, uint32_t k_used, const double* __restrict__ x0, double* __restrict__ out,
                           int* nonfinite) {
+    pdl_wait();
+    pdl_launch_dependents();
     int bad = 0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nd; j += gridDim.x * blockDim.x) {
         double v[K];
@@ -1229,6 +1252,8 @@ template <int K>
 __global__ void __launch_bounds__(RED_THREADS)
 k_warm_rhs(OpParams p, const double* __restrict__ x0, double* __restrict__ b, double* partials, unsigned* counter,
            double* out_max) {
+    pdl_wait();
+    pdl_launch_dependents();
     double mx[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) mx[k] = 0.0;
@@ -1296,12 +1321,16 @@ k_warm_rhs(OpParams p, const double* __restrict__ x0, double* __restrict__ b, do
 // x <- x + x0 after a warm-started solve (mlsmr, lsmr.rs:293-297)
 template <int K>
 __global__ void k_add_x0(uint32_t nd, double* __restrict__ x, const double* __restrict__ x0) {
+    pdl_wait();
+    pdl_launch_dependents();
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nd * K; j += gridDim.x * blockDim.x) x[j] += x0[j];
 }
 
 template <int K>
 __global__ void k_scale_u(uint32_t n, const double* __restrict__ b, double* __restrict__ u,
                           const ColState* st) {
+    pdl_wait();
+    pdl_launch_dependents();
     double inv[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) inv[k] = st[k].beta > 0.0 ? 1.0 / st[k].beta : 0.0;
@@ -1315,6 +1344,8 @@ template <int K>
 __global__ void __launch_bounds__(RED_THREADS)
 k_alpha_init(uint32_t n, const double* __restrict__ v, const double* __restrict__ p, ColState* st,
              ColState* st_other, Ctl* ctl, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_launch_dependents();
     double acc[3 * K];
 #pragma unroll
     for (int i = 0; i < 3 * K; ++i) acc[i] = 0.0;
@@ -1376,6 +1407,8 @@ template <int K>
 __global__ void k_init_vectors(uint32_t n, double* __restrict__ v, double* __restrict__ h,
                                double* __restrict__ hb, double* __restrict__ x, const ColState* st,
                                Ring ring = Ring{nullptr, nullptr, 0}, const double* __restrict__ p = nullptr) {
+    pdl_wait();
+    pdl_launch_dependents();
     double vs[K], ps[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -1403,6 +1436,8 @@ __global__ void k_init_vectors(uint32_t n, double* __restrict__ v, double* __res
 template <int K>
 __global__ void k_store_obs(uint32_t n, uint32_t k_used, const double* __restrict__ src,
                             const uint32_t* __restrict__ perm, double* __restrict__ dst) {
+    pdl_wait();
+    pdl_launch_dependents();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t d = perm ? perm[i] : i;
         double v[K];
@@ -1415,6 +1450,8 @@ __global__ void k_store_obs(uint32_t n, uint32_t k_used, const double* __restric
 template <int K>
 __global__ void k_store_dofs(uint32_t n, uint32_t k_used, const double* __restrict__ src,
                              double* __restrict__ dst) {
+    pdl_wait();
+    pdl_launch_dependents();
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         double v[K];
         ldk<K, double>(src + (size_t)j * K, v);
@@ -1432,6 +1469,8 @@ __global__ void k_store_dofs(uint32_t n, uint32_t k_used, const double* __restri
 
 __global__ void k_adjoint_rhs(uint64_t n, uint32_t k, const double* __restrict__ v,
                               const double* __restrict__ w, double* __restrict__ a) {
+    pdl_wait();
+    pdl_launch_dependents();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const double wi = w ? w[i] : 1.0;
         for (uint32_t c = 0; c < k; ++c) a[(size_t)c * n + i] = w ? v[(size_t)c * n + i] / wi : v[(size_t)c * n + i];
@@ -1441,6 +1480,8 @@ __global__ void k_adjoint_rhs(uint64_t n, uint32_t k, const double* __restrict__
 __global__ void k_demean_vjp(uint64_t n, uint32_t k, const double* __restrict__ r, const double* __restrict__ a,
                              const double* __restrict__ s, const double* __restrict__ w,
                              double* __restrict__ gz, double* __restrict__ gw) {
+    pdl_wait();
+    pdl_launch_dependents();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const double wi = w ? w[i] : 1.0;
         double g = 0.0;

@@ -26,6 +26,7 @@
 // rounding of the FP32-stored sums at least as tightly as compensated FP32
 // summation would.
 #pragma once
+#include "pdl.cuh"
 #include "kernels.cuh"
 
 namespace wgpu {
@@ -53,6 +54,8 @@ template <int K>
 __global__ void __launch_bounds__(RED_THREADS)
 k_resid64(OpParams p, const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r,
           CgCol* st, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_launch_dependents();
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
@@ -83,6 +86,8 @@ k_resid64(OpParams p, const double* __restrict__ x, const double* __restrict__ b
 // inner start: res = (T) g, d = 0
 template <int K, class T>
 __global__ void k_cg_start(uint32_t n, const double* __restrict__ g, T* __restrict__ res, T* __restrict__ d) {
+    pdl_wait();
+    pdl_launch_dependents();
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -98,6 +103,8 @@ template <int K, class T>
 __global__ void __launch_bounds__(RED_THREADS)
 k_cg_init(uint32_t n, const T* __restrict__ res, const T* __restrict__ z, T* __restrict__ p, CgCol* st, Ctl* ctl,
           int first, double* partials, unsigned* counter, int use_h, cudaGraphConditionalHandle h_in) {
+    pdl_wait();
+    pdl_launch_dependents();
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
@@ -169,6 +176,8 @@ template <int K, class T>
 __global__ void __launch_bounds__(RED_THREADS)
 k_cg_alpha(uint32_t n, const T* __restrict__ p, const T* __restrict__ q, CgCol* st, Ctl* ctl, double* partials,
            unsigned* counter) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     double acc[K];
 #pragma unroll
@@ -194,6 +203,8 @@ k_cg_alpha(uint32_t n, const T* __restrict__ p, const T* __restrict__ q, CgCol* 
 template <int K, class T>
 __global__ void k_cg_update(uint32_t n, const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ d,
                             T* __restrict__ res, const CgCol* st, const Ctl* ctl) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     double a[K];
     bool act[K];
@@ -217,6 +228,8 @@ template <int K, class T>
 __global__ void __launch_bounds__(RED_THREADS)
 k_cg_beta(uint32_t n, const T* __restrict__ res, const T* __restrict__ z, CgCol* st, Ctl* ctl, double* partials,
           unsigned* counter) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     double acc[K];
 #pragma unroll
@@ -257,6 +270,8 @@ k_cg_beta(uint32_t n, const T* __restrict__ res, const T* __restrict__ z, CgCol*
 // p = z + beta p
 template <int K, class T>
 __global__ void k_cg_dir(uint32_t n, const T* __restrict__ z, T* __restrict__ p, const CgCol* st, const Ctl* ctl) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     double b[K];
     bool act[K];
@@ -277,6 +292,8 @@ __global__ void k_cg_dir(uint32_t n, const T* __restrict__ z, T* __restrict__ p,
 // x += d (FP64 accumulation of the FP32 correction)
 template <int K, class T>
 __global__ void k_add_delta(uint32_t n, const T* __restrict__ d, double* __restrict__ x) {
+    pdl_wait();
+    pdl_launch_dependents();
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
 #pragma unroll
         for (int k = 0; k < K; ++k) x[(size_t)j * K + k] += (double)d[(size_t)j * K + k];

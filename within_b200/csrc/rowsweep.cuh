@@ -37,6 +37,7 @@
 // rest terms need it);  3 -- the refinement step's FP64 residual r = b - A x,
 // ||r||^2 and g = A^T r in one pass (r stored only when rest terms need it).
 #pragma once
+#include "pdl.cuh"
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -324,6 +325,8 @@ __device__ __forceinline__ void rw_finish(const OpParamsT<T>& p, const RwParams&
 template <int K, int MODE, class T, bool SIMPLE>
 __global__ void __launch_bounds__(256)
 k_rw_fix(OpParamsT<T> p, RwParams rw, const Ctl* ctl, const int* skip) {
+    pdl_wait();
+    pdl_launch_dependents();
     using TO = std::conditional_t<MODE == 2, T, double>;
     if (MODE == 1 && ctl->all_done) return;
     if (MODE != 1 && skip && *skip) return;
@@ -353,6 +356,8 @@ template <int K, int MODE, class T, bool SIMPLE>
 __global__ void __launch_bounds__(RW_THREADS, rw_min_blocks<K>())
 k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__ u, ColState* cur, Ctl* ctl,
            const int* skip, int store, const T* __restrict__ rhs, double* sq_out, int sq_stride) {
+    pdl_wait();
+    pdl_launch_dependents();
     using TO = std::conditional_t<MODE == 2, T, double>;
     constexpr int R = rw_rows<K>();
     constexpr int CH = 32 * R;
@@ -734,6 +739,8 @@ k_rowsweep(OpParamsT<T> p, RwParams rw, const T* __restrict__ v, T* __restrict__
 template <int K>
 __global__ void k_ptilde(uint32_t nd, const double* __restrict__ atu, double* __restrict__ pt,
                          const ColState* cur, const Ctl* ctl) {
+    pdl_wait();
+    pdl_launch_dependents();
     if (ctl->all_done) return;
     double inv[K], coef[K];
     bool act[K];

@@ -22,6 +22,7 @@
 // The tile/split tables are built once on the host (HostPlan::add) from the
 // segment pointer arrays, which never change after set-up.
 #pragma once
+#include "pdl.cuh"
 #include <cstdint>
 
 #include "segplan.hpp"
@@ -73,6 +74,8 @@ segreduce_kernel(F f, const SRTile* __restrict__ tiles, uint32_t tile_base,
                  const SRSplit* __restrict__ splits, double* __restrict__ head_buf,
                  double* __restrict__ tail_buf, unsigned* __restrict__ counters,
                  const int* __restrict__ skip) {
+    pdl_wait();
+    pdl_launch_dependents();
     constexpr int T = SR_THREADS * ITEMS;
     using Prob = typename F::Prob;
     using A = typename F::Acc;
@@ -327,6 +330,8 @@ constexpr int SEGT_THREADS = 256;
 template <class F, int K>
 __global__ void __launch_bounds__(SEGT_THREADS)
 segthread_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ skip) {
+    pdl_wait();
+    pdl_launch_dependents();
     using A = typename F::Acc;
     if (skip && *skip) return;
     const uint32_t sg = blockIdx.x * SEGT_THREADS + threadIdx.x;
@@ -350,6 +355,8 @@ segthread_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ ski
 template <class F, int K, int G>
 __global__ void __launch_bounds__(SEGT_THREADS)
 segvec_kernel(F f, uint32_t prob, uint32_t n_seg, const int* __restrict__ skip) {
+    pdl_wait();
+    pdl_launch_dependents();
     static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "lanes per segment: a power of two up to 32");
     using A = typename F::Acc;
     if (skip && *skip) return;
@@ -416,6 +423,8 @@ template <class F, int K>
 __global__ void __launch_bounds__(RF_THREADS)
 rounds_fused_kernel(F f, const uint32_t* __restrict__ round_rows, uint32_t r_lo, uint32_t r_hi, int backward,
                     const int* __restrict__ skip) {
+    pdl_wait();
+    pdl_launch_dependents();
     using A = typename F::Acc;
     if (skip && *skip) return;
     for (uint32_t i = 0; i < r_hi - r_lo; ++i) {

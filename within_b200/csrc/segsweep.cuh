@@ -25,6 +25,7 @@
 //
 // The range tables are built once on the host (SSHostPlan::add).
 #pragma once
+#include "pdl.cuh"
 #include <cstdint>
 
 #include "segplan.hpp"
@@ -69,6 +70,8 @@ segsweep_kernel(F f, const SSRange* __restrict__ ranges, uint32_t r_lo, uint32_t
                 const uint32_t* __restrict__ empties, const SSSplit* __restrict__ splits,
                 double* __restrict__ head_buf, double* __restrict__ tail_buf, unsigned* __restrict__ counters,
                 const int* __restrict__ skip) {
+    pdl_wait();
+    pdl_launch_dependents();
     using Prob = typename F::Prob;
     using A = typename F::Acc;
     constexpr uint32_t CH = 32u * R;

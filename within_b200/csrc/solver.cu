@@ -232,10 +232,36 @@ uint32_t ss_target_warps(int K) {
     return (uint32_t)(sms * blocks * (SS_THREADS / 32));
 }
 
+// Kernels launched with programmatic stream serialisation (pdl.cuh): each
+// may be scheduled while its predecessor's last blocks run and waits for it
+// in-kernel.  Process-wide; WITHIN_PDL=0 launches in plain stream order.
+bool pdl_on() {
+    static const bool on = [] {
+        const char* e = getenv("WITHIN_PDL");
+        return e ? atoi(e) != 0 : true;
+    }();
+    return on;
+}
+
+template <class... KArgs, class... Args>
+void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_on() ? 1 : 0;
+    CK(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+}
+
 template <class F, int K>
 void launch_segthread(const F& f, uint32_t prob, uint32_t n_seg, const int* skip, cudaStream_t st) {
     if (!n_seg) return;
-    segthread_kernel<F, K><<<(n_seg + SEGT_THREADS - 1) / SEGT_THREADS, SEGT_THREADS, 0, st>>>(f, prob, n_seg,
+    launch_k(segthread_kernel<F, K>, (n_seg + SEGT_THREADS - 1) / SEGT_THREADS, SEGT_THREADS, 0, st, f, prob, n_seg,
                                                                                                 skip);
     ++g_launches;
 }
@@ -246,10 +272,10 @@ void launch_segvec(const F& f, uint32_t prob, uint32_t n_seg, int lanes, const i
     const uint64_t threads = (uint64_t)n_seg * lanes;
     const unsigned grid = (unsigned)((threads + SEGT_THREADS - 1) / SEGT_THREADS);
     switch (lanes) {
-        case 4: segvec_kernel<F, K, 4><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
-        case 8: segvec_kernel<F, K, 8><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
-        case 16: segvec_kernel<F, K, 16><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
-        default: segvec_kernel<F, K, 32><<<grid, SEGT_THREADS, 0, st>>>(f, prob, n_seg, skip); break;
+        case 4: launch_k(segvec_kernel<F, K, 4>, grid, SEGT_THREADS, 0, st, f, prob, n_seg, skip); break;
+        case 8: launch_k(segvec_kernel<F, K, 8>, grid, SEGT_THREADS, 0, st, f, prob, n_seg, skip); break;
+        case 16: launch_k(segvec_kernel<F, K, 16>, grid, SEGT_THREADS, 0, st, f, prob, n_seg, skip); break;
+        default: launch_k(segvec_kernel<F, K, 32>, grid, SEGT_THREADS, 0, st, f, prob, n_seg, skip); break;
     }
     ++g_launches;
 }
@@ -259,20 +285,20 @@ void launch_sr(const F& f, const DevPlan& p, uint32_t lo, uint32_t hi, const int
     if (hi <= lo) return;
     if (p.ss) {
         constexpr uint32_t WPB = SS_THREADS / 32;
-        segsweep_kernel<F, K><<<(hi - lo + WPB - 1) / WPB, SS_THREADS, 0, st>>>(
+        launch_k(segsweep_kernel<F, K>, (hi - lo + WPB - 1) / WPB, SS_THREADS, 0, st, 
             f, p.ranges, lo, hi, p.bits, p.nz_ids, p.empties, p.ss_splits, p.head, p.tail, p.counters, skip);
         ++g_launches;
         return;
     }
     if constexpr (K <= 2) {
         if (p.wide) {
-            segreduce_kernel<F, K, sr_items_wide<K>()><<<hi - lo, SR_THREADS, 0, st>>>(
+            launch_k(segreduce_kernel<F, K, sr_items_wide<K>()>, hi - lo, SR_THREADS, 0, st, 
                 f, p.tiles, lo, p.splits, p.head, p.tail, p.counters, skip);
             ++g_launches;
             return;
         }
     }
-    segreduce_kernel<F, K><<<hi - lo, SR_THREADS, 0, st>>>(f, p.tiles, lo, p.splits, p.head, p.tail,
+    launch_k(segreduce_kernel<F, K>, hi - lo, SR_THREADS, 0, st, f, p.tiles, lo, p.splits, p.head, p.tail,
                                                            p.counters, skip);
     ++g_launches;
 }
@@ -669,13 +695,13 @@ void schwarz_apply(within_preconditioner& P, SchwarzUser& U, const T* r, T* z, c
         else launch_sr<FF, K>(FF{P.p_fwd, S}, kp.fwd, kp.fwd.range_lo[r], kp.fwd.range_hi[r], skip, st);
     }
     if (fused) {
-        rounds_fused_kernel<FF, K><<<1, RF_THREADS, 0, st>>>(FF{P.p_fwd, S}, kp.fwd_rows, kp.fuse_lo, kp.fuse_hi, 0,
+        launch_k(rounds_fused_kernel<FF, K>, 1, RF_THREADS, 0, st, FF{P.p_fwd, S}, kp.fwd_rows, kp.fuse_lo, kp.fuse_hi, 0,
                                                               skip);
         ++g_launches;
     }
     if (P.has_core) launch_sr<CoF, K>(CoF{P.p_core, S}, kp.core, 0, kp.core.n_tiles, skip, st);
     if (fused) {
-        rounds_fused_kernel<BF, K><<<1, RF_THREADS, 0, st>>>(BF{P.p_bwd, S}, kp.bwd_rows, kp.fuse_lo, kp.fuse_hi, 1,
+        launch_k(rounds_fused_kernel<BF, K>, 1, RF_THREADS, 0, st, BF{P.p_bwd, S}, kp.bwd_rows, kp.fuse_lo, kp.fuse_hi, 1,
                                                               skip);
         ++g_launches;
     }
@@ -901,7 +927,7 @@ bool launch_tgather(within_solver& s, const double* x, const double* yint, doubl
             done.emplace_back(dev, f);
         }
     }
-    f<<<TG_GRID, RW_THREADS, sm, st>>>(s.op, x, yint, out, skip, err);
+    launch_k(f, TG_GRID, RW_THREADS, sm, st, s.op, x, yint, out, skip, err);
     ++g_launches;
     return true;
 }
@@ -1167,24 +1193,24 @@ void launch_rowsweep(within_solver& s, within_solver::RowSweepK& rk, const OpPar
             if (f) {
                 rp.hist_private = 1;
                 int* e = err ? err : (ctl ? &ctl->err : s.sweep_err);
-                f<<<rk.grid, RW_THREADS, rk.ts_smem, st>>>(op, rp, rk.ts_slots, v, u, cur, ctl, e);
+                launch_k(f, rk.grid, RW_THREADS, rk.ts_smem, st, op, rp, rk.ts_slots, v, u, cur, ctl, e);
                 staged = true;
             }
         }
     }
     if (!staged) {
         if (rk.simple)
-            k_rowsweep<K, MODE, T, true><<<rk.grid, RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
+            launch_k(k_rowsweep<K, MODE, T, true>, rk.grid, RW_THREADS, smem, st, op, rp, v, u, cur, ctl, skip, store,
                                                                             rhs, sq_out, sq_stride);
         else
-            k_rowsweep<K, MODE, T, false><<<rk.grid, RW_THREADS, smem, st>>>(op, rp, v, u, cur, ctl, skip, store,
+            launch_k(k_rowsweep<K, MODE, T, false>, rk.grid, RW_THREADS, smem, st, op, rp, v, u, cur, ctl, skip, store,
                                                                              rhs, sq_out, sq_stride);
     }
     ++g_launches;
     if (rp.n_fix) {   // the runs crossing range boundaries, after every range has written its partials
         const unsigned fb = (rp.n_fix + 255) / 256;
-        if (rk.simple) k_rw_fix<K, MODE, T, true><<<fb, 256, 0, st>>>(op, rp, ctl, skip);
-        else k_rw_fix<K, MODE, T, false><<<fb, 256, 0, st>>>(op, rp, ctl, skip);
+        if (rk.simple) launch_k(k_rw_fix<K, MODE, T, true>, fb, 256, 0, st, op, rp, ctl, skip);
+        else launch_k(k_rw_fix<K, MODE, T, false>, fb, 256, 0, st, op, rp, ctl, skip);
         ++g_launches;
     }
 }
@@ -1262,13 +1288,13 @@ template <int K, class T = double>
 void precond_apply(within_solver& s, Ctl* ctl, const T* p, T* v, const int* skip, cudaStream_t st) {
     const uint32_t nd = (uint32_t)s.n_dofs;
     if (!s.precond) {
-        k_diag_apply<K, T><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, nullptr, p, v, skip ? ctl : nullptr);
+        launch_k(k_diag_apply<K, T>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, nullptr, p, v, skip ? ctl : nullptr);
         ++g_launches;
     } else if (s.precond->kind == 2) {
         const T* d;
         if constexpr (sizeof(T) == 8) d = s.precond->inv_diag;
         else d = s.precond->inv_diag_f;
-        k_diag_apply<K, T><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, d, p, v, skip ? ctl : nullptr);
+        launch_k(k_diag_apply<K, T>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, d, p, v, skip ? ctl : nullptr);
         ++g_launches;
     } else {
         schwarz_apply<K, T>(*s.precond, s.schwarz, p, v, skip, st);
@@ -1286,23 +1312,23 @@ void iteration(within_solver& s, within_solver::Work& w, int par, cudaStream_t s
         auto& rk = s.rsw[kidx(K)];
         launch_rowsweep<K, 1, double>(s, rk, s.op, rk.atu, w.v, w.u, cur, w.ctl, nullptr, 0, st);
         rowsweep_rest<K, double>(s, rk, w.u, rk.atu, skip, st);
-        k_ptilde<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, rk.atu, w.p, cur, w.ctl);
+        launch_k(k_ptilde<K>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, rk.atu, w.p, cur, w.ctl);
         ++g_launches;
     } else {
-        k_gather_update<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, w.v, w.u, cur, w.ctl, w.partials, w.counter);
+        launch_k(k_gather_update<K>, RED_GRID, RED_THREADS, 0, st, s.op, w.v, w.u, cur, w.ctl, w.partials, w.counter);
         ++g_launches;
         scatter<K, 1>(s, w.u, w.p, cur, skip, st);
     }
     precond_apply<K>(s, w.ctl, w.p, w.v, skip, st);
     for (int j = 0; j < w.ring.cap; ++j) {   // M-MGS against the stored window (bidiag.rs:489-512)
-        k_reorth_dot<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, j, w.ring, w.v, cur, w.ctl, w.coef, w.partials,
+        launch_k(k_reorth_dot<K>, RED_GRID, RED_THREADS, 0, st, nd, j, w.ring, w.v, cur, w.ctl, w.coef, w.partials,
                                                           w.counter);
-        k_reorth_axpy<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, j, w.ring, w.v, w.p, cur, w.ctl, w.coef);
+        launch_k(k_reorth_axpy<K>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, j, w.ring, w.v, w.p, cur, w.ctl, w.coef);
         g_launches += 2;
     }
-    k_alpha_step<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, cur, nxt, w.ctl, w.partials, w.counter);
+    launch_k(k_alpha_step<K>, RED_GRID, RED_THREADS, 0, st, nd, w.v, w.p, cur, nxt, w.ctl, w.partials, w.counter);
     ++g_launches;
-    k_solution_update<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, nxt, w.ctl, w.ring,
+    launch_k(k_solution_update<K>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, w.v, w.h, w.hb, w.x, nxt, w.ctl, w.ring,
                                                                       w.p);
     ++g_launches;
     (void)n;
@@ -1370,11 +1396,11 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
     const uint32_t n = (uint32_t)s.n_obs, nd = (uint32_t)s.n_dofs;
     CK(cudaMemsetAsync(w.nonfinite, 0, sizeof(int), st));
     CK(cudaMemsetAsync(w.ctl, 0, sizeof(Ctl), st));
-    k_load_rhs<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, k_used, Y, s.perm, s.op.sqrt_w, w.yint, w.b,
+    launch_k(k_load_rhs<K>, RED_GRID, RED_THREADS, 0, st, n, k_used, Y, s.perm, s.op.sqrt_w, w.yint, w.b,
                                                     w.partials, w.counter, w.bmax, w.nonfinite);
     if (ext.x0) {   // warm start: x0 into the interleaved layout (finite check)
         if (!w.x0) w.x0 = s.arena.alloc<double>(s.n_dofs * K);
-        k_load_x0<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, k_used, ext.x0, w.x0, w.nonfinite);
+        launch_k(k_load_x0<K>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, k_used, ext.x0, w.x0, w.nonfinite);
         ++g_launches;
     }
     int nonfinite = 0;
@@ -1384,17 +1410,17 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
         throw WError(ERR_INVALID, ext.x0 ? "response and warm start must be finite (a non-finite value was found)"
                                          : "response must be finite (a non-finite value was found)");
     const double t_solve0 = now_s();
-    k_norm_b<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
+    launch_k(k_norm_b<K>, RED_GRID, RED_THREADS, 0, st, n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
                                                   w.ctl, w.partials, w.counter, 0, (int)ext.stale_window,
                                                   ext.stale_threshold);
     if (ext.x0) {   // b <- b - A x0, tolerances kept relative to the original ||b||
-        k_warm_rhs<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, w.x0, w.b, w.partials, w.counter, w.bmax);
-        k_norm_b<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
+        launch_k(k_warm_rhs<K>, RED_GRID, RED_THREADS, 0, st, s.op, w.x0, w.b, w.partials, w.counter, w.bmax);
+        launch_k(k_norm_b<K>, RED_GRID, RED_THREADS, 0, st, n, w.b, w.bmax, w.st, tol, (long long)maxiter, k_used,
                                                       w.ctl, w.partials, w.counter, 1, (int)ext.stale_window,
                                                       ext.stale_threshold);
         g_launches += 2;
     }
-    k_scale_u<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, w.b, w.u, w.st);
+    launch_k(k_scale_u<K>, grid_for(n, 256, 148 * 16), 256, 0, st, n, w.b, w.u, w.st);
     if (s.path[kidx(K)] == 2) {   // p~ = A^T u through the row sweep (adjoint mode) and its rest
         auto& rk = s.rsw[kidx(K)];
         CK(cudaMemsetAsync(w.p, 0, (size_t)nd * K * sizeof(double), st));   // levels no row reaches stay 0
@@ -1405,9 +1431,9 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
         scatter<K, 0>(s, w.u, w.p, w.st, nullptr, st);
     }
     precond_apply<K>(s, w.ctl, w.p, w.v, nullptr, st);
-    k_alpha_init<K><<<RED_GRID, RED_THREADS, 0, st>>>(nd, w.v, w.p, w.st, w.st + 8, w.ctl, w.partials,
+    launch_k(k_alpha_init<K>, RED_GRID, RED_THREADS, 0, st, nd, w.v, w.p, w.st, w.st + 8, w.ctl, w.partials,
                                                       w.counter);
-    k_init_vectors<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, w.v, w.h, w.hb, w.x, w.st, w.ring, w.p);
+    launch_k(k_init_vectors<K>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, w.v, w.h, w.hb, w.x, w.st, w.ring, w.p);
     g_launches += 6;
     Ctl ctl{};
     if (build_loop_graph<K>(s, w)) {
@@ -1457,19 +1483,19 @@ void run_lsmr(within_solver& s, within_solver::Work& w, const double* Y, uint32_
     const double t_solve1 = now_s();
     // results
     if (ext.x0) {
-        k_add_x0<K><<<grid_for((uint64_t)nd * K, 256, 148 * 8), 256, 0, st>>>(nd, w.x, w.x0);
+        launch_k(k_add_x0<K>, grid_for((uint64_t)nd * K, 256, 148 * 8), 256, 0, st, nd, w.x, w.x0);
         ++g_launches;
     }
     if (K != 1 || !launch_tgather(s, w.x, w.yint, w.dm, true, nullptr, s.sweep_err, st)) {
-        k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, w.x, w.yint, w.dm);
+        launch_k(k_demean<K>, grid_for(n, 256, 148 * 16), 256, 0, st, s.op, w.x, w.yint, w.dm);
         ++g_launches;
     }
     if (D_out) {
-        k_store_obs<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, k_used, w.dm, s.perm, D_out);
+        launch_k(k_store_obs<K>, grid_for(n, 256, 148 * 16), 256, 0, st, n, k_used, w.dm, s.perm, D_out);
         ++g_launches;
     }
     if (X_out) {
-        k_store_dofs<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, k_used, w.x, X_out);
+        launch_k(k_store_dofs<K>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, k_used, w.x, X_out);
         ++g_launches;
     }
     ColState fin[8];
@@ -1573,16 +1599,16 @@ void cg_iteration(within_solver& s, within_solver::Work& w, within_solver::Mixed
                                      st);
         rowsweep_rest<K, float>(s, rk, m.t, m.q, skip, st);
     } else {
-        k_apply<K, float><<<grid_for(s.n_obs, 256 * 4, 148 * 8), 256, 0, st>>>(s.op_f, m.p, m.t, skip);
+        launch_k(k_apply<K, float>, grid_for(s.n_obs, 256 * 4, 148 * 8), 256, 0, st, s.op_f, m.p, m.t, skip);
         ++g_launches;
         scatter<K, 0, float>(s, m.t, m.q, nullptr, skip, st);
     }
-    k_cg_alpha<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.p, m.q, m.st, m.ctl, w.partials, w.counter);
-    k_cg_update<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.p, m.q, m.d, m.res, m.st, m.ctl);
+    launch_k(k_cg_alpha<K, float>, RED_GRID, RED_THREADS, 0, st, nd, m.p, m.q, m.st, m.ctl, w.partials, w.counter);
+    launch_k(k_cg_update<K, float>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, m.p, m.q, m.d, m.res, m.st, m.ctl);
     g_launches += 2;
     precond_apply<K, float>(s, m.ctl, m.res, m.z, skip, st);
-    k_cg_beta<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.st, m.ctl, w.partials, w.counter);
-    k_cg_dir<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.z, m.p, m.st, m.ctl);
+    launch_k(k_cg_beta<K, float>, RED_GRID, RED_THREADS, 0, st, nd, m.res, m.z, m.st, m.ctl, w.partials, w.counter);
+    launch_k(k_cg_dir<K, float>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, m.z, m.p, m.st, m.ctl);
     g_launches += 2;
 }
 
@@ -1629,13 +1655,13 @@ void mixed_pre(within_solver& s, within_solver::Work& w, within_solver::MixedWor
                                       (int)(sizeof(CgCol) / sizeof(double)));
         rowsweep_rest<K, double>(s, rk, m.r64, m.g64, nullptr, st);
     } else {
-        k_resid64<K><<<RED_GRID, RED_THREADS, 0, st>>>(s.op, m.x64, w.b, m.r64, m.st, w.partials, w.counter);
+        launch_k(k_resid64<K>, RED_GRID, RED_THREADS, 0, st, s.op, m.x64, w.b, m.r64, m.st, w.partials, w.counter);
         ++g_launches;
         scatter<K, 0>(s, m.r64, m.g64, nullptr, nullptr, st);
     }
-    k_cg_start<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.g64, m.res, m.d);
+    launch_k(k_cg_start<K, float>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, m.g64, m.res, m.d);
     precond_apply<K, float>(s, m.ctl, m.res, m.z, nullptr, st);
-    k_cg_init<K, float><<<RED_GRID, RED_THREADS, 0, st>>>(nd, m.res, m.z, m.p, m.st, m.ctl, first, w.partials,
+    launch_k(k_cg_init<K, float>, RED_GRID, RED_THREADS, 0, st, nd, m.res, m.z, m.p, m.st, m.ctl, first, w.partials,
                                                            w.counter, use_h, h_in);
     g_launches += 2;
 }
@@ -1688,7 +1714,7 @@ bool build_mixed_graph(within_solver& s, within_solver::Work& w, within_solver::
         CK(cudaStreamUpdateCaptureDependencies(cs, &n_in, 1, cudaStreamSetCaptureDependencies));
         m.pre_launches = g_launches - l0;
         const uint64_t l1 = g_launches;
-        k_add_delta<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, cs>>>(nd, m.d, m.x64);
+        launch_k(k_add_delta<K, float>, grid_for(nd, 256, 148 * 8), 256, 0, cs, nd, m.d, m.x64);
         k_outer_cond<<<1, 1, 0, cs>>>(m.st, m.ctl, h_out);
         m.post_launches = g_launches - l1 + 2;
         CK(cudaStreamEndCapture(cs, &body));
@@ -1720,7 +1746,7 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
     auto& m = ensure_mixed(s, K);
     const uint32_t n = (uint32_t)s.n_obs, nd = (uint32_t)s.n_dofs;
     CK(cudaMemsetAsync(w.nonfinite, 0, sizeof(int), st));
-    k_load_rhs<K><<<RED_GRID, RED_THREADS, 0, st>>>(n, k_used, Y, s.perm, s.op.sqrt_w, w.yint, w.b, w.partials,
+    launch_k(k_load_rhs<K>, RED_GRID, RED_THREADS, 0, st, n, k_used, Y, s.perm, s.op.sqrt_w, w.yint, w.b, w.partials,
                                                     w.counter, w.bmax, w.nonfinite);
     ++g_launches;
     int nonfinite = 0;
@@ -1765,7 +1791,7 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
         } else {
             CK(cudaGraphLaunch(m.loop_graph, st));
         }
-        k_add_delta<K, float><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, m.d, m.x64);
+        launch_k(k_add_delta<K, float>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, m.d, m.x64);
         ++g_launches;
         CK(cudaMemcpyAsync(&ctl, m.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1778,15 +1804,15 @@ void run_mixed(within_solver& s, const double* Y, uint32_t k_used, double tol, u
         throw WError(ERR_INDEFINITE, "mixed solve: preconditioner not positive definite (<g, M g> < 0)");
     const double t_solve1 = now_s();
     if (K != 1 || !launch_tgather(s, m.x64, w.yint, w.dm, true, nullptr, s.sweep_err, st)) {
-        k_demean<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(s.op, m.x64, w.yint, w.dm);
+        launch_k(k_demean<K>, grid_for(n, 256, 148 * 16), 256, 0, st, s.op, m.x64, w.yint, w.dm);
         ++g_launches;
     }
     if (D_out) {
-        k_store_obs<K><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, k_used, w.dm, s.perm, D_out);
+        launch_k(k_store_obs<K>, grid_for(n, 256, 148 * 16), 256, 0, st, n, k_used, w.dm, s.perm, D_out);
         ++g_launches;
     }
     if (X_out) {
-        k_store_dofs<K><<<grid_for(nd, 256, 148 * 8), 256, 0, st>>>(nd, k_used, m.x64, X_out);
+        launch_k(k_store_dofs<K>, grid_for(nd, 256, 148 * 8), 256, 0, st, nd, k_used, m.x64, X_out);
         ++g_launches;
     }
     int werr = 0;
@@ -2608,7 +2634,7 @@ int within_solver_operator_apply(within_solver* s, const double* x_dev, double* 
         set_device(s->device);
         cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
         if (!launch_tgather(*s, x_dev, nullptr, y_dev, false, nullptr, s->sweep_err, st)) {
-            k_apply<1><<<grid_for(s->n_obs, 256, 148 * 16), 256, 0, st>>>(s->op, x_dev, y_dev);
+            launch_k(k_apply<1>, grid_for(s->n_obs, 256, 148 * 16), 256, 0, st, s->op, x_dev, y_dev, (const int*)nullptr);
             ++g_launches;
         }
         CK(cudaGetLastError());
@@ -2840,7 +2866,7 @@ int within_preconditioner_apply(const within_preconditioner* pc, const double* x
         set_device(p->device);
         cudaStream_t st = stream ? (cudaStream_t)stream : nullptr;
         if (p->kind == 2) {
-            k_diag_apply<1><<<grid_for(p->n, 256, 148 * 8), 256, 0, st>>>(p->n, p->inv_diag, x_dev, y_dev, nullptr);
+            launch_k(k_diag_apply<1>, grid_for(p->n, 256, 148 * 8), 256, 0, st, p->n, p->inv_diag, x_dev, y_dev, nullptr);
             ++g_launches;
         } else {
             std::lock_guard<std::mutex> g(p->mu);
@@ -2861,7 +2887,7 @@ int within_adjoint_rhs(uint64_t n, uint64_t k, const double* v_dev, const double
         if (n == 0 || k == 0) return;
         if (!v_dev || !a_dev) throw WError(ERR_INVALID, "adjoint rhs: null buffer");
         cudaStream_t st = (cudaStream_t)stream;
-        k_adjoint_rhs<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, (uint32_t)k, v_dev, w_dev, a_dev);
+        launch_k(k_adjoint_rhs, grid_for(n, 256, 148 * 16), 256, 0, st, n, (uint32_t)k, v_dev, w_dev, a_dev);
         ++g_launches;
         CK(cudaGetLastError());
     });
@@ -2874,7 +2900,7 @@ int within_demean_vjp(uint64_t n, uint64_t k, const double* r_dev, const double*
         if (!s_dev || (grad_w_dev && (!r_dev || !a_dev)))
             throw WError(ERR_INVALID, "demean vjp: null buffer");
         cudaStream_t st = (cudaStream_t)stream;
-        k_demean_vjp<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(n, (uint32_t)k, r_dev, a_dev, s_dev, w_dev,
+        launch_k(k_demean_vjp, grid_for(n, 256, 148 * 16), 256, 0, st, n, (uint32_t)k, r_dev, a_dev, s_dev, w_dev,
                                                                   grad_z_dev, grad_w_dev);
         ++g_launches;
         CK(cudaGetLastError());

@@ -24,6 +24,7 @@
 // A term's codes are summed into A v in term order, as in k_rowsweep, so both
 // sweeps give the same u bit for bit.
 #pragma once
+#include "pdl.cuh"
 
 #include "bulk.cuh"
 #include "rowsweep.cuh"
@@ -92,6 +93,8 @@ template <int K, int MODE, int NQ, int NRUN, int NHIST, bool WTD>
 __global__ void __launch_bounds__(RW_THREADS, TS_BLOCKS_PER_SM)
 k_tsweep(OpParams p, RwParams rw, TsSlots sl, const double* __restrict__ v, double* __restrict__ u,
          ColState* cur, Ctl* ctl, int* err) {
+    pdl_wait();
+    pdl_launch_dependents();
     static_assert(NQ >= 1 && NQ <= TS_MAXQ && NRUN >= 1 && NRUN <= RW_MAX_RUN && NHIST <= RW_MAX_HIST &&
                       NRUN + NHIST <= NQ,
                   "staged sweep: unsupported term classes");
@@ -502,6 +505,8 @@ template <int NQ, bool WTD, bool DEMEAN>
 __global__ void __launch_bounds__(RW_THREADS, TG_BLOCKS_PER_SM)
 k_tgather(OpParams p, const double* __restrict__ x, const double* __restrict__ yint, double* __restrict__ out,
           const int* skip, int* err) {
+    pdl_wait();
+    pdl_launch_dependents();
     using RG = TgRing<NQ, WTD, DEMEAN>;
     constexpr int R = 4;
     extern __shared__ __align__(128) unsigned char tg_sm[];
