@@ -820,13 +820,17 @@ def kernel_timeline(args):
     """Per-kernel device durations of one solve of the bench workload, from
     CUPTI timestamps (torch.profiler), with the loop replayed as two-iteration
     graphs (WITHIN_GRAPH_LOOP=0) so that every iteration's launches are
-    recorded.  For each kernel: launches, mean and total device time; for
+    recorded, in plain stream order (WITHIN_PDL=0).  For each kernel: launches, mean and total device time; for
     each kernel family of the FP64 solve, its algorithmic bytes per
     iteration (kernel_byte_model), its device time per iteration and the
     achieved GB/s and fraction of the HBM peak."""
     import collections
     import re
     os.environ["WITHIN_GRAPH_LOOP"] = "0"
+    # plain stream order: with programmatic dependent launch a kernel starts
+    # early and waits in-kernel, so its recorded span would include its
+    # predecessor's tail
+    os.environ["WITHIN_PDL"] = "0"
     import torch
     from torch.profiler import ProfilerActivity, profile
     import within_b200 as W

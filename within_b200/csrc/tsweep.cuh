@@ -369,11 +369,16 @@ k_tsweep(OpParams p, RwParams rw, TsSlots sl, const double* __restrict__ v, doub
             }
             bool in_range = exf || started[jr];
             // heads before this lane within the chunk (ordinals of the runs of a non-direct term)
-            uint32_t ord = 0;
+            // (the chunk's head count only matters to a term summed by run ordinal)
+            uint32_t ord = 0, chunk_heads = 0;
             if (!RR.direct) {
                 int before = 0;
 #pragma unroll
-                for (int r = 0; r < R; ++r) before += __popc(__ballot_sync(FULL, hd[r]) & lt);
+                for (int r = 0; r < R; ++r) {
+                    const unsigned bl = __ballot_sync(FULL, hd[r]);
+                    before += __popc(bl & lt);
+                    chunk_heads += (uint32_t)__popc(bl);
+                }
                 ord = __ldg(RR.range_base + g) + heads[jr] + (uint32_t)before;   // ordinal of the next head
             }
             // a head ends the run before it: a complete run (its head lies in this
@@ -412,10 +417,7 @@ k_tsweep(OpParams p, RwParams rw, TsSlots sl, const double* __restrict__ v, doub
                 carry[jr][k] = chunk_has_head ? incl : carry[jr][k] + incl;
             }
             started[jr] = started[jr] || chunk_has_head;
-            int tot = lane_heads;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(FULL, tot, o);
-            heads[jr] += (uint32_t)tot;
+            heads[jr] += chunk_heads;
             prevc[jr] = __shfl_sync(FULL, c[R - 1], 31);
         }
     }
