@@ -145,3 +145,23 @@ def test_demean_unweighted_and_vector_shapes(wb):
         wb.demean(zt, cats, weights=torch.zeros(n, dtype=torch.float64, device="cuda"))
     with pytest.raises(TypeError):
         wb.demean(zt.float(), cats)
+
+
+def test_demean_rejects_a_solver_built_with_other_weights(wb):
+    """The forward solve uses the given solver's weights and the weight
+    gradient the tensor passed to demean, so a mismatch must raise."""
+    import torch
+    rng = np.random.default_rng(5)
+    n = 4000
+    cats = np.asfortranarray(np.column_stack([rng.integers(0, 40, n), rng.integers(0, 25, n)]).astype(np.uint32))
+    w = rng.lognormal(0.0, 0.5, n)
+    zt = torch.tensor(rng.standard_normal(n), device="cuda", requires_grad=True)
+    wt = torch.tensor(w, device="cuda", requires_grad=True)
+    ok = wb.Solver(cats, weights=w)
+    wb.demean(zt, cats, weights=wt, solver=ok)   # the same weights: accepted
+    with pytest.raises(ValueError):
+        wb.demean(zt, cats, weights=wt, solver=wb.Solver(cats, weights=w * 1.5))
+    with pytest.raises(ValueError):
+        wb.demean(zt, cats, weights=wt, solver=wb.Solver(cats))
+    with pytest.raises(ValueError):
+        wb.demean(zt, cats, solver=ok)

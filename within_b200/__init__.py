@@ -471,6 +471,9 @@ class Solver:
         w = None if weights is None else _as_f64_1d("weights", weights)
         if w is not None and w.shape[0] != d.n_obs:
             raise ValueError(f"weights has length {w.shape[0]}, expected {d.n_obs}")
+        # fingerprint of the weights (sum and sum of squares), which demean()
+        # checks a caller's weights tensor against when given this solver
+        self._weights_fp = None if w is None else (float(np.sum(w)), float(np.sum(w * w)))
         prebuilt = preconditioner._h if isinstance(preconditioner, Preconditioner) else None
         cfg = None if prebuilt is not None else _precond_config(preconditioner)
         tn = _tuning_struct(tuning, design, w)

@@ -105,8 +105,11 @@ def demean(z, design, weights=None, options=None, preconditioner=None, solver=No
     """Differentiable ``z - D x*`` for a CUDA float64 tensor ``z`` of shape (n,)
     or (n, k), with gradients with respect to ``z`` and ``weights`` (a CUDA
     float64 tensor of shape (n,), positive).  ``solver`` may be a ``Solver``
-    already built for ``design`` and these weights; otherwise one is built
-    (the preconditioner depends on the weights)."""
+    already built for ``design`` and these weights (the forward solve uses the
+    solver's weights, the weight gradient the tensor passed here, so the two
+    must agree: a solver built with other weights, or with none when weights
+    are passed, raises ValueError); otherwise one is built (the
+    preconditioner depends on the weights)."""
     from . import Solver
     _check_f64_cuda("z", z)
     if weights is not None:
@@ -121,4 +124,13 @@ def demean(z, design, weights=None, options=None, preconditioner=None, solver=No
                         device=-1 if z.device.index is None else z.device.index)
     if solver.n_obs != z.shape[0]:
         raise ValueError(f"z has {z.shape[0]} rows but the solver has {solver.n_obs} observations")
+    fp = getattr(solver, "_weights_fp", None)
+    if (weights is None) != (fp is None):
+        raise ValueError("the solver was built " + ("with" if fp is not None else "without") +
+                         " weights, but demean was called " + ("without" if weights is None else "with") + " them")
+    if weights is not None:
+        got = (float(weights.sum()), float((weights * weights).sum()))
+        for a, b in zip(got, fp):
+            if abs(a - b) > 1e-10 * max(abs(a), abs(b), 1e-300):
+                raise ValueError("the solver was built with other weights than the weights passed to demean")
     return DemeanFunction.get().apply(z, weights, solver, options)
