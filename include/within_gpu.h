@@ -152,8 +152,8 @@ typedef struct {
     uint32_t core_small;        /* graphs this small keep eliminating ... */
     uint32_t core_dense_late;   /* ... until this many vertices remain (then a dense core) */
     int32_t warp_ranges;        /* segmented reductions by warp ranges over a segment-start bitmap instead
-                                   of block tiles: 1 (default) C^T and the adjoint's combines, 2 every
-                                   tile plan, 0 none */
+                                   of block tiles: 1 (default) C^T and the adjoint's combines of
+                                   single-column solves, 2 every tile plan, 0 none */
     int32_t gpu_cross_tab;      /* the additive-Schwarz set-up's cross-tabs on the GPU (sort and segment;
                                    the same bits as on the host): 1 (default) for designs of at least
                                    2^18 observations, 2 always, 0 never */

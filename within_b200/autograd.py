@@ -129,7 +129,8 @@ def demean(z, design, weights=None, options=None, preconditioner=None, solver=No
         raise ValueError("the solver was built " + ("with" if fp is not None else "without") +
                          " weights, but demean was called " + ("without" if weights is None else "with") + " them")
     if weights is not None:
-        got = (float(weights.sum()), float((weights * weights).sum()))
+        wd = weights.detach()
+        got = (float(wd.sum()), float((wd * wd).sum()))
         for a, b in zip(got, fp):
             if abs(a - b) > 1e-10 * max(abs(a), abs(b), 1e-300):
                 raise ValueError("the solver was built with other weights than the weights passed to demean")

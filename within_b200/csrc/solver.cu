@@ -145,9 +145,11 @@ struct Tuning {
     bool fuse_rounds = true;     // the small tail of elimination rounds in one block
     bool segthread = true;       // one thread per segment where every segment is short
     // segmented reductions by warp ranges (segsweep.cuh) instead of block
-    // tiles: 1 = C^T and the adjoint's combines (rows of ~10-1000 positions,
-    // measured faster on the 10M-row panel), 2 = every tile plan (restrict,
-    // means, kept sums, rounds, ... measured slower there), 0 = none
+    // tiles: 1 = C^T and the adjoint's combines of single-column solves (rows
+    // of ~10-1000 positions, measured faster on the 10M-row panel; at four
+    // columns a lane holds one position and C^T was slower), 2 = every tile
+    // plan at every column count (restrict, means, kept sums, rounds, ...
+    // measured slower), 0 = none
     int warp_ranges = 1;
     // cross-tabs of the additive-Schwarz set-up on the GPU (xtab.cu): 1 for
     // designs of at least XTAB_MIN_OBS observations, 2 always, 0 never
@@ -241,6 +243,18 @@ bool pdl_on() {
         return e ? atoi(e) != 0 : true;
     }();
     return on;
+}
+
+// c_pdl_early on the current device (once per device; WITHIN_PDL_EARLY=1)
+void pdl_setup(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> g(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    const char* e = getenv("WITHIN_PDL_EARLY");
+    const int v = e ? atoi(e) : 0;
+    CK(cudaMemcpyToSymbol(c_pdl_early, &v, sizeof(int)));
+    done.push_back(dev);
 }
 
 template <class... KArgs, class... Args>
@@ -544,7 +558,7 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
         return d;
     };
     kp.restrict_ = one(H.loc_ptr, ss);
-    kp.ct = one(H.ct_ptr, U.tuning.warp_ranges >= 1);
+    kp.ct = one(H.ct_ptr, U.tuning.warp_ranges >= 2 || (U.tuning.warp_ranges == 1 && K == 1));
     kp.kept = one(H.kept_ptr, ss);
     kp.dense = one(H.dense_rows_ptr, ss);
     kp.c = one(H.c_ptr, ss);
@@ -1104,7 +1118,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
             pos += lp.back() - lp.front();
             segs += lp.size() - 1;
         }
-        if (s.schwarz.tuning.warp_ranges >= 1) {
+        if (s.schwarz.tuning.warp_ranges >= 2 || (s.schwarz.tuning.warp_ranges == 1 && K == 1)) {
             SSHostPlan sp;
             const uint32_t L = ss_range_len(pos, ss_target_warps(K));
             for (size_t i = 0; i < rk.rest_host.size(); ++i)
@@ -1934,6 +1948,7 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     s->sweep_err = s->arena.alloc<int>(1);
     s->schwarz.tuning = resolve_tuning(tuning);
+    pdl_setup(device);
     std::vector<EffectIn> effs;
     for (size_t e = 0; e < d->levels.size(); ++e) {
         EffectIn ef;
