@@ -16,7 +16,7 @@ LIB = os.path.join(LIB_DIR, "libwithin_gpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["solver.cu", "xtab.cu", "host_design.cpp", "host_schwarz.cpp"]
-HEADERS = ["host.hpp", "kernels.cuh", "segreduce.cuh", "segplan.hpp", "refine.cuh", "rowsweep.cuh",
+HEADERS = ["host.hpp", "host_pool.hpp", "kernels.cuh", "segreduce.cuh", "segplan.hpp", "refine.cuh", "rowsweep.cuh",
            "bulk.cuh", "tsweep.cuh", "segsweep.cuh", "pdl.cuh"]
 
 NVCC_FLAGS = [

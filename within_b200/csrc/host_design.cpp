@@ -6,6 +6,7 @@
 #include <numeric>
 
 #include "host.hpp"
+#include "host_pool.hpp"
 
 namespace wgpu {
 
@@ -86,14 +87,23 @@ HostDesign make_design(uint64_t n_obs, const std::vector<EffectIn>& effects) {
         if (!d.terms[dom].sorted) {
             d.obs_perm.resize(n_obs);
             stable_argsort_u32(d.codes[dom].data(), n_obs, d.terms[dom].n_levels, d.obs_perm.data());
+            // gathers by ranges of observations on the host pool
+            const size_t nch = n_obs >= ((uint64_t)1 << 20) ? 16 : 1, per = (n_obs + nch - 1) / nch;
+            const uint32_t* pm = d.obs_perm.data();
             std::vector<uint32_t> tmp(n_obs);
             for (auto& col : d.codes) {
-                for (uint64_t i = 0; i < n_obs; ++i) tmp[i] = col[d.obs_perm[i]];
+                par_for_each(nch, [&](size_t t) {
+                    const uint64_t i1 = std::min<uint64_t>(n_obs, (t + 1) * per);
+                    for (uint64_t i = t * per; i < i1; ++i) tmp[i] = col[pm[i]];
+                });
                 col.swap(tmp);
             }
             std::vector<double> tz(n_obs);
             for (auto& col : d.loads) {
-                for (uint64_t i = 0; i < n_obs; ++i) tz[i] = col[d.obs_perm[i]];
+                par_for_each(nch, [&](size_t t) {
+                    const uint64_t i1 = std::min<uint64_t>(n_obs, (t + 1) * per);
+                    for (uint64_t i = t * per; i < i1; ++i) tz[i] = col[pm[i]];
+                });
                 col.swap(tz);
             }
             for (size_t q = 0; q < d.terms.size(); ++q)

@@ -21,6 +21,7 @@
 //     per parallel step (level scheduling by construction).
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cfloat>
 #include <cmath>
 #include <exception>
@@ -29,9 +30,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <chrono>
+#include <mutex>
 #include <thread>
+#include <type_traits>
 
 #include "host.hpp"
+#include "host_pool.hpp"
 
 namespace wgpu {
 namespace {
@@ -62,38 +66,30 @@ struct BuildTrace {
     ~BuildTrace() { done(); }
 };
 
-// f(i) for i in [0, n) on up to 16 of the host's hardware threads (a build may
-// itself run on one of many threads building designs side by side;
-// WITHIN_HOST_THREADS sets the cap).  Every f(i) writes only its own outputs,
-// so the result does not depend on the schedule; the exception of the lowest
-// failing index is rethrown, as the sequential loop would have thrown it.
-template <class F>
-void par_for_each(size_t n, F&& f) {
-    size_t cap = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
-    if (const char* e = std::getenv("WITHIN_HOST_THREADS")) cap = std::max(1, std::atoi(e));
-    const size_t nt = std::min<size_t>(n, cap);
-    if (nt <= 1) {
-        for (size_t i = 0; i < n; ++i) f(i);
-        return;
+// WITHIN_TRACE=1: time spent in the named steps of a loop, summed over its
+// passes and printed as one line when the loop's owner goes out of scope
+struct StepTimes {
+    const char* what;
+    const char* const* names;
+    int n;
+    double t[8] = {};
+    double last = 0.0;
+    StepTimes(const char* w, const char* const* nm, int k) : what(w), names(nm), n(k) {
+        if (BuildTrace::on()) last = BuildTrace::now();
     }
-    std::vector<std::exception_ptr> err(n);
-    std::atomic<size_t> next{0};
-    auto work = [&]() {
-        for (size_t i; (i = next.fetch_add(1)) < n;) {
-            try {
-                f(i);
-            } catch (...) {
-                err[i] = std::current_exception();
-            }
-        }
-    };
-    std::vector<std::thread> th;
-    for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
-    work();
-    for (auto& t : th) t.join();
-    for (auto& e : err)
-        if (e) std::rethrow_exception(e);
-}
+    void mark(int i) {
+        if (!BuildTrace::on()) return;
+        const double x = BuildTrace::now();
+        t[i] += x - last;
+        last = x;
+    }
+    ~StepTimes() {
+        if (!BuildTrace::on()) return;
+        fprintf(stderr, "[within trace]       %s:", what);
+        for (int i = 0; i < n; ++i) fprintf(stderr, " %s %.3f ms", names[i], t[i] * 1e3);
+        fprintf(stderr, "\n");
+    }
+};
 
 constexpr uint32_t DENSE_MAX = 64;
 
@@ -108,6 +104,46 @@ Csr transpose(const Csr& a) {
     Csr t;
     t.nr = a.nc;
     t.nc = a.nr;
+    if (a.nnz() >= (1u << 18) && a.nr >= 64) {
+        // chunks of rows count their entries per column and scatter side by
+        // side; every column receives its entries in ascending row order
+        const size_t nch = 16;
+        std::vector<uint32_t> rb(nch + 1, a.nr);   // chunk t = rows [rb[t], rb[t+1])
+        {
+            const uint64_t goal = ((uint64_t)a.nnz() + nch - 1) / nch;
+            size_t t = 1;
+            rb[0] = 0;
+            for (uint32_t r = 0; r < a.nr && t < nch; ++r)
+                if ((uint64_t)a.ptr[r + 1] >= goal * t) rb[t++] = r + 1;
+        }
+        std::vector<std::vector<uint32_t>> cnt(nch);
+        par_for_each(nch, [&](size_t c) {
+            cnt[c].assign(a.nc, 0);
+            for (uint32_t k = a.ptr[rb[c]]; k < a.ptr[rb[c + 1]]; ++k) ++cnt[c][a.col[k]];
+        });
+        t.ptr.assign(a.nc + 1, 0);
+        for (uint32_t j = 0; j < a.nc; ++j) {
+            uint32_t o = t.ptr[j];
+            for (size_t c = 0; c < nch; ++c) {
+                const uint32_t n = cnt[c][j];
+                cnt[c][j] = o;
+                o += n;
+            }
+            t.ptr[j + 1] = o;
+        }
+        t.col.resize(a.nnz());
+        t.val.resize(a.nnz());
+        par_for_each(nch, [&](size_t c) {
+            std::vector<uint32_t>& cur = cnt[c];
+            for (uint32_t r = rb[c]; r < rb[c + 1]; ++r)
+                for (uint32_t k = a.ptr[r]; k < a.ptr[r + 1]; ++k) {
+                    const uint32_t p = cur[a.col[k]]++;
+                    t.col[p] = r;
+                    t.val[p] = a.val[k];
+                }
+        });
+        return t;
+    }
     t.ptr.assign(a.nc + 1, 0);
     for (uint32_t c : a.col) ++t.ptr[c + 1];
     for (uint32_t i = 0; i < a.nc; ++i) t.ptr[i + 1] += t.ptr[i];
@@ -164,11 +200,19 @@ double budget(double ulps, size_t n, double total) {
 
 std::vector<double> sums(const Bip& m, bool mag) {
     std::vector<double> s(m.nl());
-    for (uint32_t i = 0; i < m.nl(); ++i) {
-        double a = 0;
-        m.nb(i, [&](uint32_t, double v) { a += mag ? std::fabs(v) : v; });
-        s[i] = a;
-    }
+    auto range = [&](uint32_t i0, uint32_t i1) {
+        for (uint32_t i = i0; i < i1; ++i) {
+            double a = 0;
+            m.nb(i, [&](uint32_t, double v) { a += mag ? std::fabs(v) : v; });
+            s[i] = a;
+        }
+    };
+    const uint32_t B = 16384;
+    if (m.c.nnz() >= (1u << 18))
+        par_for_each(((size_t)m.nl() + B - 1) / B, [&](size_t b) {
+            range((uint32_t)(b * B), (uint32_t)std::min<size_t>(m.nl(), (b + 1) * (size_t)B));
+        });
+    else range(0, m.nl());
     return s;
 }
 
@@ -324,7 +368,14 @@ Lap exact_reduced(const Comp& c, const std::vector<double>& inv_e) {
         std::vector<uint32_t> col;
         std::vector<double> val;
     };
-    constexpr uint32_t RBLK = 4;
+    // the work of row i is the sum of the C-row lengths of its neighbours;
+    // over all rows that is the sum of the squared C-row lengths
+    uint64_t work_est = 0;
+    for (uint32_t k = 0; k < ne; ++k) {
+        const uint64_t len = c.m.c.ptr[k + 1] - c.m.c.ptr[k];
+        work_est += len * len;
+    }
+    const uint32_t RBLK = nk >= 1024 ? 4 : 1;
     const uint32_t nblk = (nk + RBLK - 1) / RBLK;
     std::vector<std::vector<RowOut>> rows(nblk);
     auto row_block = [&](size_t bi) {
@@ -371,7 +422,7 @@ Lap exact_reduced(const Comp& c, const std::vector<double>& inv_e) {
         }
     };
     // worth threads only when the rows reach many eliminated neighbours
-    if (c.m.c.nnz() >= (1u << 20)) par_for_each(nblk, row_block);
+    if (c.m.c.nnz() >= (1u << 20) || work_est >= ((uint64_t)1 << 22)) par_for_each(nblk, row_block);
     else for (size_t bi = 0; bi < nblk; ++bi) row_block(bi);
     for (auto& blk : rows)
         for (RowOut& R : blk) {
@@ -408,8 +459,9 @@ struct Edge { uint32_t lo, hi; double w; };
 // Clique-tree sample of one star (GKS): neighbours ascending by weight, each
 // linked to a later one drawn in proportion to weight, weight w_i S_i / d.
 // `split` > 1 first splits every neighbour edge into that many equal copies.
+// `pre` is the caller's scratch for the weight prefix sums.
 void sample_star(std::vector<std::pair<uint32_t, double>>& e, uint32_t split, Rng& rng,
-                 std::vector<Edge>& out) {
+                 std::vector<Edge>& out, std::vector<double>& pre) {
     if (split > 1) {
         std::vector<std::pair<uint32_t, double>> s;
         s.reserve(e.size() * split);
@@ -422,14 +474,15 @@ void sample_star(std::vector<std::pair<uint32_t, double>>& e, uint32_t split, Rn
         return a.second != b.second ? a.second < b.second : a.first < b.first;
     });
     const size_t m = e.size();
-    std::vector<double> pre(m + 1, 0.0);
+    pre.resize(m + 1);
+    pre[0] = 0.0;
     for (size_t i = 0; i < m; ++i) pre[i + 1] = pre[i] + e[i].second;
     const double d = pre[m];
     for (size_t i = 0; i + 1 < m; ++i) {
         double S = d - pre[i + 1];
         if (!(S > 0.0)) continue;
         double tgt = pre[i + 1] + rng.unit() * S;
-        size_t j = (size_t)(std::upper_bound(pre.begin() + i + 2, pre.end(), tgt) - pre.begin()) - 1;
+        size_t j = (size_t)(std::upper_bound(pre.begin() + i + 2, pre.begin() + m + 1, tgt) - pre.begin()) - 1;
         j = std::min(std::max(j, i + 1), m - 1);
         if (e[i].first == e[j].first) continue;
         out.push_back({std::min(e[i].first, e[j].first), std::max(e[i].first, e[j].first),
@@ -437,82 +490,167 @@ void sample_star(std::vector<std::pair<uint32_t, double>>& e, uint32_t split, Rn
     }
 }
 
-Lap lap_from_edges(std::vector<Edge>& edges, uint32_t n) {
-    // (lo, hi, w) order: a stable counting sort by lo, then each lo group
-    // sorted by (hi, w) -- the order of one global sort on (lo, hi, w), so
-    // parallel edges are summed in ascending weight
-    std::vector<uint32_t> start(n + 1, 0);
-    for (const Edge& e : edges) ++start[e.lo + 1];
-    for (uint32_t i = 0; i < n; ++i) start[i + 1] += start[i];
-    std::vector<Edge> srt(edges.size());
+// Laplacian of a weighted edge list given as consecutive parts (the parts in
+// order are the list).  Parallel edges are summed in ascending weight: the
+// edges are bucketed by lo (per-chunk counts, so chunks of parts scatter on
+// host threads; within a bucket the edges keep list order), each bucket is
+// sorted by (hi, w) and its runs of equal hi summed in that order -- the order
+// of one global sort on (lo, hi, w).
+Lap lap_from_edges(std::vector<std::vector<Edge>>& parts, uint32_t n) {
+    static const char* const steps[] = {"bucket", "sort and merge", "rows"};
+    StepTimes st("edges to rows", steps, 3);
+    size_t cap = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (const char* e = std::getenv("WITHIN_HOST_THREADS")) cap = std::max(1, std::atoi(e));
+    size_t total = 0;
+    for (auto& p : parts) total += p.size();
+    // chunks: contiguous runs of parts with about total / nch edges each
+    const size_t nch = total >= ((size_t)1 << 16) ? std::max<size_t>(1, std::min(cap, parts.size())) : 1;
+    std::vector<size_t> ch_part{0};
     {
-        std::vector<uint32_t> pos(start.begin(), start.end() - 1);
-        for (const Edge& e : edges) srt[pos[e.lo]++] = e;
+        size_t acc = 0, goal = (total + nch - 1) / nch;
+        for (size_t p = 0; p < parts.size(); ++p) {
+            acc += parts[p].size();
+            if (acc >= goal * ch_part.size() && ch_part.size() < nch) ch_part.push_back(p + 1);
+        }
+        while (ch_part.size() <= nch) ch_part.push_back(parts.size());
     }
-    // each lo group sorts on its own (blocks of groups on host threads)
+    std::vector<std::vector<uint32_t>> cnt(nch);
+    par_for_each(nch, [&](size_t t) {
+        cnt[t].assign(n, 0);
+        for (size_t p = ch_part[t]; p < ch_part[t + 1]; ++p)
+            for (const Edge& e : parts[p]) ++cnt[t][e.lo];
+    });
+    std::vector<uint32_t> start(n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t s0 = start[i];
+        for (size_t t = 0; t < nch; ++t) {
+            const uint32_t c = cnt[t][i];
+            cnt[t][i] = s0;   // now: where chunk t's first edge of bucket i goes
+            s0 += c;
+        }
+        start[i + 1] = s0;
+    }
+    std::vector<Edge> srt(total);
+    par_for_each(nch, [&](size_t t) {
+        std::vector<uint32_t>& pos = cnt[t];
+        for (size_t p = ch_part[t]; p < ch_part[t + 1]; ++p) {
+            for (const Edge& e : parts[p]) srt[pos[e.lo]++] = e;
+            std::vector<Edge>().swap(parts[p]);
+        }
+        std::vector<uint32_t>().swap(pos);
+    });
+    st.mark(0);
+    // each bucket sorts and merges on its own (blocks of buckets on host threads)
+    std::vector<uint32_t> kept(n, 0);
     const uint32_t gblk = 256;
     par_for_each(((size_t)n + gblk - 1) / gblk, [&](size_t b) {
         const uint32_t i1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)gblk);
-        for (uint32_t i = (uint32_t)(b * gblk); i < i1; ++i)
-            std::sort(srt.begin() + start[i], srt.begin() + start[i + 1], [](const Edge& a, const Edge& b2) {
+        for (uint32_t i = (uint32_t)(b * gblk); i < i1; ++i) {
+            Edge* g0 = srt.data() + start[i];
+            Edge* g1 = srt.data() + start[i + 1];
+            std::sort(g0, g1, [](const Edge& a, const Edge& b2) {
                 if (a.hi != b2.hi) return a.hi < b2.hi;
                 return a.w < b2.w;
             });
+            Edge* w = g0;
+            for (Edge* e = g0; e < g1; ++e) {
+                if (w != g0 && (w - 1)->hi == e->hi) (w - 1)->w += e->w;
+                else *w++ = *e;
+            }
+            kept[i] = (uint32_t)(w - g0);
+        }
     });
-    std::vector<Edge> dd;
-    dd.reserve(srt.size());
-    for (auto& e : srt) {
-        if (!dd.empty() && dd.back().lo == e.lo && dd.back().hi == e.hi) dd.back().w += e.w;
-        else dd.push_back(e);
+    st.mark(1);
+    // rows in one flat array sorted by column without a sort: the merged
+    // edges are ordered by (lo, hi), so the edges reaching row i from below
+    // (hi == i) arrive in ascending lo and those leaving it upwards (lo == i,
+    // bucket i) in ascending hi; row i is [lower neighbours, i, upper
+    // neighbours], its diagonal the sum of the lower then the upper weights
+    // (the order one pass over the merged list adds them).  Lower entries are
+    // scattered by chunks of buckets (contiguous lo ranges, per-chunk counts),
+    // so every row receives them in ascending lo.
+    std::vector<uint32_t> bch{0};   // chunk t = buckets [bch[t], bch[t+1])
+    {
+        uint64_t merged = 0;
+        for (uint32_t g = 0; g < n; ++g) merged += kept[g];
+        const size_t nrc = merged >= ((uint64_t)1 << 16) ? std::max<size_t>(1, cap) : 1;
+        const uint64_t goal = (merged + nrc - 1) / nrc;
+        uint64_t acc = 0;
+        for (uint32_t g = 0; g < n; ++g) {
+            acc += kept[g];
+            if (acc >= goal * bch.size() && bch.size() < nrc) bch.push_back(g + 1);
+        }
+        while (bch.back() != n) bch.push_back(n);
     }
-    // rows in one flat array sorted by column without a sort: dd is ordered
-    // by (lo, hi), so the edges reaching row i from below (hi == i) arrive in
-    // ascending lo and those leaving it upwards (lo == i) in ascending hi;
-    // row i is [lower neighbours, i, upper neighbours]
+    const size_t nrc = bch.size() - 1;
+    std::vector<std::vector<uint32_t>> lowc(nrc);
+    par_for_each(nrc, [&](size_t t) {
+        lowc[t].assign(n, 0);
+        for (uint32_t g = bch[t]; g < bch[t + 1]; ++g)
+            for (uint32_t q = start[g]; q < start[g] + kept[g]; ++q) ++lowc[t][srt[q].hi];
+    });
     std::vector<uint32_t> rp(n + 1, 0), nlow(n, 0);
-    for (auto& e : dd) {
-        ++rp[e.lo + 1];
-        ++rp[e.hi + 1];
-        ++nlow[e.hi];
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t l = 0;
+        for (size_t t = 0; t < nrc; ++t) {
+            const uint32_t c = lowc[t][i];
+            lowc[t][i] = rp[i] + l;   // now: where chunk t's first lower entry of row i goes
+            l += c;
+        }
+        nlow[i] = l;
+        rp[i + 1] = rp[i] + l + 1 + kept[i];
     }
-    for (uint32_t i = 0; i < n; ++i) rp[i + 1] += rp[i] + 1;
     Lap L;
     L.n = n;
     L.col.resize(rp[n]);
     L.val.resize(rp[n]);
     L.ptr.assign(rp.begin(), rp.end());
-    std::vector<uint32_t> lo_fill(rp.begin(), rp.end() - 1), up_fill(n);
-    for (uint32_t i = 0; i < n; ++i) up_fill[i] = rp[i] + nlow[i] + 1;
-    std::vector<double> diag(n, 0.0);
-    for (auto& e : dd) {
-        const uint32_t a = up_fill[e.lo]++, b = lo_fill[e.hi]++;
-        L.col[a] = e.hi;
-        L.val[a] = -e.w;
-        L.col[b] = e.lo;
-        L.val[b] = -e.w;
-        diag[e.lo] += e.w;
-        diag[e.hi] += e.w;
-    }
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t q = rp[i] + nlow[i];
-        L.col[q] = i;
-        L.val[q] = diag[i];
-    }
+    par_for_each(nrc, [&](size_t t) {
+        std::vector<uint32_t>& pos = lowc[t];
+        for (uint32_t g = bch[t]; g < bch[t + 1]; ++g) {
+            uint32_t up = rp[g] + nlow[g] + 1;
+            for (uint32_t q = start[g]; q < start[g] + kept[g]; ++q) {
+                const Edge& e = srt[q];
+                const uint32_t b = pos[e.hi]++;
+                L.col[b] = e.lo;
+                L.val[b] = -e.w;
+                L.col[up] = e.hi;
+                L.val[up] = -e.w;
+                ++up;
+            }
+        }
+        std::vector<uint32_t>().swap(pos);
+    });
+    const uint32_t rblk = 4096;
+    par_for_each(((size_t)n + rblk - 1) / rblk, [&](size_t b) {
+        const uint32_t i1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)rblk);
+        for (uint32_t i = (uint32_t)(b * rblk); i < i1; ++i) {
+            const uint32_t q = rp[i] + nlow[i];
+            double d = 0.0;
+            for (uint32_t a = rp[i]; a < q; ++a) d += -L.val[a];
+            for (uint32_t a = q + 1; a < rp[i + 1]; ++a) d += -L.val[a];
+            L.col[q] = i;
+            L.val[q] = d;
+        }
+    });
+    st.mark(2);
     return L;
 }
 
 Lap sampled_reduced(const Comp& c, uint64_t seed, uint32_t split) {
     const uint32_t ne = c.m.nr(), nk = c.m.nc();
     // every eliminated vertex draws from its own seeded stream, so blocks of
-    // vertices sample on host threads and their edges concatenate in vertex
-    // order: the same edge list as one sequential pass
-    const uint32_t block = 16384;
+    // vertices sample on host threads; the blocks' edge lists, in vertex
+    // order, are the list of one sequential pass
+    const uint32_t block = 2048;
     const size_t nblk = ((size_t)ne + block - 1) / block;
-    std::vector<std::vector<Edge>> part(nblk);
+    std::vector<std::vector<Edge>> part(nblk + 1);
     par_for_each(nblk, [&](size_t b) {
         std::vector<std::pair<uint32_t, double>> ent;
+        std::vector<double> pre;
         std::vector<Edge>& out = part[b];
         const uint32_t k1 = (uint32_t)std::min<size_t>(ne, (b + 1) * (size_t)block);
+        out.reserve((size_t)(c.m.c.ptr[k1] - c.m.c.ptr[(uint32_t)(b * block)]));
         for (uint32_t k = (uint32_t)(b * block); k < k1; ++k) {
             ent.clear();
             for (uint32_t a = c.m.c.ptr[k]; a < c.m.c.ptr[k + 1]; ++a) ent.push_back({c.m.c.col[a], c.m.c.val[a]});
@@ -520,23 +658,13 @@ Lap sampled_reduced(const Comp& c, uint64_t seed, uint32_t split) {
             if (c.grounded && c.ground[k] > 0.0) ent.push_back({nk, c.ground[k]});
             if (ent.size() <= 1) continue;
             Rng r{mix64(seed * 0x100000001B3ull + k)};
-            sample_star(ent, split, r, out);
+            sample_star(ent, split, r, out, pre);
         }
     });
-    std::vector<Edge> edges;
-    {
-        size_t tot = 0;
-        for (auto& v : part) tot += v.size();
-        edges.reserve(tot + (c.grounded ? nk : 0));
-        for (auto& v : part) {
-            edges.insert(edges.end(), v.begin(), v.end());
-            std::vector<Edge>().swap(v);
-        }
-    }
     if (c.grounded)
         for (uint32_t i = 0; i < nk; ++i)
-            if (c.ground[ne + i] > 0.0) edges.push_back({i, nk, c.ground[ne + i]});
-    return lap_from_edges(edges, nk + (c.grounded ? 1 : 0));
+            if (c.ground[ne + i] > 0.0) part[nblk].push_back({i, nk, c.ground[ne + i]});
+    return lap_from_edges(part, nk + (c.grounded ? 1 : 0));
 }
 
 // ---- factors of a reduced Laplacian ----
@@ -638,21 +766,30 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
     const uint64_t seed = cfg.ac_seed;
     const uint32_t split = cfg.ac_split;
     const uint32_t n = m.n;
+    static const char* const steps[] = {"adjacency", "compact", "core", "select", "eliminate", "fill"};
+    StepTimes st("rounds", steps, 6);
     std::vector<std::vector<std::pair<uint32_t, double>>> adj(n);
-    for (uint32_t i = 0; i < n; ++i)
-        for (uint32_t k = m.ptr[i]; k < m.ptr[i + 1]; ++k)
-            if (m.col[k] != i && m.val[k] < 0.0) adj[i].push_back({m.col[k], -m.val[k]});
+    par_for_each(((size_t)n + 4095) / 4096, [&](size_t b) {
+        const uint32_t i1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)4096);
+        for (uint32_t i = (uint32_t)(b * 4096); i < i1; ++i) {
+            uint32_t c = 0;
+            for (uint32_t k = m.ptr[i]; k < m.ptr[i + 1]; ++k) c += m.col[k] != i && m.val[k] < 0.0;
+            adj[i].reserve(c);
+            for (uint32_t k = m.ptr[i]; k < m.ptr[i + 1]; ++k)
+                if (m.col[k] != i && m.val[k] < 0.0) adj[i].push_back({m.col[k], -m.val[k]});
+        }
+    });
     f.n = n;
     f.dense = false;
     f.round.assign(n, 0);
     f.dinv.assign(n, 0.0);
     f.colv.assign(n, {});
     std::vector<char> alive(n, 1);
+    std::vector<uint32_t> sorted_len(n, 0);   // see the compaction below
     std::vector<uint32_t> live(n);
     std::iota(live.begin(), live.end(), 0u);
     std::vector<uint64_t> key(n);
     std::vector<uint32_t> sel;
-    std::vector<Edge> fill;
     uint32_t r = 0;
     double last_frac = 1.0;
     bool dense_graph = false;   // see the stop rules below
@@ -661,49 +798,73 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
     // vertex samples from its own seeded stream, so these run over blocks of
     // vertices on host threads; selections and fill edges are joined in
     // vertex order, which gives the sequential loop's lists exactly.
-    constexpr size_t VBLK = 4096;
-    auto blocks = [](size_t m) { return (m + VBLK - 1) / VBLK; };
-    const bool threaded = n >= 4 * VBLK;
+    // A large graph runs in blocks of 4096 vertices, a smaller one (a
+    // reduced system of a few thousand levels, whose rounds fill it in) in
+    // blocks of about n / 64.  The block size only schedules work.
+    const bool threaded = n >= 1024;
+    const size_t VBLK = n >= 16384 ? 4096 : std::max<size_t>(32, ((size_t)n + 63) / 64);
+    auto blocks = [VBLK](size_t k) { return (k + VBLK - 1) / VBLK; };
     auto par = [&](size_t nb, auto&& fn) {
         if (threaded) par_for_each(nb, fn);
         else for (size_t b = 0; b < nb; ++b) fn(b);
     };
-    struct Scratch {
-        std::vector<double> acc;
-        std::vector<char> seen;
-        std::vector<uint32_t> order;
-    };
+    st.mark(0);
     while (!live.empty()) {
-        // compact adjacency: drop dead neighbours, merge parallel edges
+        // compact adjacency: drop dead neighbours, merge parallel edges.  A
+        // list is [sorted prefix: one entry per neighbour, ascending, from the
+        // last compaction | fill edges appended since]; the tail is sorted
+        // stably by neighbour and merged in, each neighbour's weight summed as
+        // prefix entry first, then its tail entries in append order (the
+        // order of one accumulation pass over the list).
         par(blocks(live.size()), [&](size_t b) {
-            Scratch sc;
-            sc.acc.assign(n, 0.0);
-            sc.seen.assign(n, 0);
+            std::vector<std::pair<uint32_t, double>> tail, merged;
             const size_t j1 = std::min(live.size(), (b + 1) * VBLK);
             for (size_t j = b * VBLK; j < j1; ++j) {
                 const uint32_t v = live[j];
                 auto& a = adj[v];
-                size_t w = 0;
-                sc.order.clear();
-                for (auto& e : a) {
-                    if (!alive[e.first] || e.first == v) continue;
-                    if (!sc.seen[e.first]) {
-                        sc.seen[e.first] = 1;
-                        sc.order.push_back(e.first);
+                const size_t s0 = sorted_len[v];
+                if (s0 == a.size()) {
+                    size_t w = 0;
+                    for (auto& e : a)
+                        if (alive[e.first] && e.first != v) a[w++] = e;
+                    a.resize(w);
+                } else {
+                    tail.clear();
+                    for (size_t q = s0; q < a.size(); ++q)
+                        if (alive[a[q].first] && a[q].first != v) tail.push_back(a[q]);
+                    std::stable_sort(tail.begin(), tail.end(),
+                                     [](const std::pair<uint32_t, double>& x, const std::pair<uint32_t, double>& y) {
+                                         return x.first < y.first;
+                                     });
+                    merged.clear();
+                    size_t p = 0, t = 0;
+                    while (p < s0 || t < tail.size()) {
+                        if (p < s0 && (!alive[a[p].first] || a[p].first == v)) {
+                            ++p;
+                            continue;
+                        }
+                        uint32_t u;
+                        double acc;
+                        if (p < s0 && (t >= tail.size() || a[p].first <= tail[t].first)) {
+                            u = a[p].first;
+                            acc = a[p].second;
+                            ++p;
+                        } else {
+                            u = tail[t].first;
+                            acc = tail[t].second;
+                            ++t;
+                        }
+                        for (; t < tail.size() && tail[t].first == u; ++t) acc += tail[t].second;
+                        merged.push_back({u, acc});
                     }
-                    sc.acc[e.first] += e.second;
+                    a.assign(merged.begin(), merged.end());
                 }
-                std::sort(sc.order.begin(), sc.order.end());
-                a.resize(sc.order.size());
-                for (uint32_t u : sc.order) {
-                    a[w++] = {u, sc.acc[u]};
-                    sc.acc[u] = 0.0;
-                    sc.seen[u] = 0;
-                }
+                sorted_len[v] = (uint32_t)a.size();
                 uint64_t deg = std::min<uint64_t>(a.size(), 255);
                 key[v] = (deg << 56) | (mix64(seed ^ ((uint64_t)v << 20) ^ r) & 0x00FFFFFFFF000000ull) | 0;
             }
         });
+        st.mark(1);
         // Stop the rounds once the remaining graph is a small or dense core:
         // a dense core (<= core_dense_max vertices) is inverted exactly; a
         // larger one, reached when rounds stop paying (fewer than
@@ -766,8 +927,10 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
                 }
             }
             ++r;
+            st.mark(2);
             break;
         }
+        st.mark(2);
         // the round: every live vertex that is the minimum of (key, id) over its neighbours
         std::vector<std::vector<uint32_t>> sel_part(blocks(live.size()));
         par(sel_part.size(), [&](size_t b) {
@@ -787,12 +950,16 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
         });
         sel.clear();
         for (auto& p : sel_part) sel.insert(sel.end(), p.begin(), p.end());
+        st.mark(3);
         // eliminate the round: columns of L, pivots and sampled fill edges
-        std::vector<std::vector<Edge>> fill_part(blocks(sel.size()));
+        // (a dense graph's rounds select few vertices of high degree: small blocks)
+        const size_t EBLK = n >= 16384 ? VBLK : 4;
+        std::vector<std::vector<Edge>> fill_part((sel.size() + EBLK - 1) / EBLK);
         par(fill_part.size(), [&](size_t b) {
             std::vector<std::pair<uint32_t, double>> ent;
-            const size_t j1 = std::min(sel.size(), (b + 1) * VBLK);
-            for (size_t j = b * VBLK; j < j1; ++j) {
+            std::vector<double> pre;
+            const size_t j1 = std::min(sel.size(), (b + 1) * EBLK);
+            for (size_t j = b * EBLK; j < j1; ++j) {
                 const uint32_t v = sel[j];
                 f.round[v] = r;
                 double d = 0;
@@ -806,19 +973,76 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
                 for (auto& e : adj[v]) cv.push_back({e.first, -e.second / d});
                 ent = adj[v];
                 Rng rng{mix64(seed * 0x9E3779B97F4A7C15ull + v + 1)};
-                sample_star(ent, split, rng, fill_part[b]);
+                sample_star(ent, split, rng, fill_part[b], pre);
             }
         });
-        fill.clear();
-        for (auto& p : fill_part) fill.insert(fill.end(), p.begin(), p.end());
+        st.mark(4);
         for (uint32_t v : sel) {
             alive[v] = 0;
             adj[v].clear();
             adj[v].shrink_to_fit();
         }
-        for (auto& e : fill) {
-            adj[e.lo].push_back({e.hi, e.w});
-            adj[e.hi].push_back({e.lo, e.w});
+        // append every fill edge to both endpoints' lists in fill order (the
+        // parts in order are the fill list): chunks of parts count their
+        // entries per vertex, then scatter them into a flat array by
+        // (vertex, chunk), and blocks of vertices append their runs
+        {
+            size_t n_fill = 0;
+            for (auto& p : fill_part) n_fill += p.size();
+            size_t nch = 1;
+            if (threaded && n_fill >= 4096)
+                nch = std::min<size_t>({(size_t)16, fill_part.size(), std::max<size_t>(1, 2 * n_fill / n)});
+            if (nch <= 1) {
+                for (auto& p : fill_part)
+                    for (auto& e : p) {
+                        adj[e.lo].push_back({e.hi, e.w});
+                        adj[e.hi].push_back({e.lo, e.w});
+                    }
+            } else {
+                std::vector<size_t> cp{0};
+                {
+                    size_t acc = 0, goal = (n_fill + nch - 1) / nch;
+                    for (size_t q = 0; q < fill_part.size(); ++q) {
+                        acc += fill_part[q].size();
+                        if (acc >= goal * cp.size() && cp.size() < nch) cp.push_back(q + 1);
+                    }
+                    while (cp.size() <= nch) cp.push_back(fill_part.size());
+                }
+                std::vector<std::vector<uint32_t>> cnt(nch);
+                par_for_each(nch, [&](size_t t) {
+                    cnt[t].assign(n, 0);
+                    for (size_t q = cp[t]; q < cp[t + 1]; ++q)
+                        for (auto& e : fill_part[q]) {
+                            ++cnt[t][e.lo];
+                            ++cnt[t][e.hi];
+                        }
+                });
+                std::vector<size_t> beg(n + 1, 0);
+                for (uint32_t u = 0; u < n; ++u) {
+                    size_t o = beg[u];
+                    for (size_t t = 0; t < nch; ++t) {
+                        const uint32_t c = cnt[t][u];
+                        cnt[t][u] = (uint32_t)(o - beg[u]);   // chunk t's first entry within u's run
+                        o += c;
+                    }
+                    beg[u + 1] = o;
+                }
+                std::vector<std::pair<uint32_t, double>> flat(beg[n]);
+                par_for_each(nch, [&](size_t t) {
+                    std::vector<uint32_t>& pos = cnt[t];
+                    for (size_t q = cp[t]; q < cp[t + 1]; ++q)
+                        for (auto& e : fill_part[q]) {
+                            flat[beg[e.lo] + pos[e.lo]++] = {e.hi, e.w};
+                            flat[beg[e.hi] + pos[e.hi]++] = {e.lo, e.w};
+                        }
+                });
+                par_for_each(((size_t)n + 4095) / 4096, [&](size_t b) {
+                    const uint32_t u1 = (uint32_t)std::min<size_t>(n, (b + 1) * (size_t)4096);
+                    for (uint32_t u = (uint32_t)(b * 4096); u < u1; ++u)
+                        if (beg[u + 1] > beg[u])
+                            adj[u].insert(adj[u].end(), flat.begin() + beg[u], flat.begin() + beg[u + 1]);
+                });
+            }
         }
         const size_t before = live.size();
         size_t w = 0;
@@ -827,6 +1051,7 @@ void ac_rounds(const Lap& m, const PrecondCfg& cfg, Factor& f) {
         live.resize(w);
         last_frac = (double)sel.size() / (double)before;
         ++r;
+        st.mark(5);
     }
     f.n_rounds = r;
 }
@@ -1124,10 +1349,13 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             if (BuildTrace::on())
                 fprintf(stderr, "[within trace]     pair %zu: %u components after %.3f ms\n", pi, ncomp,
                         (BuildTrace::now() - tr_pair.t0) * 1e3);
+            static const char* const steps[] = {"extract", "forms", "lists", "rows", "transpose"};
+            StepTimes st(ncomp > 1 ? "components" : "component", steps, 5);
             std::vector<std::vector<uint32_t>> crow(ncomp), ccol(ncomp);
             for (uint32_t i = 0; i < nr; ++i) crow[lab[i]].push_back(i);
             for (uint32_t k = 0; k < nc; ++k) ccol[lab[nr + k]].push_back(k);
             std::vector<uint32_t> rre(nr, UINT32_MAX), cre(nc, UINT32_MAX);
+            st.mark(2);
             for (uint32_t ci = 0; ci < ncomp; ++ci) {
                 Comp cp;
                 std::vector<double> diag;
@@ -1140,21 +1368,61 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                     for (uint32_t i = 0; i < ccol[ci].size(); ++i) cre[ccol[ci][i]] = i;
                     cp.m.c.nr = (uint32_t)crow[ci].size();
                     cp.m.c.nc = (uint32_t)ccol[ci].size();
-                    for (uint32_t o : crow[ci]) {
-                        for (uint32_t k = full.c.ptr[o]; k < full.c.ptr[o + 1]; ++k) {
-                            uint32_t nj = cre[full.c.col[k]];
-                            if (nj != UINT32_MAX) { cp.m.c.col.push_back(nj); cp.m.c.val.push_back(full.c.val[k]); }
+                    const std::vector<uint32_t>& rows = crow[ci];
+                    if (rows.size() >= 65536) {   // rows counted, then filled, by blocks on the host pool
+                        const size_t RB = 16384, nb = (rows.size() + RB - 1) / RB;
+                        std::vector<uint32_t>& ptr = cp.m.c.ptr;
+                        ptr.assign(rows.size() + 1, 0);
+                        par_for_each(nb, [&](size_t b) {
+                            const size_t i1 = std::min(rows.size(), (b + 1) * RB);
+                            for (size_t i = b * RB; i < i1; ++i) {
+                                uint32_t c = 0;
+                                for (uint32_t k = full.c.ptr[rows[i]]; k < full.c.ptr[rows[i] + 1]; ++k)
+                                    c += cre[full.c.col[k]] != UINT32_MAX;
+                                ptr[i + 1] = c;
+                            }
+                        });
+                        for (size_t i = 0; i < rows.size(); ++i) ptr[i + 1] += ptr[i];
+                        cp.m.c.col.resize(ptr.back());
+                        cp.m.c.val.resize(ptr.back());
+                        par_for_each(nb, [&](size_t b) {
+                            const size_t i1 = std::min(rows.size(), (b + 1) * RB);
+                            for (size_t i = b * RB; i < i1; ++i) {
+                                uint32_t q = ptr[i];
+                                for (uint32_t k = full.c.ptr[rows[i]]; k < full.c.ptr[rows[i] + 1]; ++k) {
+                                    const uint32_t nj = cre[full.c.col[k]];
+                                    if (nj != UINT32_MAX) {
+                                        cp.m.c.col[q] = nj;
+                                        cp.m.c.val[q] = full.c.val[k];
+                                        ++q;
+                                    }
+                                }
+                            }
+                        });
+                    } else {
+                        for (uint32_t o : rows) {
+                            for (uint32_t k = full.c.ptr[o]; k < full.c.ptr[o + 1]; ++k) {
+                                uint32_t nj = cre[full.c.col[k]];
+                                if (nj != UINT32_MAX) { cp.m.c.col.push_back(nj); cp.m.c.val.push_back(full.c.val[k]); }
+                            }
+                            cp.m.c.ptr.push_back((uint32_t)cp.m.c.col.size());
                         }
-                        cp.m.c.ptr.push_back((uint32_t)cp.m.c.col.size());
                     }
+                    st.mark(3);
                     cp.m.ct = transpose(cp.m.c);
+                    st.mark(4);
                     for (uint32_t o : crow[ci]) { rre[o] = UINT32_MAX; diag.push_back(rdiag[o]); }
                     for (uint32_t o : ccol[ci]) { cre[o] = UINT32_MAX; diag.push_back(cdiag[o]); }
                 }
+                st.mark(0);
                 bool allzero = true;
                 for (double v : diag) allzero = allzero && v == 0.0;
-                if (allzero) continue;
+                if (allzero) {
+                    st.mark(1);
+                    continue;
+                }
                 std::vector<uint32_t> globals;
+                globals.reserve(crow[ci].size() + ccol[ci].size());
                 for (uint32_t o : crow[ci]) globals.push_back(l2g[o]);
                 for (uint32_t o : ccol[ci]) globals.push_back(l2g[nr + o]);
                 if (cp.m.nc() > cp.m.nr()) {  // orient_for_elimination (sddm.rs:85-106)
@@ -1185,6 +1453,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 dm.globals = std::move(globals);
                 dm.comp = std::move(cp);
                 doms.push_back(std::move(dm));
+                st.mark(1);
             }
         });
     tr_pairs.done();

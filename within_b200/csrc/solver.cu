@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -101,12 +102,44 @@ struct Arena {
     }
     template <class T>
     T* upload(const std::vector<T>& v) {
-        T* p = alloc<T>(v.size());
-        if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
-        return p;
+        if (v.empty()) return alloc<T>(1);
+        void* p = nullptr;
+        CK(cudaMalloc(&p, v.size() * sizeof(T)));
+        ptrs.push_back(p);
+        CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return (T*)p;
     }
     ~Arena() {
         for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+// Many host arrays uploaded into one device allocation of the arena (each
+// at a 256-byte aligned offset; empty arrays get a zeroed slot): one
+// cudaMalloc instead of one per array.
+struct UploadBatch {
+    struct Item {
+        const void* src;
+        size_t bytes, off;
+        std::function<void(char*)> set;
+    };
+    std::vector<Item> items;
+    size_t total = 0;
+    template <class T, class P>
+    void add(P*& dst, const std::vector<T>& v) {
+        const size_t b = v.size() * sizeof(T);
+        items.push_back({v.data(), b, total, [&dst](char* p) { dst = reinterpret_cast<P*>(p); }});
+        total += (std::max<size_t>(b, 1) + 255) / 256 * 256;
+    }
+    void commit(Arena& A) {
+        char* base = nullptr;
+        CK(cudaMalloc(&base, std::max<size_t>(total, 256)));
+        A.ptrs.push_back(base);
+        CK(cudaMemset(base, 0, std::max<size_t>(total, 256)));
+        for (Item& it : items) {
+            it.set(base + it.off);
+            if (it.bytes) CK(cudaMemcpy(base + it.off, it.src, it.bytes, cudaMemcpyHostToDevice));
+        }
     }
 };
 
@@ -368,55 +401,64 @@ namespace {
 
 int kidx(int K) { return K == 1 ? 0 : K == 2 ? 1 : K == 4 ? 2 : 3; }
 
-void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
+// The device image of P.host (set by the caller).
+void upload_schwarz_image(within_preconditioner& P) {
     Arena& A = P.arena;
-    P.host = std::move(S);
     SchwarzHost& H = P.host;
     SchwarzDev& D = P.dev_const;
     D.n_sub = H.n_sub;
-    D.loc_ptr = A.upload(H.loc_ptr);
-    D.n_elim = A.upload(H.n_elim);
-    D.red_off = A.upload(H.red_off);
-    D.n_kept = A.upload(H.n_kept);
-    D.red_n = A.upload(H.red_n);
-    D.mode = A.upload(H.mode);
-    D.glob = A.upload(H.glob);
-    D.scale = A.upload(H.scale);
-    D.slot_sub = A.upload(H.slot_sub);
-    D.inv_e = A.upload(H.inv_e);
-    D.ct_col = A.upload(H.ct_col);
-    D.ct_val = A.upload(H.ct_val);
-    D.ct_rowsum = A.upload(H.ct_rowsum);
-    D.ct_row_slot = A.upload(H.ct_row_slot);
-    D.ct_row_red = A.upload(H.ct_row_red);
-    D.elim_slot = A.upload(H.elim_slot);
-    D.c_col = A.upload(H.c_col);
-    D.c_val = A.upload(H.c_val);
-    D.red_sub = A.upload(H.red_sub);
-    D.dense_row_slot = A.upload(H.dense_row_slot);
-    D.dense_col = A.upload(H.dense_col);
-    D.dense_val = A.upload(H.dense_val);
-    D.dinv = A.upload(H.dinv);
-    D.fwd_row = A.upload(H.fwd_row);
-    D.fwd_col = A.upload(H.fwd_col);
-    D.fwd_val = A.upload(H.fwd_val);
-    D.bwd_row = A.upload(H.bwd_row);
-    D.bwd_col = A.upload(H.bwd_col);
-    D.bwd_val = A.upload(H.bwd_val);
-    D.dof_slot = A.upload(H.dof_slot);
-    D.kept_ptr = A.upload(H.kept_ptr);
-    D.core_row_slot = A.upload(H.core_row_slot);
-    D.core_col = A.upload(H.core_col);
-    D.core_val = A.upload(H.core_val);
+    UploadBatch U;
+    U.add(D.loc_ptr, H.loc_ptr);
+    U.add(D.n_elim, H.n_elim);
+    U.add(D.red_off, H.red_off);
+    U.add(D.n_kept, H.n_kept);
+    U.add(D.red_n, H.red_n);
+    U.add(D.mode, H.mode);
+    U.add(D.glob, H.glob);
+    U.add(D.scale, H.scale);
+    U.add(D.slot_sub, H.slot_sub);
+    U.add(D.inv_e, H.inv_e);
+    U.add(D.ct_col, H.ct_col);
+    U.add(D.ct_val, H.ct_val);
+    U.add(D.ct_rowsum, H.ct_rowsum);
+    U.add(D.ct_row_slot, H.ct_row_slot);
+    U.add(D.ct_row_red, H.ct_row_red);
+    U.add(D.elim_slot, H.elim_slot);
+    U.add(D.c_col, H.c_col);
+    U.add(D.c_val, H.c_val);
+    U.add(D.red_sub, H.red_sub);
+    U.add(D.dense_row_slot, H.dense_row_slot);
+    U.add(D.dense_col, H.dense_col);
+    U.add(D.dense_val, H.dense_val);
+    U.add(D.dinv, H.dinv);
+    U.add(D.fwd_row, H.fwd_row);
+    U.add(D.fwd_col, H.fwd_col);
+    U.add(D.fwd_val, H.fwd_val);
+    U.add(D.bwd_row, H.bwd_row);
+    U.add(D.bwd_col, H.bwd_col);
+    U.add(D.bwd_val, H.bwd_val);
+    U.add(D.dof_slot, H.dof_slot);
+    U.add(D.kept_ptr, H.kept_ptr);
+    U.add(D.core_row_slot, H.core_row_slot);
+    U.add(D.core_col, H.core_col);
+    U.add(D.core_val, H.core_val);
+    uint32_t* ct_ptr = nullptr;
+    U.add(ct_ptr, H.ct_ptr);
+    uint32_t* dense_ptr = nullptr;
+    U.add(dense_ptr, H.dense_rows_ptr);
+    uint32_t* fwd_ptr = nullptr;
+    U.add(fwd_ptr, H.fwd_ptr);
+    uint32_t* bwd_ptr = nullptr;
+    U.add(bwd_ptr, H.bwd_ptr);
+    uint32_t* c_ptr = nullptr;
+    U.add(c_ptr, H.c_ptr);
+    uint32_t* dof_ptr = nullptr;
+    U.add(dof_ptr, H.dof_ptr);
+    uint32_t* core_ptr = nullptr;
+    U.add(core_ptr, H.core_rows_ptr);
+    U.commit(A);
     uint32_t* loc_ptr = const_cast<uint32_t*>(D.loc_ptr);
-    uint32_t* ct_ptr = A.upload(H.ct_ptr);
     uint32_t* kept_ptr = const_cast<uint32_t*>(D.kept_ptr);
-    uint32_t* dense_ptr = A.upload(H.dense_rows_ptr);
-    uint32_t* fwd_ptr = A.upload(H.fwd_ptr);
-    uint32_t* bwd_ptr = A.upload(H.bwd_ptr);
-    uint32_t* c_ptr = A.upload(H.c_ptr);
-    uint32_t* dof_ptr = A.upload(H.dof_ptr);
-    uint32_t* core_ptr = A.upload(H.core_rows_ptr);
     auto one = [&](uint32_t* ptr) { return A.upload(std::vector<SegProb>{SegProb{ptr, 0, 0}}); };
     P.p_restrict = one(loc_ptr);
     P.p_ct = one(ct_ptr);
@@ -435,6 +477,11 @@ void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
     }
     P.p_fwd = A.upload(fw);
     P.p_bwd = A.upload(bw);
+}
+
+void upload_schwarz(within_preconditioner& P, SchwarzHost&& S) {
+    P.host = std::move(S);
+    upload_schwarz_image(P);
 }
 
 // Schwarz work buffers of one user (solver) for K columns.
@@ -760,6 +807,7 @@ struct within_solver {
     // workspaces per K
     struct Work {
         bool ready = false;
+        bool buffers = false;   // the vectors below are allocated
         double *u, *b, *yint, *v, *p, *h, *hb, *x, *dm;
         double* x0 = nullptr;   // warm start, interleaved (allocated on first use)
         double* partials;
@@ -1250,10 +1298,10 @@ int env_path(int dflt) {
     return dflt;
 }
 
-within_solver::Work& ensure_work(within_solver& s, int K) {
+// The device vectors of the LSMR loop for K columns (no plans).
+within_solver::Work& work_buffers(within_solver& s, int K) {
     auto& w = s.work[kidx(K)];
-    if (w.ready) return w;
-    PhaseTrace pt("first use of a column bucket: workspaces and plans");
+    if (w.buffers) return w;
     Arena& A = s.arena;
     w.u = A.alloc<double>(s.n_obs * K);
     w.b = A.alloc<double>(s.n_obs * K);
@@ -1270,6 +1318,15 @@ within_solver::Work& ensure_work(within_solver& s, int K) {
     w.nonfinite = A.alloc<int>(1);
     w.st = A.alloc<ColState>(2 * 8);
     w.ctl = A.alloc<Ctl>(1);
+    w.buffers = true;
+    return w;
+}
+
+within_solver::Work& ensure_work(within_solver& s, int K) {
+    auto& w = s.work[kidx(K)];
+    if (w.ready) return w;
+    PhaseTrace pt("first use of a column bucket: workspaces and plans");
+    work_buffers(s, K);
     if (s.precond && s.precond->kind == 1) schwarz_user_plans(s.schwarz, *s.precond, K);
     ensure_scatter(s, K);
     // Path choice per column count, fixed per process so results stay bitwise
@@ -1938,8 +1995,12 @@ int guarded(F f) {
     }
 }
 
+// prepare_single: also make the single-column workspaces and Schwarz plans
+// (the first solve's set-up), overlapping the preconditioner's host build and
+// upload; solver sets, which solve column batches, leave them to first use.
 within_solver* make_solver(const within_design* d, const double* weights, const within_precond_config* cfg,
-                           const within_preconditioner* prebuilt, int device, const within_tuning* tuning = nullptr) {
+                           const within_preconditioner* prebuilt, int device, const within_tuning* tuning = nullptr,
+                           bool prepare_single = true) {
     if (!d) throw WError(ERR_INVALID, "design is NULL");
     if (device < 0) CK(cudaGetDevice(&device));
     set_device(device);
@@ -2132,6 +2193,10 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         if (env_path(2) == 2) ensure_rowsweep<1>(*s);
     }
     pt_op.done();
+    if (prepare_single) {
+        PhaseTrace pt("single-column workspaces");
+        work_buffers(*s, 1);
+    }
     if (pre_thread.joinable()) {
         PhaseTrace pt_wait("wait for the preconditioner host build");
         pre_thread.join();
@@ -2148,8 +2213,30 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
                 if (pre.kind == 2) {
                     P->inv_diag = P->arena.upload(pre.inv_diag);
                     P->host_inv_diag = pre.inv_diag;
+                } else {
+                    // the single-column plans read only the host image: built
+                    // on a second thread while the image uploads
+                    P->host = std::move(pre.schwarz);
+                    std::exception_ptr plan_err;
+                    std::thread plans;
+                    if (prepare_single)
+                        plans = std::thread([&] {
+                            try {
+                                set_device(device);
+                                schwarz_user_plans(s->schwarz, *P, 1);
+                            } catch (...) {
+                                plan_err = std::current_exception();
+                            }
+                        });
+                    try {
+                        upload_schwarz_image(*P);
+                    } catch (...) {
+                        if (plans.joinable()) plans.join();
+                        throw;
+                    }
+                    if (plans.joinable()) plans.join();
+                    if (plan_err) std::rethrow_exception(plan_err);
                 }
-                else upload_schwarz(*P, std::move(pre.schwarz));
             } catch (...) {
                 delete P;
                 throw;
@@ -2472,7 +2559,7 @@ int within_solvers_new(uint64_t n, const within_design* const* designs, const do
         try {
             parallel_for(n, threads, dev, [&](uint64_t i) {
                 if (!designs[i]) throw WError(ERR_INVALID, "design " + std::to_string(i) + " is null");
-                out[i] = make_solver(designs[i], weights ? weights[i] : nullptr, cfg, nullptr, dev);
+                out[i] = make_solver(designs[i], weights ? weights[i] : nullptr, cfg, nullptr, dev, nullptr, false);
             });
         } catch (...) {
             for (uint64_t i = 0; i < n; ++i) {
