@@ -55,6 +55,19 @@ def test_tile_planner_properties(tmp_path):
     assert "plan ok" in out
 
 
+def test_host_pool(tmp_path):
+    """The set-up's host thread pool (host_pool.hpp): every item once, jobs
+    posted from inside items and from several caller threads, the lowest
+    failing index's exception rethrown, WITHIN_HOST_THREADS=1 serial on the
+    caller (tests/cpp/pool_test.cpp)."""
+    exe = tmp_path / "pool_test"
+    csrc = os.path.join(ROOT, "within_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-I", csrc, "-o", str(exe),
+                    os.path.join(ROOT, "tests", "cpp", "pool_test.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True, timeout=120).stdout
+    assert "pool ok" in out
+
+
 def test_segsweep_planner_and_warp_algorithm(tmp_path):
     """The warp-range segmented sweep (segsweep.cuh) executed lane by lane on
     the host over random multi-problem layouts planned by SSHostPlan::add:

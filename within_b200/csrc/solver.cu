@@ -608,8 +608,6 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
     kp.ct = one(H.ct_ptr, U.tuning.warp_ranges >= 2 || (U.tuning.warp_ranges == 1 && K == 1));
     kp.kept = one(H.kept_ptr, ss);
     kp.dense = one(H.dense_rows_ptr, ss);
-    kp.c = one(H.c_ptr, ss);
-    kp.prolong = one(H.dof_ptr, ss);
     const bool segt_on = U.tuning.segthread;
     if (segt_on && H.c_ptr.size() > 1 && seg_max_len(H.c_ptr.data(), H.c_ptr.size() - 1) <= SEGT_MAX_LEN)
         kp.c_thread = (uint32_t)(H.c_ptr.size() - 1);
@@ -617,6 +615,9 @@ KPlans& schwarz_user_plans(SchwarzUser& U, const within_preconditioner& P, int K
         kp.c_lanes = segvec_lanes((double)(H.c_ptr.back() - H.c_ptr.front()) / (double)kp.c_thread);
     if (segt_on && H.dof_ptr.size() > 1 && seg_max_len(H.dof_ptr.data(), H.dof_ptr.size() - 1) <= SEGT_MAX_LEN)
         kp.prolong_thread = (uint32_t)(H.dof_ptr.size() - 1);
+    // tile plans only where the one-thread-per-segment kernels are not used
+    if (!kp.c_thread) kp.c = one(H.c_ptr, ss);
+    if (!kp.prolong_thread) kp.prolong = one(H.dof_ptr, ss);
     kp.core = one(H.core_rows_ptr, ss);
     auto rounds = [&](const std::vector<uint32_t>& rptr, const std::vector<uint32_t>& ptr) {
         if (ss) {
@@ -3035,11 +3036,14 @@ void* g_noalloc_dev_ptr[NOALLOC_MAX_DEVICES] = {};
 
 // Device address of g_noalloc_scratch on `dev` (which must be current).  On the
 // host the array's name only identifies the symbol; the address is looked up
-// once per device and cached.
-void* noalloc_scratch(int dev) {
+// on every call outside stream capture (so a context created after a device
+// reset gets its own) and the last one is reused while `st` is capturing.
+void* noalloc_scratch(int dev, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
     std::lock_guard<std::mutex> g(g_noalloc_mu);
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw WError(ERR_UNSUPPORTED, "device ordinal out of range");
-    if (!g_noalloc_dev_ptr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone || !g_noalloc_dev_ptr[dev]) {
         void* p = nullptr;
         CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         g_noalloc_dev_ptr[dev] = p;
@@ -3072,12 +3076,12 @@ extern "C" int within_solver_operator_apply_adjoint_noalloc(within_solver* s, co
                          " bytes of scratch (" + std::to_string(pl.n_tiles) + " tiles, " +
                          std::to_string(pl.n_splits) + " split segments); the static maximum is " +
                          std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes");
-        char* base = (char*)noalloc_scratch(s->device);
+        cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+        char* base = (char*)noalloc_scratch(s->device, st);
         DevPlan p = pl;
         p.head = (double*)base;
         p.tail = (double*)(base + head_b);
         p.counters = (unsigned*)(base + head_b + tail_b);
-        cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
         // the completion counters must start at zero; partials are written before they are read
         CK(cudaMemsetAsync(p.counters, 0, cnt_b, st));
         ScatterF<1, 0> f{s->scatter_probs, u_dev, s->op.sqrt_w, y_dev, nullptr};
