@@ -1190,6 +1190,8 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
     BuildTrace tr_pairs("channel pairs: cross-tabs, components, SDDM forms");
     par_for_each(pairs.size(), [&](size_t pi) {
             BuildTrace tr_pair("pair", (long)pi);
+            static const char* const psteps[] = {"maps", "cells", "diagonals", "labels"};
+            StepTimes pst("pair set-up", psteps, 4);
             std::vector<Domain>& doms = pair_doms[pi];
             uint64_t& n_warnings = pair_warnings[pi];
             Ch R = ch[pairs[pi].first], Cc = ch[pairs[pi].second];
@@ -1202,6 +1204,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             for (uint32_t k = 0; k < TC.n_levels; ++k)
                 if (active[Cc.term][k]) { cmap[k] = nc++; l2g.push_back(TC.offset + Cc.col * TC.n_levels + k); }
             if (nr == 0 || nc == 0) return;
+            pst.mark(0);
             // weighted cross-tab, each cell summed in observation order (accumulate.rs)
             const uint32_t* rl = d.codes[R.term].data();
             const uint32_t* cl = d.codes[Cc.term].data();
@@ -1225,36 +1228,51 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                     full.ct.col = std::move(X.row);
                     full.ct.val = std::move(X.tval);
                 } else {
-                    full.c.col.reserve(X.col.size());
-                    full.c.val.reserve(X.col.size());
-                    for (uint32_t j = 0; j < TR.n_levels; ++j) {
-                        if (!active[R.term][j]) continue;
-                        for (uint32_t p = X.row_ptr[j]; p < X.row_ptr[j + 1]; ++p) {
-                            full.c.col.push_back(cmap[X.col[p]]);
-                            full.c.val.push_back(X.val[p]);
-                        }
-                        full.c.ptr.push_back((uint32_t)full.c.col.size());
-                    }
+                    // the active levels' rows (every cell of one is kept), renumbered;
+                    // rows copied by blocks on the host pool
+                    auto renumber = [&](const std::vector<char>& act, uint32_t n_levels,
+                                        const std::vector<uint32_t>& xptr, const std::vector<uint32_t>& xidx,
+                                        const std::vector<double>& xval, const std::vector<uint32_t>& map,
+                                        Csr& o) {
+                        std::vector<uint32_t> src;
+                        for (uint32_t j = 0; j < n_levels; ++j)
+                            if (act[j]) src.push_back(j);
+                        o.ptr.assign(src.size() + 1, 0);
+                        for (size_t i = 0; i < src.size(); ++i)
+                            o.ptr[i + 1] = o.ptr[i] + (xptr[src[i] + 1] - xptr[src[i]]);
+                        o.col.resize(o.ptr.back());
+                        o.val.resize(o.ptr.back());
+                        const size_t RB = 16384;
+                        par_for_each((src.size() + RB - 1) / RB, [&](size_t b) {
+                            const size_t i1 = std::min(src.size(), (b + 1) * RB);
+                            for (size_t i = b * RB; i < i1; ++i) {
+                                uint32_t q = o.ptr[i];
+                                for (uint32_t p = xptr[src[i]]; p < xptr[src[i] + 1]; ++p, ++q) {
+                                    o.col[q] = map[xidx[p]];
+                                    o.val[q] = xval[p];
+                                }
+                            }
+                        });
+                    };
+                    renumber(active[R.term], TR.n_levels, X.row_ptr, X.col, X.val, cmap, full.c);
                     full.ct.nr = nc;
                     full.ct.nc = nr;
-                    full.ct.col.reserve(X.row.size());
-                    full.ct.val.reserve(X.row.size());
-                    for (uint32_t k = 0; k < TC.n_levels; ++k) {
-                        if (!active[Cc.term][k]) continue;
-                        for (uint32_t p = X.col_ptr[k]; p < X.col_ptr[k + 1]; ++p) {
-                            full.ct.col.push_back(rmap[X.row[p]]);
-                            full.ct.val.push_back(X.tval[p]);
-                        }
-                        full.ct.ptr.push_back((uint32_t)full.ct.col.size());
-                    }
+                    renumber(active[Cc.term], TC.n_levels, X.col_ptr, X.row, X.tval, rmap, full.ct);
                 }
+                pst.mark(1);
                 if (!w && kr < 0 && kc < 0) {
                     // unweighted intercepts: the diagonals are observation counts,
                     // integer sums of the cells (exact in any order)
-                    for (uint32_t r = 0; r < nr; ++r)
-                        for (uint32_t p = full.c.ptr[r]; p < full.c.ptr[r + 1]; ++p) rdiag[r] += full.c.val[p];
-                    for (uint32_t c = 0; c < nc; ++c)
-                        for (uint32_t p = full.ct.ptr[c]; p < full.ct.ptr[c + 1]; ++p) cdiag[c] += full.ct.val[p];
+                    auto row_sums = [&](const Csr& m, std::vector<double>& out) {
+                        const uint32_t RB = 16384;
+                        par_for_each(((size_t)m.nr + RB - 1) / RB, [&](size_t b) {
+                            const uint32_t r1 = (uint32_t)std::min<size_t>(m.nr, (b + 1) * (size_t)RB);
+                            for (uint32_t r = (uint32_t)(b * RB); r < r1; ++r)
+                                for (uint32_t p = m.ptr[r]; p < m.ptr[r + 1]; ++p) out[r] += m.val[p];
+                        });
+                    };
+                    row_sums(full.c, rdiag);
+                    row_sums(full.ct, cdiag);
                 } else {
                     for (uint64_t i = 0; i < d.n_obs; ++i) {
                         double wi = w ? w[i] : 1.0;
@@ -1307,6 +1325,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             if (BuildTrace::on())
                 fprintf(stderr, "[within trace]     pair %zu cross-tab %u x %u, %u cells%s\n", pi, nr, nc,
                         full.c.nnz(), cross_tabs ? " (GPU)" : "");
+            pst.mark(2);
             const bool known = kr < 0 && kc < 0;
             // components (cross_tab.rs:175-211): label by DFS, then group;
             // numbered in the order of their smallest vertex
@@ -1346,6 +1365,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
                 }
                 ++ncomp;
             }
+            pst.mark(3);
             if (BuildTrace::on())
                 fprintf(stderr, "[within trace]     pair %zu: %u components after %.3f ms\n", pi, ncomp,
                         (BuildTrace::now() - tr_pair.t0) * 1e3);
@@ -1656,16 +1676,39 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
     // rows (= eliminated columns) pull from later rows.
     S.n_rounds = rounds;
     std::vector<std::vector<uint32_t>> by_round(rounds);
-    std::vector<std::vector<std::vector<std::pair<uint32_t, double>>>> rowents(S.n_sub);
+    // rows of each subdomain's L (the transpose of its columns colv), one flat
+    // CSR per subdomain: row u lists (reduced slot of column v, l) in ascending v
+    struct Rows {
+        std::vector<uint32_t> ptr, col;
+        std::vector<double> val;
+    };
+    std::vector<Rows> rowents(S.n_sub);
+    par_for_each(S.n_sub, [&](size_t si) {
+        const Factor& f = doms[si].fac;
+        if (f.dense) return;
+        const uint32_t ro = S.red_off[si];
+        Rows& R = rowents[si];
+        R.ptr.assign((size_t)f.n + 1, 0);
+        for (uint32_t v = 0; v < f.n; ++v)
+            for (auto& e : f.colv[v]) ++R.ptr[e.first + 1];
+        for (uint32_t u = 0; u < f.n; ++u) R.ptr[u + 1] += R.ptr[u];
+        R.col.resize(R.ptr[f.n]);
+        R.val.resize(R.ptr[f.n]);
+        std::vector<uint32_t> cur(R.ptr.begin(), R.ptr.end() - 1);
+        for (uint32_t v = 0; v < f.n; ++v)
+            for (auto& e : f.colv[v]) {
+                const uint32_t q = cur[e.first]++;
+                R.col[q] = ro + v;
+                R.val[q] = e.second;
+            }
+    });
     for (uint32_t s = 0; s < S.n_sub; ++s) {
         const Factor& f = doms[s].fac;
         if (f.dense) continue;
         const uint32_t ro = S.red_off[s];
-        rowents[s].assign(f.n, {});
         for (uint32_t v = 0; v < f.n; ++v) {
             S.dinv[ro + v] = f.dinv[v];
             by_round[f.round[v]].push_back(ro + v);
-            for (auto& e : f.colv[v]) rowents[s][e.first].push_back({ro + v, e.second});
             S.factor_nnz += f.colv[v].size();
         }
     }
@@ -1678,10 +1721,9 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         for (uint32_t slot : by_round[r]) {
             uint32_t s = S.red_sub[slot], v = slot - S.red_off[s];
             S.fwd_row.push_back(slot);
-            for (auto& e : rowents[s][v]) {
-                S.fwd_col.push_back(e.first);
-                S.fwd_val.push_back(e.second);
-            }
+            const Rows& R = rowents[s];
+            S.fwd_col.insert(S.fwd_col.end(), R.col.begin() + R.ptr[v], R.col.begin() + R.ptr[v + 1]);
+            S.fwd_val.insert(S.fwd_val.end(), R.val.begin() + R.ptr[v], R.val.begin() + R.ptr[v + 1]);
             S.fwd_ptr.push_back((uint32_t)S.fwd_col.size());
             S.bwd_row.push_back(slot);
             for (auto& e : doms[s].fac.colv[v]) {
