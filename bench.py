@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--kernel-timeline", choices=["fp64", "mixed"], default=None,
                     help="instead of the bench line: per-kernel device times of one solve (torch.profiler "
                          "/ CUPTI timestamps); 'mixed' = weighted panel, k = 4, mixed precision")
+    ap.add_argument("--setup-trace", action="store_true",
+                    help="instead of the bench line: Solver::new + first solve (best of 3) of the fixest-like "
+                         "1M design and the 10M panel, each in its own process, with the set-up's phase "
+                         "trace (WITHIN_TRACE=1) of the best run")
     ap.add_argument("--tuning", default="auto",
                     help="tuning record of the headline solver: 'auto' (the autotuner's table), 'none' (the "
                          "defaults and WITHIN_* overrides) or a JSON dict of within_tuning fields")
@@ -889,8 +893,54 @@ def kernel_timeline(args):
                       "kernels": out, "families": fam}, indent=1))
 
 
+_SETUP_CHILD = r"""
+import json, sys, time
+import numpy as np
+import within_b200 as W
+from within_b200 import workloads as WL
+wl = sys.argv[1]
+if wl == "akm10m":
+    codes = WL.akm_panel(); y = np.random.default_rng(7).standard_normal(codes.shape[0]); tol = 1e-8
+else:
+    codes, y = WL.fixest_like(); tol = 1e-6
+opts = W.LsmrOptions(tol=tol, maxiter=200)
+best = None
+for rep in range(3):
+    print("=== rep", rep, file=sys.stderr, flush=True)
+    t0 = time.perf_counter(); s = W.Solver(codes); t1 = time.perf_counter()
+    r = s.solve(y, opts); t2 = time.perf_counter()
+    cur = (t2 - t0, t1 - t0, t2 - t1, int(r.iterations), rep)
+    best = cur if best is None or cur[0] < best[0] else best
+    del s
+print(json.dumps({"workload": wl, "best_total_ms": best[0] * 1e3, "new_ms": best[1] * 1e3,
+                  "first_solve_ms": best[2] * 1e3, "iterations": best[3], "best_rep": best[4]}))
+"""
+
+
+def setup_trace(args):
+    """Solver::new + first solve of two designs with the set-up's phase trace."""
+    env = dict(os.environ)
+    env["WITHIN_TRACE"] = "1"
+    root = os.path.dirname(os.path.abspath(__file__))
+    env["PYTHONPATH"] = root + os.pathsep + env.get("PYTHONPATH", "")
+    for wl in ("fixest", "akm10m"):
+        out = subprocess.run([sys.executable, "-c", _SETUP_CHILD, wl], capture_output=True, text=True,
+                             timeout=900, env=env)
+        if out.returncode:
+            print(out.stderr[-3000:], flush=True)
+            raise SystemExit(out.returncode)
+        res = json.loads(out.stdout.strip().splitlines()[-1])
+        reps = out.stderr.split("=== rep ")
+        trace = reps[res["best_rep"] + 1] if len(reps) > res["best_rep"] + 1 else ""
+        print(json.dumps(res), flush=True)
+        print("\n".join(l for l in trace.splitlines() if "within trace" in l), flush=True)
+
+
 def main():
     args = parse()
+    if args.setup_trace:
+        setup_trace(args)
+        return
     if args.kernel_timeline:
         kernel_timeline(args)
         return

@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <stdexcept>
 #include <string>
+#include <future>
 #include <vector>
 
 #include "segplan.hpp"
@@ -182,9 +183,12 @@ std::vector<ChannelPair> schwarz_channel_pairs(const HostDesign& d);
 
 // cross_tabs: the GPU cross-tab of every channel pair (schwarz_channel_pairs
 // order; the build may move their arrays out), or nullptr to accumulate them
-// on the host; both give the same bits.
+// on the host; both give the same bits.  ready (with cross_tabs): one future
+// per pair, ready when that pair's cross-tab is filled in (its exception is
+// the build's), so a pair starts as soon as its own cross-tab is back.
 BuildResult build_preconditioner(const HostDesign& d, const double* weights_internal,
-                                 const PrecondCfg& cfg, std::vector<CrossTab>* cross_tabs = nullptr);
+                                 const PrecondCfg& cfg, std::vector<CrossTab>* cross_tabs = nullptr,
+                                 const std::vector<std::shared_future<void>>* ready = nullptr);
 
 // ---- segmented-reduction plans ----
 struct HostPlan {

@@ -1139,7 +1139,8 @@ std::vector<ChannelPair> schwarz_channel_pairs(const HostDesign& d) {
 }
 
 BuildResult build_preconditioner(const HostDesign& d, const double* w, const PrecondCfg& cfg,
-                                 std::vector<CrossTab>* cross_tabs) {
+                                 std::vector<CrossTab>* cross_tabs,
+                                 const std::vector<std::shared_future<void>>* ready) {
     BuildResult out;
     if (cfg.kind == 0) return out;
     if (cfg.kind == 2) {  // operator/schwarz.rs:185-229
@@ -1216,6 +1217,7 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
             if (cross_tabs) {
                 // the GPU cross-tab over raw level ids: keep the active levels
                 // (every cell's levels are active) and renumber them
+                if (ready) (*ready)[pi].get();
                 CrossTab& X = (*cross_tabs)[pi];
                 if (nr == TR.n_levels && nc == TC.n_levels) {
                     // every level is active: the renumbering is the identity

@@ -24,6 +24,7 @@
 #include <cstring>
 #include <exception>
 #include <functional>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -2062,12 +2063,21 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
     std::vector<CrossTab> pre_xtabs;
     std::exception_ptr pre_err;
     std::thread pre_thread;
-    struct Joiner {   // the host build never outlives this frame, whatever throws
+    // the GPU cross-tabs: one host thread and stream per pair, each pair's
+    // future ready once its cross-tab is back on the host
+    std::unique_ptr<Arena> xt_arena;
+    std::vector<std::thread> xt_threads;
+    std::vector<std::promise<void>> xt_done;
+    std::vector<std::shared_future<void>> xt_ready;
+    struct Joiner {   // the host build and the cross-tab threads never outlive this frame, whatever throws
         std::thread& t;
+        std::vector<std::thread>& xt;
         ~Joiner() {
+            for (auto& x : xt)
+                if (x.joinable()) x.join();
             if (t.joinable()) t.join();
         }
-    } pre_join{pre_thread};
+    } pre_join{pre_thread, xt_threads};
     if (prebuilt) {
         if (prebuilt->n != D.n_dofs)
             throw WError(ERR_DIMENSION, "prebuilt preconditioner shape (" + std::to_string(prebuilt->n) + "x" +
@@ -2114,19 +2124,18 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         const int gx = s->schwarz.tuning.gpu_cross_tab;
         const bool use_xtab = pc.kind == 1 && (gx >= 2 || (gx == 1 && D.n_obs >= XTAB_MIN_OBS));
         if (use_xtab) {
-            PhaseTrace pt("GPU cross-tabs");
             double* w_dev = nullptr;
-            std::unique_ptr<Arena> tmp(new Arena());
-            if (weights) w_dev = tmp->upload(w);
+            xt_arena.reset(new Arena());
+            if (weights) w_dev = xt_arena->upload(w);
             const std::vector<ChannelPair> cps = schwarz_channel_pairs(D);
             pre_xtabs.resize(cps.size());
-            // one host thread and stream per pair: the pairs' device work and
-            // their copies back (page faults of fresh host memory included) overlap
-            std::vector<std::string> errs(cps.size());
-            std::vector<std::thread> th;
+            xt_done.resize(cps.size());
+            for (auto& p : xt_done) xt_ready.push_back(p.get_future().share());
+            // the pairs' device work and their copies back (page faults of
+            // fresh host memory included) overlap, and the host build starts
+            // each pair as soon as its cross-tab is back
             for (size_t i = 0; i < cps.size(); ++i)
-                th.emplace_back([&, i] {
-                    const ChannelPair& cp = cps[i];
+                xt_threads.emplace_back([&, i, cp = cps[i], w_dev] {
                     cudaStream_t st = nullptr;
                     try {
                         set_device(device);
@@ -2135,19 +2144,20 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
                                       op.codes[cp.term_b], D.terms[cp.term_b].n_levels, w_dev,
                                       cp.load_a < 0 ? nullptr : op.loads[cp.load_a],
                                       cp.load_b < 0 ? nullptr : op.loads[cp.load_b], pre_xtabs[i], st);
+                        xt_done[i].set_value();
                     } catch (const std::exception& e) {
-                        errs[i] = e.what();
+                        xt_done[i].set_exception(std::make_exception_ptr(WError(ERR_CUDA, e.what())));
+                    } catch (...) {
+                        xt_done[i].set_exception(std::current_exception());
                     }
                     if (st) cudaStreamDestroy(st);
                 });
-            for (auto& t : th) t.join();
-            for (const std::string& e : errs)
-                if (!e.empty()) throw WError(ERR_CUDA, e);
         }
         pre_thread = std::thread([&, use_xtab] {
             try {
                 PhaseTrace pt("preconditioner host build");
-                pre = build_preconditioner(D, weights ? w.data() : nullptr, pre_cfg, use_xtab ? &pre_xtabs : nullptr);
+                pre = build_preconditioner(D, weights ? w.data() : nullptr, pre_cfg, use_xtab ? &pre_xtabs : nullptr,
+                                           use_xtab ? &xt_ready : nullptr);
             } catch (...) {
                 pre_err = std::current_exception();
             }
@@ -2198,6 +2208,9 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         PhaseTrace pt("single-column workspaces");
         work_buffers(*s, 1);
     }
+    for (auto& x : xt_threads) x.join();
+    xt_threads.clear();
+    xt_arena.reset();
     if (pre_thread.joinable()) {
         PhaseTrace pt_wait("wait for the preconditioner host build");
         pre_thread.join();
