@@ -55,6 +55,18 @@ def test_tile_planner_properties(tmp_path):
     assert "plan ok" in out
 
 
+def test_locality_argsort(tmp_path):
+    """The locality sort's stable argsort (one- and two-pass parallel forms
+    and the counting sort) equals std::stable_sort (tests/cpp/argsort_test.cpp)."""
+    exe = tmp_path / "argsort_test"
+    csrc = os.path.join(ROOT, "within_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-I", csrc, "-o", str(exe),
+                    os.path.join(ROOT, "tests", "cpp", "argsort_test.cpp"),
+                    os.path.join(csrc, "host_design.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True, timeout=300).stdout
+    assert "argsort ok 12" in out
+
+
 def test_host_pool(tmp_path):
     """The set-up's host thread pool (host_pool.hpp): every item once, jobs
     posted from inside items and from several caller threads, the lowest

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <memory>
 #include <numeric>
 
 #include "host.hpp"
@@ -14,10 +15,62 @@ namespace wgpu {
 // The reference switches between a counting sort and a stable comparison sort
 // on n_obs < n_levels; both give the same permutation, which is all that is
 // observable, so the counting sort runs whenever its bucket array is small.
+//
+// A large input is sorted in two stable passes on the host pool: chunks of
+// the input partition the indices by the key's top 11 bits (per-chunk counts,
+// so every bucket keeps input order), then every bucket is counting-sorted by
+// the full key on its own; equal keys share a bucket and keep their order, so
+// the result is the same stable permutation.
 void stable_argsort_u32(const uint32_t* key, size_t n, size_t n_levels, uint32_t* perm) {
     if (n < n_levels && n_levels > (size_t)1 << 26) {
         for (size_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
         std::stable_sort(perm, perm + n, [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+        return;
+    }
+    if (n >= ((size_t)1 << 20) && n_levels <= ((size_t)1 << 26)) {
+        int bits = 0;
+        while (((size_t)1 << bits) < n_levels) ++bits;
+        const int hb = std::min(bits, 11), shift = bits - hb;
+        const size_t NB = (size_t)1 << hb, nch = 16, per = (n + nch - 1) / nch;
+        std::vector<size_t> cnt(nch * NB, 0);
+        par_for_each(nch, [&](size_t t) {
+            size_t* c = &cnt[t * NB];
+            const size_t i1 = std::min(n, (t + 1) * per);
+            for (size_t i = t * per; i < i1; ++i) ++c[key[i] >> shift];
+        });
+        std::vector<size_t> bstart(NB + 1, 0);
+        size_t o = 0;
+        for (size_t b = 0; b < NB; ++b) {
+            bstart[b] = o;
+            for (size_t t = 0; t < nch; ++t) {
+                const size_t c = cnt[t * NB + b];
+                cnt[t * NB + b] = o;
+                o += c;
+            }
+        }
+        bstart[NB] = o;
+        // with at most 2^11 levels the partition is the whole sort
+        std::unique_ptr<uint32_t[]> tmp(shift ? new uint32_t[n] : nullptr);   // first touched by the scatter
+        uint32_t* dst = shift ? tmp.get() : perm;
+        par_for_each(nch, [&](size_t t) {
+            size_t* c = &cnt[t * NB];
+            const size_t i1 = std::min(n, (t + 1) * per);
+            for (size_t i = t * per; i < i1; ++i) dst[c[key[i] >> shift]++] = (uint32_t)i;
+        });
+        if (!shift) return;
+        const size_t width = (size_t)1 << shift, BB = 16;
+        par_for_each((NB + BB - 1) / BB, [&](size_t g) {
+            std::vector<uint32_t> h(width + 1);
+            for (size_t b = g * BB; b < std::min(NB, (g + 1) * BB); ++b) {
+                const size_t b0 = bstart[b], b1 = bstart[b + 1];
+                if (b0 == b1) continue;
+                std::fill(h.begin(), h.end(), 0u);
+                const uint32_t base = (uint32_t)(b << shift);
+                for (size_t q = b0; q < b1; ++q) ++h[key[tmp[q]] - base + 1];
+                for (size_t l = 0; l < width; ++l) h[l + 1] += h[l];
+                for (size_t q = b0; q < b1; ++q) perm[b0 + h[key[tmp[q]] - base]++] = tmp[q];
+            }
+        });
         return;
     }
     std::vector<uint64_t> cur(n_levels + 1, 0);
