@@ -349,15 +349,18 @@ void HostPlan::add(uint32_t problem, const uint32_t* ptr, uint32_t n_seg, int T)
         tiles.push_back(t);
         p = hi;
     } while (p < pend || s < n_seg);
-    // split segments: positions spread over more than one tile
-    auto tile_of = [&](uint32_t pos) {
-        size_t i = (size_t)(std::upper_bound(starts.begin(), starts.end(), pos) - starts.begin()) - 1;
-        return ids[i];
+    // split segments: positions spread over more than one tile.  The tile of
+    // a position is the last position-holding tile starting at or before it;
+    // segment starts and ends only grow with g, so two cursors find them.
+    size_t ca = 0, cb = 0;
+    auto tile_of = [&](uint32_t pos, size_t& c) {
+        while (c + 1 < starts.size() && starts[c + 1] <= pos) ++c;
+        return ids[c];
     };
     for (uint32_t g = 0; g < n_seg; ++g) {
         uint32_t a = ptr[g], b = ptr[g + 1];
         if (b <= a) continue;
-        uint32_t t0 = tile_of(a), t1 = tile_of(b - 1);
+        uint32_t t0 = tile_of(a, ca), t1 = tile_of(b - 1, cb);
         if (t1 == t0) continue;
         int id = (int)splits.size();
         splits.push_back(SRSplit{problem, g, t0, t1});

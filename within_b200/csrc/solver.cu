@@ -34,6 +34,7 @@
 
 #include "../../include/within_gpu.h"
 #include "host.hpp"
+#include "host_pool.hpp"
 #include "kernels.cuh"
 #include "refine.cuh"
 #include "rowsweep.cuh"
@@ -892,6 +893,74 @@ constexpr int RED_GRID = 148 * 8;    // fixed reduction grid: deterministic part
 
 void set_device(int dev) { CK(cudaSetDevice(dev)); }
 
+// Integer passes over a column of codes on the host pool (chunks of 2^20
+// observations; every result is an exact count, so it does not depend on the
+// schedule).
+constexpr uint64_t CODE_CHUNK = (uint64_t)1 << 20;
+
+// number of runs (maximal blocks of equal consecutive codes)
+uint64_t count_runs(const uint32_t* codes, uint64_t n) {
+    const size_t nch = (size_t)((n + CODE_CHUNK - 1) / CODE_CHUNK);
+    std::vector<uint64_t> part(nch, 0);
+    par_for_each(nch, [&](size_t c) {
+        const uint64_t i0 = c * CODE_CHUNK, i1 = std::min(n, i0 + CODE_CHUNK);
+        uint64_t r = 0;
+        for (uint64_t i = i0; i < i1; ++i) r += (i == 0 || codes[i] != codes[i - 1]) ? 1 : 0;
+        part[c] = r;
+    });
+    uint64_t runs = 0;
+    for (uint64_t r : part) runs += r;
+    return runs;
+}
+
+// the level of every run, in run order
+std::vector<uint32_t> run_levels(const uint32_t* codes, uint64_t n, uint64_t runs) {
+    const size_t nch = (size_t)((n + CODE_CHUNK - 1) / CODE_CHUNK);
+    std::vector<uint64_t> off(nch + 1, 0);
+    par_for_each(nch, [&](size_t c) {
+        const uint64_t i0 = c * CODE_CHUNK, i1 = std::min(n, i0 + CODE_CHUNK);
+        uint64_t r = 0;
+        for (uint64_t i = i0; i < i1; ++i) r += (i == 0 || codes[i] != codes[i - 1]) ? 1 : 0;
+        off[c + 1] = r;
+    });
+    for (size_t c = 0; c < nch; ++c) off[c + 1] += off[c];
+    std::vector<uint32_t> lv(runs);
+    par_for_each(nch, [&](size_t c) {
+        const uint64_t i0 = c * CODE_CHUNK, i1 = std::min(n, i0 + CODE_CHUNK);
+        uint64_t q = off[c];
+        for (uint64_t i = i0; i < i1; ++i)
+            if (i == 0 || codes[i] != codes[i - 1]) lv[q++] = codes[i];
+    });
+    return lv;
+}
+
+// lp[l] = number of codes below l (lp has n_levels + 1 entries)
+void level_counts(const uint32_t* codes, uint64_t n, uint32_t n_levels, std::vector<uint32_t>& lp) {
+    lp.assign((size_t)n_levels + 1, 0);
+    const size_t nch = (size_t)std::min<uint64_t>(16, (n + CODE_CHUNK - 1) / CODE_CHUNK);
+    if (nch <= 1 || (uint64_t)n_levels * nch > ((uint64_t)1 << 24)) {
+        for (uint64_t i = 0; i < n; ++i) ++lp[(size_t)codes[i] + 1];
+    } else {
+        const uint64_t per = (n + nch - 1) / nch;
+        std::vector<std::vector<uint32_t>> h(nch);
+        par_for_each(nch, [&](size_t c) {
+            h[c].assign((size_t)n_levels + 1, 0);
+            const uint64_t i0 = c * per, i1 = std::min(n, i0 + per);
+            for (uint64_t i = i0; i < i1; ++i) ++h[c][(size_t)codes[i] + 1];
+        });
+        const size_t B = 65536;
+        par_for_each(((size_t)n_levels + 1 + B - 1) / B, [&](size_t b) {
+            const size_t l1 = std::min<size_t>((size_t)n_levels + 1, (b + 1) * B);
+            for (size_t l = b * B; l < l1; ++l) {
+                uint32_t t = 0;
+                for (size_t c = 0; c < nch; ++c) t += h[c][l];
+                lp[l] = t;
+            }
+        });
+    }
+    for (uint32_t l = 0; l < n_levels; ++l) lp[l + 1] += lp[l];
+}
+
 void ensure_scatter(within_solver& s, int K) {
     int ki = kidx(K);
     if (s.scatter_ready[ki]) return;
@@ -1024,8 +1093,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
                 nbk += (int)(T.n_levels * ncol);
                 continue;
             }
-            uint64_t runs = 0;
-            for (uint64_t i = 0; i < n; ++i) runs += (i == 0 || codes[i] != codes[i - 1]) ? 1 : 0;
+            const uint64_t runs = count_runs(codes.data(), n);
             n_runs[t] = runs;
             if (nr < RW_MAX_RUN && ncol <= rw_max_cols<K>() && (T.sorted != 0 || runs * 3 <= n)) {
                 cls[t] = CLS_RUN;
@@ -1083,8 +1151,14 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
             // run heads per range
             std::vector<uint32_t> cnt(G, 0);
             const uint64_t runs = n_runs[t];
-            for (uint64_t i = 0; i < n; ++i)
-                if (i == 0 || codes[i] != codes[i - 1]) ++cnt[i / rpr];
+            par_for_each((size_t)((G + 63) / 64), [&](size_t b) {
+                for (uint64_t g = b * 64; g < std::min<uint64_t>(G, (b + 1) * 64); ++g) {
+                    const uint64_t i0 = g * rpr, i1 = std::min<uint64_t>(n, i0 + rpr);
+                    uint32_t c = 0;
+                    for (uint64_t i = i0; i < i1; ++i) c += (i == 0 || codes[i] != codes[i - 1]) ? 1u : 0u;
+                    cnt[g] = c;
+                }
+            });
             const bool sorted_runs = T.sorted != 0;
             const int j = rp.n_run++;
             RwRun& rr = rp.run[j];
@@ -1118,10 +1192,7 @@ within_solver::RowSweepK& ensure_rowsweep(within_solver& s) {
                 rr.range_base = A.upload(base);
                 rr.run_sum = A.alloc<double>(runs * ncol * K);
                 // combine: run sums grouped by level (stable in run order)
-                std::vector<uint32_t> run_level;
-                run_level.reserve(runs);
-                for (uint64_t i = 0; i < n; ++i)
-                    if (i == 0 || codes[i] != codes[i - 1]) run_level.push_back(codes[i]);
+                std::vector<uint32_t> run_level = run_levels(codes.data(), n, runs);
                 std::vector<uint32_t> perm(runs);
                 stable_argsort_u32(run_level.data(), runs, T.n_levels, perm.data());
                 std::vector<uint32_t> lp((size_t)T.n_levels + 1, 0);
@@ -2177,9 +2248,7 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
         const Term& T = D.terms[t];
         const auto& codes = D.codes[t];
         std::vector<uint32_t>& lp = s->level_ptr_host[t];
-        lp.assign((size_t)T.n_levels + 1, 0);
-        for (uint32_t c : codes) ++lp[(size_t)c + 1];
-        for (uint32_t l = 0; l < T.n_levels; ++l) lp[l + 1] += lp[l];
+        level_counts(codes.data(), D.n_obs, T.n_levels, lp);
         uint32_t* dlp = A.upload(lp);
         uint32_t* order = nullptr;
         if (!T.sorted) {
