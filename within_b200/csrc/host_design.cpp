@@ -87,44 +87,70 @@ HostDesign make_design(uint64_t n_obs, const std::vector<EffectIn>& effects) {
     HostDesign d;
     if (effects.size() > (size_t)MAX_TERMS)
         throw WError(ERR_UNSUPPORTED, "at most " + std::to_string(MAX_TERMS) + " effects are supported");
+    // the finiteness of every slope column, checked side by side (the first
+    // failing column in effect order is reported, at its first bad index)
+    std::vector<const double*> zcols;
+    for (const EffectIn& ef : effects)
+        for (const double* z : ef.slopes) zcols.push_back(z);
+    std::vector<uint64_t> bad(zcols.size(), UINT64_MAX);
+    par_for_each(zcols.size(), [&](size_t j) {
+        for (uint64_t i = 0; i < n_obs; ++i)
+            if (!std::isfinite(zcols[j][i])) {
+                bad[j] = i;
+                break;
+            }
+    });
+    size_t zj = 0;
     for (size_t e = 0; e < effects.size(); ++e) {
         const EffectIn& ef = effects[e];
         Term t;
         if (ef.intercept) t.cols.push_back(-1);
-        for (size_t s = 0; s < ef.slopes.size(); ++s) {
-            const double* z = ef.slopes[s];
-            for (uint64_t i = 0; i < n_obs; ++i)
-                if (!std::isfinite(z[i]))
-                    throw WError(ERR_BUILD, "slope " + std::to_string(s) + " loading at index " +
-                                                std::to_string(i) + " must be finite, got " +
-                                                std::to_string(z[i]));
-            d.loads.emplace_back(z, z + n_obs);
-            t.cols.push_back((int)d.loads.size() - 1);
+        for (size_t s = 0; s < ef.slopes.size(); ++s, ++zj) {
+            if (bad[zj] != UINT64_MAX)
+                throw WError(ERR_BUILD, "slope " + std::to_string(s) + " loading at index " +
+                                            std::to_string(bad[zj]) + " must be finite, got " +
+                                            std::to_string(ef.slopes[s][bad[zj]]));
+            t.cols.push_back((int)zj);
         }
         if (t.cols.empty()) throw WError(ERR_BUILD, "an effect must have an intercept or at least one slope");
         if (t.cols.size() > (size_t)MAX_COLS)
             throw WError(ERR_UNSUPPORTED, "at most " + std::to_string(MAX_COLS - 1) + " slopes per effect are supported");
         d.terms.push_back(t);
-        d.codes.emplace_back(ef.levels, ef.levels + n_obs);
     }
-    if (d.loads.size() > (size_t)MAX_LOADS)
+    if (zcols.size() > (size_t)MAX_LOADS)
         throw WError(ERR_UNSUPPORTED, "at most " + std::to_string(MAX_LOADS) + " slope columns are supported");
     if (n_obs == 0) throw WError(ERR_BUILD, "no observations provided");
     if (n_obs > (uint64_t)std::numeric_limits<uint32_t>::max())
         throw WError(ERR_UNSUPPORTED, "more than 2^32-1 observations in one design");
     d.n_obs = n_obs;
+    // codes and loading columns copied, and every term's largest code and
+    // sortedness found, side by side
+    d.codes.resize(effects.size());
+    d.loads.resize(zcols.size());
+    std::vector<uint32_t> mxs(effects.size(), 0);
+    std::vector<char> srt(effects.size(), 1);
+    par_for_each(effects.size() + zcols.size(), [&](size_t i) {
+        if (i < effects.size()) {
+            d.codes[i].assign(effects[i].levels, effects[i].levels + n_obs);
+            uint32_t mx = 0, prev = 0;
+            bool sorted = true;
+            for (uint32_t v : d.codes[i]) {
+                mx = std::max(mx, v);
+                sorted = sorted && v >= prev;
+                prev = v;
+            }
+            mxs[i] = mx;
+            srt[i] = sorted ? 1 : 0;
+        } else {
+            const size_t j = i - effects.size();
+            d.loads[j].assign(zcols[j], zcols[j] + n_obs);
+        }
+    });
     uint64_t offset = 0;
     for (size_t q = 0; q < d.terms.size(); ++q) {
-        uint32_t mx = 0, prev = 0;
-        bool sorted = true;
-        for (uint32_t v : d.codes[q]) {
-            mx = std::max(mx, v);
-            sorted = sorted && v >= prev;
-            prev = v;
-        }
         Term& t = d.terms[q];
-        uint64_t nl = (uint64_t)mx + 1;
-        t.sorted = sorted;
+        uint64_t nl = (uint64_t)mxs[q] + 1;
+        t.sorted = srt[q] != 0;
         t.offset = (uint32_t)std::min<uint64_t>(offset, std::numeric_limits<uint32_t>::max());
         offset += nl * t.cols.size();
         t.n_levels = (uint32_t)std::min<uint64_t>(nl, std::numeric_limits<uint32_t>::max());

@@ -2555,13 +2555,17 @@ int within_design_from_categories(const uint32_t* codes, uint64_t n_obs, uint64_
         if (n_obs == 0) throw WError(ERR_BUILD, "no observations provided");
         auto d = std::make_unique<within_design>();
         d->n_obs = n_obs;
-        for (uint64_t f = 0; f < n_factors; ++f) {
-            d->levels.emplace_back(codes + f * n_obs, codes + (f + 1) * n_obs);
-            d->intercept.push_back(1);
-            d->slope_of.emplace_back();
-        }
+        d->levels.resize(n_factors);
+        d->intercept.assign(n_factors, 1);
+        d->slope_of.resize(n_factors);
+        // the columns copied (and their largest codes found) side by side
+        std::vector<uint32_t> mx(n_factors, 0);
+        par_for_each(n_factors, [&](size_t f) {
+            d->levels[f].assign(codes + f * n_obs, codes + (f + 1) * n_obs);
+            mx[f] = *std::max_element(d->levels[f].begin(), d->levels[f].end());
+        });
         uint64_t nd = 0;
-        for (auto& l : d->levels) nd += (uint64_t)*std::max_element(l.begin(), l.end()) + 1;
+        for (uint32_t m : mx) nd += (uint64_t)m + 1;
         d->n_dofs = nd;
         *out = d.release();
     });
@@ -2575,21 +2579,31 @@ int within_design_from_effects(uint64_t n_obs, uint64_t n_effects, const uint32_
         if (n_obs == 0) throw WError(ERR_BUILD, "no observations provided");
         auto d = std::make_unique<within_design>();
         d->n_obs = n_obs;
-        uint64_t si = 0, nd = 0;
+        uint64_t si = 0;
         for (uint64_t e = 0; e < n_effects; ++e) {
-            d->levels.emplace_back(levels[e], levels[e] + n_obs);
             d->intercept.push_back(intercept[e] ? 1 : 0);
             std::vector<size_t> idx;
-            for (uint64_t j = 0; j < n_slopes[e]; ++j, ++si) {
-                d->slopes.emplace_back(slopes[si], slopes[si] + n_obs);
-                idx.push_back(d->slopes.size() - 1);
-            }
+            for (uint64_t j = 0; j < n_slopes[e]; ++j, ++si) idx.push_back(si);
             if (!intercept[e] && idx.empty())
                 throw WError(ERR_BUILD, "an effect must have an intercept or at least one slope");
             d->slope_of.push_back(idx);
-            nd += ((uint64_t)*std::max_element(levels[e], levels[e] + n_obs) + 1) *
-                  ((intercept[e] ? 1 : 0) + idx.size());
         }
+        // the level and slope columns copied (and the largest codes found) side by side
+        d->levels.resize(n_effects);
+        d->slopes.resize(si);
+        std::vector<uint32_t> mx(n_effects, 0);
+        par_for_each(n_effects + si, [&](size_t i) {
+            if (i < n_effects) {
+                d->levels[i].assign(levels[i], levels[i] + n_obs);
+                mx[i] = *std::max_element(d->levels[i].begin(), d->levels[i].end());
+            } else {
+                const size_t j = i - n_effects;
+                d->slopes[j].assign(slopes[j], slopes[j] + n_obs);
+            }
+        });
+        uint64_t nd = 0;
+        for (uint64_t e = 0; e < n_effects; ++e)
+            nd += ((uint64_t)mx[e] + 1) * ((intercept[e] ? 1 : 0) + d->slope_of[e].size());
         d->n_dofs = nd;
         *out = d.release();
     });
