@@ -1175,10 +1175,36 @@ BuildResult build_preconditioner(const HostDesign& d, const double* w, const Pre
         for (uint32_t c = 0; c < d.terms[t].cols.size(); ++c) ch.push_back({t, c});
     bool any_slope = false;
     for (auto& x : ch) any_slope = any_slope || d.terms[x.term].cols[x.col] >= 0;
+    // the levels that occur, per term: chunks of observations mark their own
+    // copy, merged by blocks of levels (all on the host pool)
     std::vector<std::vector<char>> active(d.terms.size());
     for (size_t t = 0; t < d.terms.size(); ++t) {
-        active[t].assign(d.terms[t].n_levels, 0);
-        for (uint32_t v : d.codes[t]) active[t][v] = 1;
+        const uint32_t L = d.terms[t].n_levels;
+        const uint32_t* cd = d.codes[t].data();
+        const uint64_t n = d.n_obs;
+        const size_t nch = n >= ((uint64_t)1 << 20) && (uint64_t)L * 16 <= ((uint64_t)1 << 28) ? 16 : 1;
+        if (nch == 1) {
+            active[t].assign(L, 0);
+            for (uint64_t i = 0; i < n; ++i) active[t][cd[i]] = 1;
+            continue;
+        }
+        const uint64_t per = (n + nch - 1) / nch;
+        std::vector<std::vector<char>> part(nch);
+        par_for_each(nch, [&](size_t c) {
+            part[c].assign(L, 0);
+            const uint64_t i1 = std::min(n, (c + 1) * per);
+            for (uint64_t i = c * per; i < i1; ++i) part[c][cd[i]] = 1;
+        });
+        active[t].assign(L, 0);
+        const size_t B = 1 << 16;
+        par_for_each(((size_t)L + B - 1) / B, [&](size_t b) {
+            const size_t l1 = std::min<size_t>(L, (b + 1) * B);
+            for (size_t l = b * B; l < l1; ++l) {
+                char a = 0;
+                for (size_t c = 0; c < nch; ++c) a |= part[c][l];
+                active[t][l] = a;
+            }
+        });
     }
     // channel pairs of different terms, each built on its own host thread
     // and concatenated in pair order
