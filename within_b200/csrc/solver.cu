@@ -2336,23 +2336,16 @@ within_solver* make_solver(const within_design* d, const double* weights, const 
 // allocated caller buffers fault page by page, so a single-threaded copy of a
 // 10M-row column costs more than the device solve.
 void par_memcpy(void* dst, const void* src, size_t bytes) {
-    const size_t chunk = (size_t)8 << 20;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned t = (unsigned)std::min<size_t>(std::min<unsigned>(hw, 16u), (bytes + chunk - 1) / chunk);
-    if (t <= 1) {
+    const size_t piece = (size_t)1 << 20;   // pieces of 1 MiB on the host pool
+    const size_t n = (bytes + piece - 1) / piece;
+    if (n <= 1) {
         std::memcpy(dst, src, bytes);
         return;
     }
-    const size_t per = (bytes + t - 1) / t;
-    std::vector<std::thread> pool;
-    for (unsigned j = 1; j < t; ++j) {
-        const size_t a = j * per;
-        if (a >= bytes) break;
-        const size_t len = std::min(per, bytes - a);
-        pool.emplace_back([=] { std::memcpy((char*)dst + a, (const char*)src + a, len); });
-    }
-    std::memcpy(dst, src, std::min(per, bytes));
-    for (auto& th : pool) th.join();
+    par_for_each(n, [&](size_t j) {
+        const size_t a = j * piece, len = std::min(piece, bytes - a);
+        std::memcpy((char*)dst + a, (const char*)src + a, len);
+    });
 }
 
 // Whether a host pointer is page-locked memory the DMA engines can read or
