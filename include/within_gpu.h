@@ -128,7 +128,11 @@ uint64_t within_design_n_dofs(const within_design* d);
 /* Solver::new (solver.rs:361-411).  weights (host, caller order) may be NULL;
  * cfg NULL = PreconditionerInput::Default; prebuilt non-NULL =
  * PreconditionerInput::Prebuilt (its DOF count must match).  device < 0 picks
- * the current device.  The design is copied; it may be freed afterwards. */
+ * the current device.  The design is copied; it may be freed afterwards.
+ * The host side of the build runs on a process-wide pool of up to 16 host
+ * threads (the environment variable WITHIN_HOST_THREADS lowers that; 1 runs
+ * it on the calling thread); the result does not depend on the count.  The
+ * single-column workspaces and plans of the first solve are made here. */
 int within_solver_new(const within_design* design, const double* weights,
                       const within_precond_config* cfg, const within_preconditioner* prebuilt,
                       int32_t device, within_solver** out);
