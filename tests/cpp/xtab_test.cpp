@@ -12,6 +12,9 @@
 #include <cstring>
 #include <numeric>
 #include <random>
+#include <chrono>
+#include <future>
+#include <thread>
 using namespace wgpu;
 
 static CrossTab cross_tab_like_gpu(const HostDesign& d, const double* w, const ChannelPair& cp) {
@@ -136,11 +139,33 @@ int main() {
         if (trial % 5 == 4) cfg.dense_threshold = 8;   // sampled Schur complements and round factors
         std::vector<CrossTab> xt;
         for (const ChannelPair& cp : schwarz_channel_pairs(d)) xt.push_back(cross_tab_like_gpu(d, wp, cp));
+        std::vector<CrossTab> xt2 = xt;   // for the hand-over through per-pair futures below
         BuildResult host = build_preconditioner(d, wp, cfg, nullptr);
         BuildResult pre = build_preconditioner(d, wp, cfg, &xt);
         if (host.kind != pre.kind || host.n_warnings != pre.n_warnings || !same_host(host.schwarz, pre.schwarz)) {
             printf("FAIL trial %d (weighted %d slopes %d)\n", trial, (int)weighted, (int)slopes);
             return 1;
+        }
+        // the cross-tabs handed over one pair at a time, in reverse order and late,
+        // through the per-pair futures: the same image
+        {
+            std::vector<CrossTab> late(xt2.size());
+            std::vector<std::promise<void>> done(xt2.size());
+            std::vector<std::shared_future<void>> ready;
+            for (auto& p : done) ready.push_back(p.get_future().share());
+            std::thread feeder([&] {
+                for (size_t i = xt2.size(); i-- > 0;) {
+                    std::this_thread::sleep_for(std::chrono::milliseconds(2));
+                    late[i] = std::move(xt2[i]);
+                    done[i].set_value();
+                }
+            });
+            BuildResult fut = build_preconditioner(d, wp, cfg, &late, &ready);
+            feeder.join();
+            if (fut.kind != host.kind || fut.n_warnings != host.n_warnings || !same_host(host.schwarz, fut.schwarz)) {
+                printf("FAIL trial %d (futures)\n", trial);
+                return 1;
+            }
         }
         ++cases;
     }

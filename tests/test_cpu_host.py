@@ -98,8 +98,9 @@ def test_schwarz_build_from_gpu_form_cross_tabs(tmp_path):
     """The additive-Schwarz build from cross-tabs in the GPU cross-tab's form
     (sorted keys, per-cell sums in observation order, CSR + CSC over raw level
     ids) gives the host-accumulated build's image bit for bit: unweighted,
-    weighted with zero weights, slopes, unused levels, round factors
-    (tests/cpp/xtab_test.cpp)."""
+    weighted with zero weights, slopes, unused levels, round factors; also
+    when the cross-tabs arrive late, one pair at a time, through the per-pair
+    futures the build waits on (tests/cpp/xtab_test.cpp)."""
     exe = tmp_path / "xtab_test"
     csrc = os.path.join(ROOT, "within_b200", "csrc")
     subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-I", csrc, "-o", str(exe),
